@@ -1,0 +1,884 @@
+// The host side of World.step around the solve stage, for boxes, spheres and capsules.
+// Restates, for the parts it covers:
+//   src/world.js     addBody/_write 2152-2274 (mass, inertia, size, reach), _bounds/_boundsOf
+//                    1574-1630, step 880-1072 (order of the step), transforms 1040-1057
+//   src/shapes.js    volume 14-21, inertia 37-56
+//   src/core/check.js quat 106-117
+//   src/broadphase.js fat boxes (fat 206-219, FAT 1/4, AHEAD 16), update 121-137, overlap 176-181
+//   src/pairs.js     found 180-215, remove 217-232, forget 235-241, holds 340-357
+//   src/contact.js   narrow 296-327, find 334-368, emit 889-921, carry 999-1036, basis 1283-1292,
+//                    load 1244-1276, rest 1318-1329, store 1067-1088, keep 1091-1115,
+//                    touched 2178-2213 (the touching flags; no event list)
+//   src/graph.js     colour 105-170, arrange 178-214
+// The broadphase files fat boxes in a uniform grid instead of the reference's two AABB trees
+// (src/tree.js): the same pairs are found, offered in ascending slot order rather than tree
+// order, so pair order (and with it row order and colours) can differ from the reference's.
+#include "../../include/bearing_world.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "collide.hpp"
+
+namespace {
+
+using bearing::Manifold;
+using bearing::Shape;
+
+constexpr int P = 4;
+constexpr int COLOURS = 32;
+constexpr int OVERFLOW_ = 32;
+constexpr int RESTING = 33;
+constexpr int DIGIT = 12;
+constexpr int DIGITS = 1 << DIGIT;
+constexpr double PIXEL = 1.0 / 200.0;     // src/contact.js:125
+constexpr double FAT = 1.0 / 4.0;         // src/broadphase.js:15
+constexpr double AHEAD = 16;              // src/broadphase.js:37
+constexpr double PI = 3.141592653589793;
+constexpr double INF = std::numeric_limits<double>::infinity();
+constexpr int KINEMATIC = 2;
+
+inline double jmax(double a, double b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  if (a > b) return a;
+  if (b > a) return b;
+  if (a == 0 && b == 0) return std::signbit(a) ? b : a;
+  return a;
+}
+inline double jmin(double a, double b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  if (a < b) return a;
+  if (b < a) return b;
+  if (a == 0 && b == 0) return std::signbit(a) ? a : b;
+  return a;
+}
+
+// axesOf: src/core/math.js:222-227.
+inline void axesOf(const double* q, double* ax) {
+  const double x = q[0], y = q[1], z = q[2], w = q[3];
+  ax[0] = 1 - 2 * (y * y + z * z); ax[1] = 2 * (x * y + z * w); ax[2] = 2 * (x * z - y * w);
+  ax[3] = 2 * (x * y - z * w); ax[4] = 1 - 2 * (x * x + z * z); ax[5] = 2 * (y * z + x * w);
+  ax[6] = 2 * (x * z + y * w); ax[7] = 2 * (y * z - x * w); ax[8] = 1 - 2 * (x * x + y * y);
+}
+
+template <class T>
+void grow(std::vector<T>& v, size_t n, T fill = T()) {
+  if (v.size() < n) v.resize(n, fill);
+}
+
+// The step's manifolds: src/contact.js:149-269, the columns this path uses.
+struct Contacts {
+  int count = 0, solved = 0, capacity = 0;
+  int starts[COLOURS + 3] = {};
+  std::vector<int32_t> a, b, pair, colour, order, row;
+  std::vector<uint8_t> points, sliding;
+  std::vector<double> normal, t1, t2, friction, restitution, tolerance, patch;
+  std::vector<double> rollImpulse1, rollImpulse2, spinImpulse, tangentImpulse1, tangentImpulse2, drift1, drift2;
+  std::vector<double> separation, normalImpulse, point, shift, gap, maxNormalImpulse, relativeVelocity;
+  std::vector<double> anchorA, anchorB;
+  std::vector<uint32_t> pid;
+  std::vector<double> room;
+  std::vector<int32_t> digits;
+
+  void alloc(int c) {
+    const size_t m = static_cast<size_t>(c), p = m * P;
+    a.resize(m); b.resize(m); pair.resize(m); colour.resize(m); order.resize(m); row.resize(m);
+    points.resize(m); sliding.resize(m);
+    normal.resize(3 * m); t1.resize(3 * m); t2.resize(3 * m);
+    friction.resize(m); restitution.resize(m); tolerance.resize(m); patch.resize(m);
+    rollImpulse1.resize(m); rollImpulse2.resize(m); spinImpulse.resize(m);
+    tangentImpulse1.resize(m); tangentImpulse2.resize(m); drift1.resize(m); drift2.resize(m);
+    separation.resize(p); normalImpulse.resize(p); point.resize(3 * p); shift.resize(3 * p);
+    gap.resize(m); maxNormalImpulse.resize(p); relativeVelocity.resize(p);
+    anchorA.resize(3 * m); anchorB.resize(3 * m);
+    pid.resize(p);
+    room.resize(3 * p);
+    capacity = c;
+  }
+  // ensure: src/contact.js:250-255.
+  void ensure(int n) {
+    if (n <= capacity) return;
+    int c = capacity > 1 ? capacity : 1;
+    while (c < n) c *= 2;
+    alloc(c);
+  }
+};
+
+// The pair list: src/pairs.js (awake pairs only: every pair here has an awake body).
+struct Pairs {
+  int count = 0, active = 0;
+  std::vector<int32_t> a, b;
+  std::vector<uint8_t> points, touching;
+  std::vector<uint32_t> pid;
+  std::vector<double> normalImpulse, friction, slip, twist;
+  std::unordered_map<uint64_t, int32_t> index;
+
+  static uint64_t key(int x, int y) { return (static_cast<uint64_t>(x) << 32) | static_cast<uint32_t>(y); }
+  void reserve(int n) {
+    const size_t c = static_cast<size_t>(n);
+    if (a.size() >= c) return;
+    size_t cap = a.size() > 16 ? a.size() : 16;
+    while (cap < c) cap *= 2;
+    a.resize(cap); b.resize(cap); points.resize(cap); touching.resize(cap);
+    pid.resize(P * cap); normalImpulse.resize(P * cap);
+    friction.resize(3 * cap); slip.resize(3 * cap); twist.resize(3 * cap);
+  }
+  // found: src/pairs.js:180-215 (whole bodies, no sensors or filters).
+  void found(int x, int y, const uint8_t* type) {
+    if (type[x] != BG_DYNAMIC && type[y] != BG_DYNAMIC) return;
+    const int lo = x < y ? x : y, hi = x < y ? y : x;
+    if (index.count(key(lo, hi))) return;
+    const int p = count;
+    reserve(p + 1);
+    a[p] = lo; b[p] = hi; points[p] = 0; touching[p] = 0;
+    index[key(lo, hi)] = p;
+    count++;
+    active = count;
+  }
+  void moveTo(int from, int to) {
+    a[to] = a[from]; b[to] = b[from]; points[to] = points[from]; touching[to] = touching[from];
+    for (int k = 0; k < P; k++) { pid[P * to + k] = pid[P * from + k]; normalImpulse[P * to + k] = normalImpulse[P * from + k]; }
+    for (int k = 0; k < 3; k++) {
+      friction[3 * to + k] = friction[3 * from + k];
+      slip[3 * to + k] = slip[3 * from + k];
+      twist[3 * to + k] = twist[3 * from + k];
+    }
+    index[key(a[to], b[to])] = to;
+  }
+  // remove: src/pairs.js:217-232 (one run).
+  void remove(int p) {
+    index.erase(key(a[p], b[p]));
+    const int last = --count;
+    if (p != last) moveTo(last, p);
+    active = count;
+  }
+  // forget: src/pairs.js:235-241.
+  void forget(int p) {
+    points[p] = 0;
+    touching[p] = 0;
+  }
+};
+
+}  // namespace
+
+struct bw_world {
+  std::string error;
+  double gravity[3] = {0, -9.81, 0};
+  int substeps = 8;
+  int64_t stepCount = 0;
+  double stepDt = 0;
+  int n = 0;   // slots in use
+  // Per-slot columns: src/world.js:228-311.
+  std::vector<double> position, rotation, velocity, angular, dims, mass, inertia, invInertia, tumbled, ceiling;
+  std::vector<double> friction, restitution, damping, angularDamping, gravityScale, invMass, size, reach;
+  std::vector<double> axes, box, motion, invI, start, startQ;
+  std::vector<uint8_t> type, shape, framed, lock, frozen, awake;
+  std::vector<int32_t> jointHead, awakeList;
+  std::vector<float> transforms;
+  // Broadphase: each slot's fat box (src/broadphase.js), filed in a uniform grid.
+  std::vector<double> fat;
+  std::vector<uint8_t> filed, isMoved, large;
+  std::vector<int32_t> moved;
+  double cell = 0;
+  std::unordered_map<uint64_t, std::vector<int32_t>> grid;
+  std::vector<int32_t> largeList;
+  std::vector<int32_t> seen;
+  int32_t seenMark = 0;
+  Pairs pairs;
+  Contacts c;
+  bw_solver solver = nullptr;
+  void* solverUser = nullptr;
+  bool begun = false;
+  bw_stats stats = {};
+
+  void resize(int slots) {
+    const size_t s = static_cast<size_t>(slots);
+    grow(position, 3 * s); grow(rotation, 4 * s); grow(velocity, 3 * s); grow(angular, 3 * s);
+    grow(dims, 3 * s); grow(mass, s); grow(inertia, 3 * s); grow(invInertia, 3 * s);
+    grow(tumbled, 3 * s); grow(ceiling, s); grow(friction, s); grow(restitution, s); grow(damping, s);
+    grow(angularDamping, s); grow(gravityScale, s); grow(invMass, s); grow(size, s); grow(reach, s);
+    grow(axes, 9 * s); grow(box, 6 * s); grow(motion, s); grow(invI, 6 * s); grow(start, 3 * s); grow(startQ, 4 * s);
+    grow(type, s); grow(shape, s); grow(framed, s); grow(lock, s); grow(frozen, s); grow(awake, s);
+    grow(jointHead, s); grow(awakeList, s); grow(transforms, 7 * s);
+    grow(fat, 6 * s); grow(filed, s); grow(isMoved, s); grow(large, s); grow(seen, s);
+  }
+
+  // _boundsOf: src/world.js:1581-1630 (boxes, spheres, capsules).
+  void boundsOf(int s, double dt, double gl) {
+    const int s3 = s * 3, s4 = s * 4, a9 = s * 9, b6 = s * 6;
+    double* ax = &axes[a9];
+    axesOf(&rotation[s4], ax);
+    double m = 0;
+    if (type[s] != BG_STATIC) {
+      const double* v = &velocity[s3];
+      const double* w = &angular[s3];
+      const double speed = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+        + (type[s] == BG_DYNAMIC ? gl * std::fabs(gravityScale[s]) * dt : 0)
+        + std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]) * reach[s];
+      m = speed * dt;
+    }
+    motion[s] = m;
+    double ex, ey, ez;
+    const double* d = &dims[s3];
+    if (shape[s] == BG_BOX) {
+      const double hx = d[0] * 0.5, hy = d[1] * 0.5, hz = d[2] * 0.5;
+      ex = std::fabs(ax[0]) * hx + std::fabs(ax[3]) * hy + std::fabs(ax[6]) * hz;
+      ey = std::fabs(ax[1]) * hx + std::fabs(ax[4]) * hy + std::fabs(ax[7]) * hz;
+      ez = std::fabs(ax[2]) * hx + std::fabs(ax[5]) * hy + std::fabs(ax[8]) * hz;
+    } else if (shape[s] == BG_SPHERE) {
+      ex = ey = ez = d[0];
+    } else {
+      const double r = d[0], hl = (d[1] - 2 * r) * 0.5;
+      ex = std::fabs(ax[3]) * hl + r; ey = std::fabs(ax[4]) * hl + r; ez = std::fabs(ax[5]) * hl + r;
+    }
+    const double g = m + size[s] * PIXEL;
+    const double cx = position[s3], cy = position[s3 + 1], cz = position[s3 + 2];
+    box[b6] = cx - ex - g; box[b6 + 1] = cy - ey - g; box[b6 + 2] = cz - ez - g;
+    box[b6 + 3] = cx + ex + g; box[b6 + 4] = cy + ey + g; box[b6 + 5] = cz + ez + g;
+  }
+
+  // fat(): src/broadphase.js:206-219.
+  void fatten(int s, double time) {
+    const int b = 6 * s;
+    if (type[s] == BG_STATIC) {
+      for (int k = 0; k < 6; k++) fat[b + k] = box[b + k];
+      return;
+    }
+    const double mg = size[s] * FAT;
+    for (int k = 0; k < 3; k++) {
+      const double d = velocity[3 * s + k] * time;
+      fat[b + k] = box[b + k] - mg + (d < 0 ? d : 0);
+      fat[b + k + 3] = box[b + k + 3] + mg + (d > 0 ? d : 0);
+    }
+  }
+
+  // The grid the fat boxes are filed in.
+  void cellRange(int s, int64_t* lo, int64_t* hi) const {
+    for (int k = 0; k < 3; k++) {
+      lo[k] = static_cast<int64_t>(std::floor(fat[6 * s + k] / cell));
+      hi[k] = static_cast<int64_t>(std::floor(fat[6 * s + k + 3] / cell));
+    }
+  }
+  static uint64_t cellKey(int64_t x, int64_t y, int64_t z) {
+    return (static_cast<uint64_t>(x & 0x1fffff) << 42) | (static_cast<uint64_t>(y & 0x1fffff) << 21) |
+           static_cast<uint64_t>(z & 0x1fffff);
+  }
+  void fileIn(int s) {
+    int64_t lo[3], hi[3];
+    cellRange(s, lo, hi);
+    const int64_t cells = (hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+    if (cells > 64) {
+      large[s] = 1;
+      largeList.push_back(s);
+      return;
+    }
+    large[s] = 0;
+    for (int64_t x = lo[0]; x <= hi[0]; x++)
+      for (int64_t y = lo[1]; y <= hi[1]; y++)
+        for (int64_t z = lo[2]; z <= hi[2]; z++) grid[cellKey(x, y, z)].push_back(s);
+  }
+  void fileOut(int s) {
+    if (large[s]) {
+      largeList.erase(std::find(largeList.begin(), largeList.end(), s));
+      large[s] = 0;
+      return;
+    }
+    int64_t lo[3], hi[3];
+    cellRange(s, lo, hi);
+    for (int64_t x = lo[0]; x <= hi[0]; x++)
+      for (int64_t y = lo[1]; y <= hi[1]; y++)
+        for (int64_t z = lo[2]; z <= hi[2]; z++) {
+          auto it = grid.find(cellKey(x, y, z));
+          if (it == grid.end()) continue;
+          auto& v = it->second;
+          v.erase(std::find(v.begin(), v.end(), s));
+          if (v.empty()) grid.erase(it);
+        }
+  }
+  void mark(int s) {
+    if (isMoved[s]) return;
+    isMoved[s] = 1;
+    moved.push_back(s);
+  }
+  bool fatOverlap(int x, int y) const {
+    const double* fa = &fat[6 * x];
+    const double* fb = &fat[6 * y];
+    return fa[0] <= fb[3] && fa[3] >= fb[0] && fa[1] <= fb[4] && fa[4] >= fb[1] && fa[2] <= fb[5] && fa[5] >= fb[2];
+  }
+
+  // Broadphase.update (src/broadphase.js:121-137) and candidates (146-165).
+  void broadphase(double dt) {
+    if (cell == 0) {
+      double sum = 0;
+      int count = 0;
+      for (int s = 0; s < n; s++)
+        if (type[s] != BG_STATIC) { sum += reach[s]; count++; }
+      cell = count > 0 ? jmax(4 * sum / count, 0.25) : 1;
+      for (int s = 0; s < n; s++) if (filed[s]) fileIn(s);
+    }
+    for (int i = 0; i < static_cast<int>(awakeList.size()) && i < awakeCount; i++) {
+      const int s = awakeList[i], o = 6 * s;
+      if (type[s] == BG_STATIC) continue;
+      if (box[o] >= fat[o] && box[o + 1] >= fat[o + 1] && box[o + 2] >= fat[o + 2]
+          && box[o + 3] <= fat[o + 3] && box[o + 4] <= fat[o + 4] && box[o + 5] <= fat[o + 5]) continue;
+      fileOut(s);
+      fatten(s, AHEAD * dt);
+      fileIn(s);
+      mark(s);
+    }
+    std::vector<int32_t> found;
+    for (size_t i = 0; i < moved.size(); i++) {
+      const int a = moved[i];
+      isMoved[a] = 0;
+      const bool aStatic = type[a] == BG_STATIC;
+      found.clear();
+      seenMark++;
+      auto consider = [&](int b) {
+        if (b == a || seen[b] == seenMark) return;
+        seen[b] = seenMark;
+        if (aStatic && type[b] == BG_STATIC) return;
+        if (fatOverlap(a, b)) found.push_back(b);
+      };
+      if (large[a]) {
+        for (auto& kv : grid)
+          for (int b : kv.second) consider(b);
+      } else {
+        int64_t lo[3], hi[3];
+        cellRange(a, lo, hi);
+        for (int64_t x = lo[0]; x <= hi[0]; x++)
+          for (int64_t y = lo[1]; y <= hi[1]; y++)
+            for (int64_t z = lo[2]; z <= hi[2]; z++) {
+              auto it = grid.find(cellKey(x, y, z));
+              if (it == grid.end()) continue;
+              for (int b : it->second) consider(b);
+            }
+      }
+      for (int b : largeList) consider(b);
+      std::sort(found.begin(), found.end());
+      for (int b : found) pairs.found(a, b, type.data());
+    }
+    moved.clear();
+  }
+
+  int awakeCount = 0;
+
+  // load(): src/contact.js:1244-1276 (box, sphere, capsule).
+  void load(int slot, Shape& s) const {
+    const int s3 = slot * 3;
+    const double* d = &dims[s3];
+    if (shape[slot] == BG_BOX) {
+      s.kind = bearing::K_BOX;
+      s.half[0] = d[0] * 0.5; s.half[1] = d[1] * 0.5; s.half[2] = d[2] * 0.5;
+    } else if (shape[slot] == BG_SPHERE) {
+      s.kind = bearing::K_SPHERE;
+      s.half[0] = d[0];
+    } else {
+      s.kind = bearing::K_CAPSULE;
+      s.half[0] = d[0];
+      s.half[1] = (d[1] - 2 * d[0]) * 0.5;
+    }
+    s.center[0] = position[s3]; s.center[1] = position[s3 + 1]; s.center[2] = position[s3 + 2];
+    const double scale = type[slot] == BG_DYNAMIC ? gravityScale[slot] : 0;
+    s.weight[0] = gravity[0] * scale; s.weight[1] = gravity[1] * scale; s.weight[2] = gravity[2] * scale;
+    for (int k = 0; k < 9; k++) s.axes[k] = axes[9 * slot + k];
+  }
+
+  // basis(): src/contact.js:1283-1292.
+  void basis(int m) {
+    const double nx = c.normal[3 * m], ny = c.normal[3 * m + 1], nz = c.normal[3 * m + 2];
+    const double ax = std::fabs(nx), ay = std::fabs(ny), az = std::fabs(nz);
+    double tx, ty, tz;
+    if (ax <= ay && ax <= az) { tx = 0; ty = nz; tz = -ny; } else if (ay <= az) { tx = -nz; ty = 0; tz = nx; } else { tx = ny; ty = -nx; tz = 0; }
+    const double l = 1 / std::sqrt(tx * tx + ty * ty + tz * tz);
+    tx *= l; ty *= l; tz *= l;
+    c.t1[3 * m] = tx; c.t1[3 * m + 1] = ty; c.t1[3 * m + 2] = tz;
+    c.t2[3 * m] = ny * tz - nz * ty; c.t2[3 * m + 1] = nz * tx - nx * tz; c.t2[3 * m + 2] = nx * ty - ny * tx;
+  }
+
+  // emit(): src/contact.js:889-921 (whole bodies, sign 1, no parts, never shifted).
+  int emit(int p, int a, int b, const Manifold& mf, double tol) {
+    const int m = c.count++;
+    c.ensure(c.count);
+    c.a[m] = a; c.b[m] = b; c.pair[m] = p;
+    c.points[m] = static_cast<uint8_t>(mf.count);
+    for (int k = 0; k < 3; k++) c.normal[3 * m + k] = 1 * mf.normal[k];
+    c.friction[m] = std::sqrt(friction[a] * friction[b]);
+    c.restitution[m] = jmax(restitution[a], restitution[b]);
+    c.tolerance[m] = tol;
+    c.patch[m] = PIXEL * (type[a] != BG_DYNAMIC ? size[b] : type[b] != BG_DYNAMIC ? size[a] : jmin(size[a], size[b]));
+    c.rollImpulse1[m] = 0; c.rollImpulse2[m] = 0; c.spinImpulse[m] = 0;
+    c.tangentImpulse1[m] = 0; c.tangentImpulse2[m] = 0; c.drift1[m] = 0; c.drift2[m] = 0;
+    for (int k = 0; k < mf.count; k++) {
+      const int i = m * P + k;
+      c.pid[i] = mf.ids[k];
+      c.separation[i] = mf.separations[k];
+      for (int q = 0; q < 3; q++) c.point[3 * i + q] = mf.points[3 * k + q];
+      for (int q = 0; q < 3; q++) c.shift[3 * i + q] = 0;
+      c.normalImpulse[i] = 0;
+    }
+    basis(m);
+    return m;
+  }
+
+  // carry(): src/contact.js:999-1036, from the pair list.
+  void carry(int p, int m) {
+    const int remembered = pairs.points[p];
+    if (remembered == 0) return;
+    const int m3 = 3 * m;
+    const double t1x = c.t1[m3], t1y = c.t1[m3 + 1], t1z = c.t1[m3 + 2];
+    const double t2x = c.t2[m3], t2y = c.t2[m3 + 1], t2z = c.t2[m3 + 2];
+    const int count = c.points[m], p3 = 3 * p;
+    const double lx = pairs.twist[p3], ly = pairs.twist[p3 + 1], lz = pairs.twist[p3 + 2];
+    if (count <= 2) {
+      c.rollImpulse1[m] = lx * t1x + ly * t1y + lz * t1z;
+      c.rollImpulse2[m] = lx * t2x + ly * t2y + lz * t2z;
+    }
+    c.spinImpulse[m] = lx * c.normal[m3] + ly * c.normal[m3 + 1] + lz * c.normal[m3 + 2];
+    const double fx = pairs.friction[p3], fy = pairs.friction[p3 + 1], fz = pairs.friction[p3 + 2];
+    c.tangentImpulse1[m] = fx * t1x + fy * t1y + fz * t1z;
+    c.tangentImpulse2[m] = fx * t2x + fy * t2y + fz * t2z;
+    bool same = false;
+    for (int k = 0; k < count; k++) {
+      const int i = m * P + k;
+      const uint32_t id = c.pid[i];
+      for (int j = 0; j < remembered; j++) {
+        const int o = p * P + j;
+        if (pairs.pid[o] != id) continue;
+        c.normalImpulse[i] = pairs.normalImpulse[o];
+        same = true;
+        break;
+      }
+    }
+    if (same) {
+      const double sx = pairs.slip[p3], sy = pairs.slip[p3 + 1], sz = pairs.slip[p3 + 2];
+      c.drift1[m] = sx * t1x + sy * t1y + sz * t1z;
+      c.drift2[m] = sx * t2x + sy * t2y + sz * t2z;
+    }
+  }
+
+  // narrow(): src/contact.js:296-327 with find() 334-368 (no reuse cache, no time of impact).
+  void narrow() {
+    Shape sa, sb;
+    Manifold mf;
+    for (int p = 0; p < pairs.active;) {
+      const int a = pairs.a[p], b = pairs.b[p];
+      if (!fatOverlap(a, b)) {
+        pairs.remove(p);
+        continue;
+      }
+      const double tol = jmin(size[a], size[b]) * PIXEL;
+      const int a6 = a * 6, b6 = b * 6;
+      bool met = true;
+      if (box[a6] > box[b6 + 3] || box[b6] > box[a6 + 3] || box[a6 + 1] > box[b6 + 4]
+          || box[b6 + 1] > box[a6 + 4] || box[a6 + 2] > box[b6 + 5] || box[b6 + 2] > box[a6 + 5]) {
+        pairs.forget(p);
+        met = false;
+      } else {
+        const double margin = motion[a] + motion[b] + tol;
+        load(a, sa);
+        load(b, sb);
+        if (bearing::collide(sa, sb, margin, tol, mf) == 0) {
+          pairs.forget(p);
+          met = false;
+        }
+      }
+      if (met) {
+        const int m = emit(p, a, b, mf, tol);
+        carry(p, m);
+      }
+      p++;
+    }
+  }
+
+  // colour(): src/graph.js:105-170, and arrange() 178-214.
+  void colourRows() {
+    const int cnt = c.count;
+    std::vector<int32_t> used(static_cast<size_t>(n), 0);
+    const bool anyFrozen = std::any_of(frozen.begin(), frozen.begin() + n, [](uint8_t f) { return f != 0; });
+    for (int m = 0; m < cnt; m++) {
+      const int a = c.a[m], b = c.b[m];
+      bool da = type[a] == BG_DYNAMIC, db = type[b] == BG_DYNAMIC;
+      if (anyFrozen) {
+        const bool fa = frozen[a] != 0, fb = frozen[b] != 0;
+        if ((fa || type[a] == BG_STATIC) && (fb || type[b] == BG_STATIC)) {
+          c.colour[m] = RESTING;
+          continue;
+        }
+        if (fa) da = false;
+        if (fb) db = false;
+      }
+      const int32_t held = (da ? used[a] : 0) | (db ? used[b] : 0);
+      if (held == -1) {
+        c.colour[m] = OVERFLOW_;
+        continue;
+      }
+      const uint32_t uheld = static_cast<uint32_t>(held);
+      const uint32_t bit = ~uheld & (uheld + 1u);
+      c.colour[m] = 31 - __builtin_clz(bit);
+      if (da) used[a] |= static_cast<int32_t>(bit);
+      if (db) used[b] |= static_cast<int32_t>(bit);
+    }
+    c.digits.assign(DIGITS + 1, 0);
+    std::vector<int32_t>& count = c.digits;
+    const bool high = n > DIGITS;
+    int32_t* from = high ? c.order.data() : c.row.data();
+    for (int m = 0; m < cnt; m++) count[(c.b[m] & (DIGITS - 1)) + 1]++;
+    for (int k = 0; k < DIGITS; k++) count[k + 1] += count[k];
+    for (int m = 0; m < cnt; m++) from[count[c.b[m] & (DIGITS - 1)]++] = m;
+    if (high) {
+      std::fill(count.begin(), count.end(), 0);
+      for (int i = 0; i < cnt; i++) count[(static_cast<uint32_t>(c.b[c.order[i]]) >> DIGIT) + 1]++;
+      for (int k = 0; k < DIGITS; k++) count[k + 1] += count[k];
+      for (int i = 0; i < cnt; i++) {
+        const int m = c.order[i];
+        c.row[count[static_cast<uint32_t>(c.b[m]) >> DIGIT]++] = m;
+      }
+      from = c.row.data();
+    }
+    int* starts = c.starts;
+    std::fill(starts, starts + COLOURS + 3, 0);
+    for (int m = 0; m < cnt; m++) starts[c.colour[m] + 1]++;
+    for (int k = 0; k <= RESTING; k++) starts[k + 1] += starts[k];
+    for (int i = 0; i < cnt; i++) {
+      const int m = from[i];
+      c.order[starts[c.colour[m]]++] = m;
+    }
+    for (int k = RESTING; k > 0; k--) starts[k] = starts[k - 1];
+    starts[0] = 0;
+    c.solved = starts[RESTING];
+    arrange(cnt);
+  }
+  template <class T>
+  void moveColumn(std::vector<T>& column, int per, int cnt) {
+    std::vector<T> tmp(column.begin(), column.begin() + static_cast<size_t>(cnt) * per);
+    for (int o = 0; o < cnt; o++) {
+      const int f = c.order[o] * per, t = o * per;
+      for (int i = 0; i < per; i++) column[t + i] = tmp[f + i];
+    }
+  }
+  void arrange(int cnt) {
+    moveColumn(c.normal, 3, cnt); moveColumn(c.t1, 3, cnt); moveColumn(c.t2, 3, cnt);
+    moveColumn(c.friction, 1, cnt); moveColumn(c.restitution, 1, cnt); moveColumn(c.tolerance, 1, cnt);
+    moveColumn(c.patch, 1, cnt); moveColumn(c.rollImpulse1, 1, cnt); moveColumn(c.rollImpulse2, 1, cnt);
+    moveColumn(c.spinImpulse, 1, cnt); moveColumn(c.tangentImpulse1, 1, cnt); moveColumn(c.tangentImpulse2, 1, cnt);
+    moveColumn(c.drift1, 1, cnt); moveColumn(c.drift2, 1, cnt); moveColumn(c.separation, P, cnt);
+    moveColumn(c.normalImpulse, P, cnt); moveColumn(c.point, 3 * P, cnt); moveColumn(c.shift, 3 * P, cnt);
+    moveColumn(c.a, 1, cnt); moveColumn(c.b, 1, cnt); moveColumn(c.pair, 1, cnt); moveColumn(c.colour, 1, cnt);
+    moveColumn(c.pid, P, cnt); moveColumn(c.points, 1, cnt);
+    for (int o = 0; o < cnt; o++) c.row[c.order[o]] = o;
+  }
+
+  // rest(): src/contact.js:1318-1329.
+  void rest() {
+    for (int m = c.solved; m < c.count; m++) {
+      double least = INF;
+      for (int k = 0; k < c.points[m]; k++) {
+        const int i = m * P + k;
+        if (c.separation[i] < least) least = c.separation[i];
+        c.maxNormalImpulse[i] = c.normalImpulse[i];
+        c.relativeVelocity[i] = 0;
+      }
+      c.gap[m] = least;
+    }
+  }
+
+  // keep(): src/contact.js:1091-1115, into the pair list.
+  void keep(int p, int m) {
+    const int count = c.points[m], m3 = 3 * m, p3 = 3 * p;
+    pairs.points[p] = static_cast<uint8_t>(count);
+    const double t1x = c.t1[m3], t1y = c.t1[m3 + 1], t1z = c.t1[m3 + 2];
+    const double t2x = c.t2[m3], t2y = c.t2[m3 + 1], t2z = c.t2[m3 + 2];
+    const double r1 = c.rollImpulse1[m], r2 = c.rollImpulse2[m], sp = c.spinImpulse[m];
+    pairs.twist[p3] = t1x * r1 + t2x * r2 + c.normal[m3] * sp;
+    pairs.twist[p3 + 1] = t1y * r1 + t2y * r2 + c.normal[m3 + 1] * sp;
+    pairs.twist[p3 + 2] = t1z * r1 + t2z * r2 + c.normal[m3 + 2] * sp;
+    const double l1 = c.tangentImpulse1[m], l2 = c.tangentImpulse2[m];
+    pairs.friction[p3] = t1x * l1 + t2x * l2;
+    pairs.friction[p3 + 1] = t1y * l1 + t2y * l2;
+    pairs.friction[p3 + 2] = t1z * l1 + t2z * l2;
+    const double d1 = c.drift1[m], d2 = c.drift2[m];
+    pairs.slip[p3] = t1x * d1 + t2x * d2;
+    pairs.slip[p3 + 1] = t1y * d1 + t2y * d2;
+    pairs.slip[p3 + 2] = t1z * d1 + t2z * d2;
+    for (int k = 0; k < count; k++) {
+      pairs.pid[p * P + k] = c.pid[m * P + k];
+      pairs.normalImpulse[p * P + k] = c.normalImpulse[m * P + k];
+    }
+  }
+
+  void fillBodies(bg_bodies* B) {
+    B->capacity = n;
+    B->awake_count = awakeCount;
+    B->awake_list = awakeList.data();
+    B->awake = awake.data();
+    B->position = position.data(); B->rotation = rotation.data(); B->velocity = velocity.data();
+    B->angular = angular.data(); B->tumbled = tumbled.data(); B->ceiling = ceiling.data();
+    B->start = start.data(); B->start_q = startQ.data(); B->inv_i = invI.data();
+    B->inv_mass = invMass.data(); B->inertia = inertia.data(); B->inv_inertia = invInertia.data();
+    B->dims = dims.data(); B->damping = damping.data(); B->angular_damping = angularDamping.data();
+    B->gravity_scale = gravityScale.data(); B->type = type.data(); B->shape = shape.data();
+    B->frozen = frozen.data(); B->framed = framed.data(); B->lock = lock.data(); B->joint_head = jointHead.data();
+  }
+  void fillRows(bg_rows* R) {
+    c.ensure(1);
+    R->count = c.count;
+    R->solved = c.solved;
+    for (int k = 0; k < COLOURS + 3; k++) R->starts[k] = c.starts[k];
+    R->row = c.row.data(); R->a = c.a.data(); R->b = c.b.data(); R->points = c.points.data();
+    R->normal = c.normal.data(); R->t1 = c.t1.data(); R->t2 = c.t2.data();
+    R->friction = c.friction.data(); R->restitution = c.restitution.data(); R->tolerance = c.tolerance.data();
+    R->patch = c.patch.data(); R->separation = c.separation.data(); R->point = c.point.data(); R->shift = c.shift.data();
+    R->normal_impulse = c.normalImpulse.data(); R->tangent_impulse1 = c.tangentImpulse1.data();
+    R->tangent_impulse2 = c.tangentImpulse2.data(); R->roll_impulse1 = c.rollImpulse1.data();
+    R->roll_impulse2 = c.rollImpulse2.data(); R->spin_impulse = c.spinImpulse.data();
+    R->drift1 = c.drift1.data(); R->drift2 = c.drift2.data(); R->gap = c.gap.data();
+    R->max_normal_impulse = c.maxNormalImpulse.data(); R->relative_velocity = c.relativeVelocity.data();
+    R->sliding = c.sliding.data(); R->anchor_a = c.anchorA.data(); R->anchor_b = c.anchorB.data();
+  }
+};
+
+extern "C" {
+
+bw_world* bw_create(const bw_options* options) {
+  bw_world* w = new bw_world();
+  if (options != nullptr) {
+    for (int k = 0; k < 3; k++) w->gravity[k] = options->gravity[k];
+    w->substeps = options->substeps > 0 ? options->substeps : 8;
+  }
+  w->c.alloc(0);
+  return w;
+}
+
+void bw_destroy(bw_world* world) { delete world; }
+
+const char* bw_last_error(const bw_world* world) { return world == nullptr ? "no world" : world->error.c_str(); }
+
+int32_t bw_add_body(bw_world* w, const bw_body* spec) {
+  if (w == nullptr || spec == nullptr) return BG_EINVAL;
+  if (spec->shape < BG_BOX || spec->shape > BG_CAPSULE) {
+    w->error = "addBody: only box, sphere and capsule shapes are on this path";
+    return BG_EUNSUPPORTED;
+  }
+  if (spec->type != BG_DYNAMIC && spec->type != BG_STATIC && spec->type != KINEMATIC) {
+    w->error = "addBody: type must be dynamic, static or kinematic";
+    return BG_EINVAL;
+  }
+  // quat(): src/core/check.js:106-117.
+  const double* r = spec->rotation;
+  const double mq = jmax(jmax(jmax(std::fabs(r[0]), std::fabs(r[1])), std::fabs(r[2])), std::fabs(r[3]));
+  if (!(mq > 0) || !std::isfinite(mq)) {
+    w->error = "addBody: rotation must be 4 finite numbers, not all zero";
+    return BG_EINVAL;
+  }
+  const int s = w->n++;
+  w->resize(w->n);
+  const int s3 = 3 * s, s4 = 4 * s;
+  w->type[s] = static_cast<uint8_t>(spec->type);
+  w->shape[s] = static_cast<uint8_t>(spec->shape);
+  double* d = &w->dims[s3];
+  const double rad = spec->radius;
+  if (spec->shape == BG_BOX) { d[0] = spec->size[0]; d[1] = spec->size[1]; d[2] = spec->size[2]; }
+  else { d[0] = rad; d[1] = spec->shape == BG_CAPSULE ? spec->height : 0; d[2] = 0; }
+  // volume(): src/shapes.js:14-21.
+  double v;
+  if (spec->shape == BG_BOX) v = spec->size[0] * spec->size[1] * spec->size[2];
+  else {
+    const double ball = (4.0 / 3.0) * PI * rad * rad * rad;
+    v = spec->shape == BG_SPHERE ? ball : PI * rad * rad * (spec->height - 2 * rad) + ball;
+  }
+  w->mass[s] = spec->mass > 0 ? spec->mass : spec->density * v;
+  const double mass = w->mass[s];
+  // inertia(): src/shapes.js:37-56.
+  double* I = &w->inertia[s3];
+  if (spec->shape == BG_BOX) {
+    const double wd = spec->size[0], h = spec->size[1], dd = spec->size[2];
+    I[0] = mass * (h * h + dd * dd) / 12;
+    I[1] = mass * (wd * wd + dd * dd) / 12;
+    I[2] = mass * (wd * wd + h * h) / 12;
+  } else if (spec->shape == BG_SPHERE) {
+    I[0] = I[1] = I[2] = 0.4 * mass * rad * rad;
+  } else {
+    const double L = spec->height - 2 * rad;
+    const double cylinder = PI * rad * rad * L, ball = (4.0 / 3.0) * PI * rad * rad * rad;
+    const double mc = mass * cylinder / (cylinder + ball), ms = mass * ball / (cylinder + ball);
+    I[1] = mc * rad * rad / 2 + ms * 0.4 * rad * rad;
+    I[0] = I[2] = mc * (L * L / 12 + rad * rad / 4) + ms * (0.4 * rad * rad + L * L / 4 + 3 * L * rad / 8);
+  }
+  for (int k = 0; k < 3; k++) w->invInertia[s3 + k] = I[k] > 0 ? 1 / I[k] : 0;
+  w->invMass[s] = spec->type == BG_DYNAMIC ? 1 / mass : 0;
+  if (spec->shape == BG_BOX) {
+    w->size[s] = jmin(jmin(spec->size[0], spec->size[1]), spec->size[2]);
+    w->reach[s] = 0.5 * std::sqrt(spec->size[0] * spec->size[0] + spec->size[1] * spec->size[1] + spec->size[2] * spec->size[2]);
+  } else {
+    w->size[s] = 2 * rad;
+    w->reach[s] = spec->shape == BG_CAPSULE ? spec->height * 0.5 : rad;
+  }
+  w->friction[s] = spec->friction;
+  w->restitution[s] = spec->restitution;
+  w->damping[s] = spec->damping;
+  w->angularDamping[s] = spec->angular_damping;
+  w->gravityScale[s] = spec->gravity_scale;
+  const double x = r[0] / mq, y = r[1] / mq, z = r[2] / mq, ww = r[3] / mq;
+  const double sc = 1 / std::sqrt(x * x + y * y + z * z + ww * ww);
+  for (int k = 0; k < 3; k++) w->position[s3 + k] = spec->position[k];
+  w->rotation[s4] = x * sc; w->rotation[s4 + 1] = y * sc; w->rotation[s4 + 2] = z * sc; w->rotation[s4 + 3] = ww * sc;
+  for (int k = 0; k < 3; k++) {
+    w->velocity[s3 + k] = spec->velocity[k];
+    w->angular[s3 + k] = spec->angular[k];
+    w->tumbled[s3 + k] = std::numeric_limits<double>::quiet_NaN();
+  }
+  w->ceiling[s] = 0;
+  // Where the solver measures a step's movement from, for a body not moving in it: _place,
+  // src/world.js:2294-2296.
+  for (int k = 0; k < 3; k++) w->start[s3 + k] = w->position[s3 + k];
+  // Transform as placed.
+  for (int k = 0; k < 3; k++) w->transforms[7 * s + k] = static_cast<float>(w->position[s3 + k]);
+  for (int k = 0; k < 4; k++) w->transforms[7 * s + 3 + k] = static_cast<float>(w->rotation[s4 + k]);
+  // Bounds, the broadphase, and the awake list (src/world.js:563-578).
+  w->boundsOf(s, 0, 0);
+  w->fatten(s, 0);
+  w->filed[s] = 1;
+  if (w->cell != 0) w->fileIn(s);
+  w->mark(s);
+  if (spec->type != BG_STATIC) {
+    w->awakeList[w->awakeCount++] = s;
+    w->awake[s] = 1;
+  }
+  return s;
+}
+
+int32_t bw_set_solver(bw_world* w, bw_solver solver, void* user) {
+  if (w == nullptr) return BG_EINVAL;
+  w->solver = solver;
+  w->solverUser = user;
+  return BG_OK;
+}
+
+int32_t bw_begin_step(bw_world* w, double dt) {
+  if (w == nullptr) return BG_EINVAL;
+  if (!(dt > 0) || !std::isfinite(dt)) {
+    w->error = "step: dt must be a positive number of seconds";
+    return BG_EINVAL;
+  }
+  w->stepCount++;
+  w->stepDt = dt;
+  const double* g = w->gravity;
+  const double gl = std::sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+  for (int i = 0; i < w->awakeCount; i++) w->boundsOf(w->awakeList[i], dt, gl);
+  w->broadphase(dt);
+  w->c.count = 0;
+  w->narrow();
+  if (w->c.count > 0) {
+    w->colourRows();
+    if (w->c.solved < w->c.count) w->rest();
+  } else {
+    std::fill(w->c.starts, w->c.starts + COLOURS + 3, 0);
+    w->c.solved = 0;
+  }
+  w->begun = true;
+  return BG_OK;
+}
+
+int32_t bw_end_step(bw_world* w) {
+  if (w == nullptr || !w->begun) return BG_EINVAL;
+  w->begun = false;
+  Contacts& c = w->c;
+  // store(): src/contact.js:1067-1088 (slipped() ran in the solve stage).
+  for (int f = 0; f < c.count; f++) {
+    const int m = c.row[f];
+    if (m >= c.solved) continue;
+    w->keep(c.pair[m], m);
+  }
+  // touched(): src/contact.js:2178-2213, the touching flags only.
+  for (int f = 0; f < c.count; f++) {
+    const int m = c.row[f];
+    bool meets = c.gap[m] <= c.tolerance[m];
+    for (int k = 0; k < c.points[m] && !meets; k++) meets = c.maxNormalImpulse[m * P + k] > 0;
+    w->pairs.touching[c.pair[m]] = meets ? 1 : 0;
+  }
+  // transforms: src/world.js:1040-1057.
+  for (int i = 0; i < w->awakeCount; i++) {
+    const int s = w->awakeList[i], t7 = 7 * s;
+    if (w->frozen[s] == 1) continue;
+    for (int k = 0; k < 3; k++) w->transforms[t7 + k] = static_cast<float>(w->position[3 * s + k]);
+    for (int k = 0; k < 4; k++) w->transforms[t7 + 3 + k] = static_cast<float>(w->rotation[4 * s + k]);
+  }
+  // stats
+  bw_stats& st = w->stats;
+  st.bodies = w->n;
+  st.awake = w->awakeCount;
+  st.pairs = w->pairs.count;
+  st.rows = c.count;
+  st.solved = c.solved;
+  int pts = 0;
+  for (int m = 0; m < c.solved; m++) pts += c.points[m];
+  st.points = pts;
+  int colours = 0;
+  for (int k = 0; k < COLOURS; k++) if (c.starts[k + 1] > c.starts[k]) colours++;
+  st.colours = colours;
+  st.overflow = c.count > 0 ? c.starts[OVERFLOW_ + 1] - c.starts[OVERFLOW_] : 0;
+  st.step = w->stepCount;
+  w->stepDt = 0;
+  return BG_OK;
+}
+
+int32_t bw_bodies_view(bw_world* w, bg_bodies* out) {
+  if (w == nullptr || out == nullptr) return BG_EINVAL;
+  w->fillBodies(out);
+  return BG_OK;
+}
+
+int32_t bw_rows_view(bw_world* w, bg_rows* out) {
+  if (w == nullptr || out == nullptr) return BG_EINVAL;
+  w->fillRows(out);
+  return BG_OK;
+}
+
+int32_t bw_step_params(const bw_world* w, bg_step* out) {
+  if (w == nullptr || out == nullptr) return BG_EINVAL;
+  out->dt = w->stepDt;
+  out->substeps = w->substeps;
+  for (int k = 0; k < 3; k++) out->gravity[k] = w->gravity[k];
+  return BG_OK;
+}
+
+int32_t bw_step(bw_world* w, double dt) {
+  if (w == nullptr) return BG_EINVAL;
+  if (w->solver == nullptr) {
+    w->error = "step: no solve stage set (bw_set_solver)";
+    return BG_EUNSUPPORTED;
+  }
+  int32_t rc = bw_begin_step(w, dt);
+  if (rc != BG_OK) return rc;
+  bg_bodies B;
+  bg_rows R;
+  bg_step S;
+  w->fillBodies(&B);
+  w->fillRows(&R);
+  bw_step_params(w, &S);
+  rc = w->solver(w->solverUser, &B, &R, &S);
+  if (rc != BG_OK) {
+    w->begun = false;
+    w->error = "step: the solve stage failed";
+    return rc;
+  }
+  return bw_end_step(w);
+}
+
+const float* bw_transforms(const bw_world* w) { return w == nullptr ? nullptr : w->transforms.data(); }
+
+int32_t bw_stats_get(const bw_world* w, bw_stats* out) {
+  if (w == nullptr || out == nullptr) return BG_EINVAL;
+  *out = w->stats;
+  return BG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,217 @@
+"""World: the reference's World API (src/world.js, src/bearing.d.ts:512-575) for boxes, spheres
+and capsules, with the contact solve stage on a B200.
+
+The host side of each step (bounds, pair finding, narrowphase, colouring, warm-start memory,
+store, transforms) runs in ``libbearing_host.so``; the solve stage (src/world.js:962-1032) runs
+in ``libbearing_gpu.so`` through its C ABI.  ``world.step(dt)``, ``world.transforms`` and
+``world.workers`` mean what they mean in the reference.  There is no CPU fallback for the solve
+stage: a World made with the GPU solver fails loudly if the CUDA library cannot run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+from . import _ffi
+
+SHAPES = {"box": _ffi.BG_BOX, "sphere": _ffi.BG_SPHERE, "capsule": _ffi.BG_CAPSULE}
+TYPES = {"dynamic": _ffi.BG_DYNAMIC, "static": _ffi.BG_STATIC, "kinematic": _ffi.BG_KINEMATIC}
+
+# Defaults: src/world.js:205-221.
+DEFAULTS = dict(
+    type="dynamic", shape="box", size=(1.0, 1.0, 1.0), radius=0.5, height=2.0, density=1000.0, mass=0.0,
+    friction=0.5, restitution=0.0, damping=0.0, angularDamping=0.0, gravityScale=1.0,
+    position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0, 1.0), velocity=(0.0, 0.0, 0.0),
+    angularVelocity=(0.0, 0.0, 0.0),
+)
+BODY_OPTIONS = set(DEFAULTS)
+WORLD_OPTIONS = {"gravity", "substeps", "sleeping", "workers"}
+
+
+class BearingError(RuntimeError):
+    """A step or a setter failed; the message is the library's."""
+
+
+class GpuSolver:
+    """The solve stage on one CUDA device, through bg_solve_step (bearing_gpu.h)."""
+
+    def __init__(self, device: int = 0, flags: int = 0):
+        self.lib = _ffi.gpu()
+        self.ctx = self.lib.bg_create(device, flags)
+        if not self.ctx:
+            raise BearingError(f"bg_create({device}) failed: no usable CUDA device")
+        self.fn = C.cast(self.lib.bg_solve_step, C.c_void_p).value
+        # bw_solver takes (user, bodies, rows, step); bg_solve_step takes (ctx, bodies, rows, step).
+        self.user = self.ctx
+
+    def error(self) -> str:
+        return self.lib.bg_last_error(self.ctx).decode()
+
+    def close(self):
+        if self.ctx:
+            self.lib.bg_destroy(self.ctx)
+            self.ctx = None
+
+
+def _vec(v, n, name):
+    v = tuple(float(x) for x in v)
+    if len(v) != n or not all(math.isfinite(x) for x in v):
+        raise BearingError(f"addBody: {name} must be {n} finite numbers, got {v!r}")
+    return v
+
+
+class World:
+    """A world of bodies, stepped with the solve stage on the GPU (or another bw_solver)."""
+
+    def __init__(self, options: dict | None = None, solver=None):
+        o = dict(options or {})
+        unknown = set(o) - WORLD_OPTIONS
+        if unknown:
+            raise BearingError(f"World: unknown option {sorted(unknown)[0]!r}")
+        g = _vec(o.get("gravity", (0.0, -9.81, 0.0)), 3, "gravity")
+        substeps = int(o.get("substeps", 8))
+        if substeps < 1:
+            raise BearingError("World: substeps must be a whole number from 1")
+        if o.get("sleeping", False):
+            raise BearingError("World: sleeping islands are not on this path; pass sleeping: false")
+        self._workers = o.get("workers", "auto")
+        self._lib = _ffi.host()
+        opts = _ffi.Options((C.c_double * 3)(*g), substeps)
+        self._w = self._lib.bw_create(C.byref(opts))
+        self._count = 0
+        self._solver = None
+        self._solver_keep = None
+        if solver is None:
+            solver = GpuSolver()
+        self.set_solver(solver)
+
+    # -- the solve stage ---------------------------------------------------------------------
+    def set_solver(self, solver):
+        """solver: a GpuSolver, or (function address, user pointer) of a bw_solver."""
+        if isinstance(solver, GpuSolver):
+            fn, user = solver.fn, solver.user
+        else:
+            fn, user = solver
+        self._solver = solver
+        rc = self._lib.bw_set_solver(self._w, C.c_void_p(fn), C.c_void_p(user))
+        if rc != 0:
+            raise BearingError(self._error())
+
+    def _error(self) -> str:
+        return self._lib.bw_last_error(self._w).decode()
+
+    # -- bodies ------------------------------------------------------------------------------
+    def addBody(self, spec: dict | None = None) -> int:
+        """Adds a box, sphere or capsule (src/world.js:563-578); returns its slot."""
+        s = dict(DEFAULTS)
+        spec = dict(spec or {})
+        unknown = set(spec) - BODY_OPTIONS
+        if unknown:
+            raise BearingError(f"addBody: unknown option {sorted(unknown)[0]!r}")
+        s.update(spec)
+        if s["shape"] not in SHAPES:
+            raise BearingError(f"addBody: shape must be 'box', 'sphere' or 'capsule', got {s['shape']!r}")
+        if s["type"] not in TYPES:
+            raise BearingError(f"addBody: type must be 'dynamic', 'static' or 'kinematic', got {s['type']!r}")
+        b = _ffi.BodySpec()
+        b.type = TYPES[s["type"]]
+        b.shape = SHAPES[s["shape"]]
+        b.size = (C.c_double * 3)(*_vec(s["size"], 3, "size"))
+        b.radius = float(s["radius"])
+        b.height = float(s["height"])
+        b.density = float(s["density"])
+        b.mass = float(s["mass"])
+        b.friction = float(s["friction"])
+        b.restitution = float(s["restitution"])
+        b.damping = float(s["damping"])
+        b.angular_damping = float(s["angularDamping"])
+        b.gravity_scale = float(s["gravityScale"])
+        b.position = (C.c_double * 3)(*_vec(s["position"], 3, "position"))
+        b.rotation = (C.c_double * 4)(*_vec(s["rotation"], 4, "rotation"))
+        b.velocity = (C.c_double * 3)(*_vec(s["velocity"], 3, "velocity"))
+        b.angular = (C.c_double * 3)(*_vec(s["angularVelocity"], 3, "angularVelocity"))
+        slot = self._lib.bw_add_body(self._w, C.byref(b))
+        if slot < 0:
+            raise BearingError(self._error())
+        self._count = slot + 1
+        return slot
+
+    # -- stepping ----------------------------------------------------------------------------
+    def step(self, dt: float):
+        """One step of dt seconds (src/world.js:880-1072)."""
+        if not isinstance(dt, (int, float)) or not (dt > 0) or dt == math.inf:
+            raise BearingError(f"step: dt must be a positive number of seconds, got {dt!r}")
+        rc = self._lib.bw_step(self._w, float(dt))
+        if rc != 0:
+            extra = ""
+            if isinstance(self._solver, GpuSolver):
+                extra = f" ({self._solver.error()})"
+            raise BearingError(f"step failed ({rc}): {self._error()}{extra}")
+
+    def begin_step(self, dt: float):
+        """The step up to the solve stage; the views then hold the solve stage's input."""
+        rc = self._lib.bw_begin_step(self._w, float(dt))
+        if rc != 0:
+            raise BearingError(self._error())
+
+    def end_step(self):
+        rc = self._lib.bw_end_step(self._w)
+        if rc != 0:
+            raise BearingError(self._error())
+
+    def views(self):
+        """(bg_bodies, bg_rows, bg_step) over the world's own columns."""
+        B, R, S = _ffi.Bodies(), _ffi.Rows(), _ffi.Step()
+        self._lib.bw_bodies_view(self._w, C.byref(B))
+        self._lib.bw_rows_view(self._w, C.byref(R))
+        self._lib.bw_step_params(self._w, C.byref(S))
+        return B, R, S
+
+    # -- reading -----------------------------------------------------------------------------
+    @property
+    def transforms(self) -> np.ndarray:
+        """World.transforms: 7 float32 per slot, position then rotation x y z w (a copy)."""
+        ptr = self._lib.bw_transforms(self._w)
+        return np.ctypeslib.as_array(ptr, shape=(7 * self._count,)).copy()
+
+    @property
+    def workers(self):
+        """World.workers (src/world.js:501-524).  The solve stage runs on the GPU whatever it
+        is; as in the reference, results do not depend on it."""
+        return self._workers
+
+    @workers.setter
+    def workers(self, value):
+        if value != "auto" and (not isinstance(value, int) or value < 0):
+            raise BearingError(f"workers must be 'auto' or a whole number from 0, got {value!r}")
+        self._workers = value
+
+    def stats(self) -> dict:
+        st = _ffi.Stats()
+        self._lib.bw_stats_get(self._w, C.byref(st))
+        return {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
+
+    def state(self) -> dict:
+        """FP64 body state by slot (position, rotation, velocity, angular), copies."""
+        B, _, _ = self.views()
+        n = self._count
+        def arr(p, k):
+            return np.ctypeslib.as_array(p, shape=(k * n,)).copy() if n else np.zeros(0)
+        return {"position": arr(B.position, 3), "rotation": arr(B.rotation, 4),
+                "velocity": arr(B.velocity, 3), "angular": arr(B.angular, 3)}
+
+    def destroy(self):
+        if self._w:
+            self._lib.bw_destroy(self._w)
+            self._w = None
+        if isinstance(self._solver, GpuSolver):
+            self._solver.close()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

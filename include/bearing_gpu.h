@@ -1,0 +1,215 @@
+/*
+ * bearing_gpu.h - the C ABI of the B200 contact-solve library (libbearing_gpu.so).
+ *
+ * It takes the place of Bearing's worker threads (src/core/jobs.js, src/worker.js) for one
+ * block of World.step: src/world.js:962-1032, the "solve stage".  In order, each step:
+ *
+ *   inertias        src/contact.js:1302-1310, 1493-1549   world inverse inertia per awake body
+ *   start snapshot  src/world.js:964-974                  start / startQ of every awake body
+ *   prepare         src/contact.js:1346-1445               per-row levers, masses, anchors, block K
+ *   makeSoft        src/contact.js:1591-1597               soft-contact constants for h = dt/substeps
+ *   substeps x N    src/world.js:1011-1024
+ *     accelerate    src/world.js:1495-1530
+ *     warm start    src/contact.js:1604-1663               colour by colour
+ *     solve (bias)  src/contact.js:1782-2090               colour by colour, overflow in row order
+ *     move          src/world.js:1533-1563, 2739-2834      incl. tumble() / untwist()
+ *     relax         src/contact.js:1782-2090 (bias=false)
+ *   restitution     src/contact.js:2229-2251               in found order (rows.row)
+ *   slipped         src/contact.js:1122-1182               the drift half of store(); keep() stays on host
+ *
+ * The caller (the host side of World.step: broadphase, narrowphase, colouring in
+ * src/graph.js:105-185) hands over the step's manifolds already laid out colour by colour,
+ * with the reference's own column meanings (src/contact.js:184-248, src/graph.js:78-83).
+ * Every array is plain FP64 / int32 / uint8 host memory owned by the caller.  The library owns
+ * device memory, one CUDA stream and its kernels per context; two contexts never share state.
+ *
+ * Arithmetic is IEEE FP64 with no contraction (built with -fmad=false), in the reference's
+ * operation order, so results are bit-identical to the reference's CPU solve over the same rows.
+ *
+ * Return codes: BG_OK (0) or a negative BG_E* code; bg_last_error() says why.  A failed
+ * validation changes no state.  A device wait that runs past its budget returns BG_ETIMEOUT,
+ * which the caller treats as src/core/jobs.js:384-391 treats a lost step: fall back to the CPU.
+ */
+#ifndef BEARING_GPU_H
+#define BEARING_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Points per manifold: src/contact.js:128 (P). */
+#define BG_POINTS 4
+/* Colours and the runs after them: src/graph.js:67-71 (COLOURS, OVERFLOW, RESTING). */
+#define BG_COLOURS 32
+#define BG_OVERFLOW 32
+#define BG_RESTING 33
+/* Length of rows.starts: src/contact.js:161 (COLOURS + 3). */
+#define BG_STARTS 35
+
+#define BG_OK 0
+#define BG_EINVAL (-1)
+#define BG_ECUDA (-2)
+#define BG_ETIMEOUT (-3)
+#define BG_ENOMEM (-4)
+#define BG_EUNSUPPORTED (-5)
+#define BG_EFAULT (-6)
+
+/* bg_create flags */
+#define BG_FLAG_NONE 0u
+/* Register the caller's host arrays as pinned on first use (cudaHostRegister) and keep them so. */
+#define BG_FLAG_PIN_HOST 1u
+
+/* World body type codes: src/world.js TYPES (dynamic 0, static 1, kinematic 2, character 3). */
+#define BG_DYNAMIC 0
+#define BG_STATIC 1
+/* World shape codes: src/world.js:63 (box 0, sphere 1, capsule 2, hull 3, compound 4, mesh 5). */
+#define BG_BOX 0
+#define BG_SPHERE 1
+#define BG_CAPSULE 2
+
+typedef struct bg_ctx bg_ctx;
+
+/*
+ * Per-body columns, indexed by slot as World keeps them (src/world.js:228-311).  `capacity`
+ * slots; vectors are packed (3 per slot, quaternions 4 per slot as x y z w).
+ */
+typedef struct bg_bodies {
+  int32_t capacity;            /* slots in every per-body array */
+  int32_t awake_count;         /* World._awakeCount */
+  const int32_t* awake_list;   /* World._awakeList: the awake slots */
+  const uint8_t* awake;        /* World._awake: 1 while awake (slipped() reads it) */
+  /* read and written */
+  double* position;            /* 3 per slot */
+  double* rotation;            /* 4 per slot */
+  double* velocity;            /* 3 per slot */
+  double* angular;             /* 3 per slot */
+  double* tumbled;             /* 3 per slot: world.js _tumbled */
+  double* ceiling;             /* 1 per slot: world.js _ceiling */
+  /* written */
+  double* start;               /* 3 per slot: position as the step began (awake slots) */
+  double* start_q;             /* 4 per slot */
+  double* inv_i;               /* 6 per slot: world inverse inertia xx xy xz yy yz zz */
+  /* read only */
+  const double* inv_mass;      /* 1 */
+  const double* inertia;       /* 3: principal moments */
+  const double* inv_inertia;   /* 3 */
+  const double* dims;          /* 3: box size; sphere radius; capsule radius, height */
+  const double* damping;       /* 1 */
+  const double* angular_damping; /* 1 */
+  const double* gravity_scale; /* 1 */
+  const uint8_t* type;         /* BG_DYNAMIC, BG_STATIC, ... */
+  const uint8_t* shape;        /* BG_BOX, BG_SPHERE, BG_CAPSULE */
+  const uint8_t* frozen;       /* World._frozen: nonzero frozen */
+  const uint8_t* framed;       /* World._framed */
+  const uint8_t* lock;         /* World._lock: bit k, no turning about world axis k */
+  const int32_t* joint_head;   /* World._jointHead: nonzero for a jointed body */
+} bg_bodies;
+
+/*
+ * One step's manifolds (src/contact.js Contacts), rows in colour order: colour k is rows
+ * starts[k] .. starts[k+1]-1, the overflow starts[32] .. starts[33]-1, the resting run
+ * starts[33] .. count-1 (not solved).  Point columns hold BG_POINTS entries per row,
+ * vectors 3 per row or per point, as in the reference.
+ */
+typedef struct bg_rows {
+  int32_t count;               /* Contacts.count */
+  int32_t solved;              /* Contacts.solved == starts[33] */
+  int32_t starts[BG_STARTS];   /* Contacts.starts */
+  const int32_t* row;          /* found order -> row (Contacts.row), count entries */
+  const int32_t* a;
+  const int32_t* b;
+  const uint8_t* points;       /* 1..4 */
+  const double* normal;        /* 3 per row, from a to b */
+  const double* t1;            /* 3 per row: basis() */
+  const double* t2;            /* 3 per row */
+  const double* friction;
+  const double* restitution;
+  const double* tolerance;
+  const double* patch;
+  const double* separation;    /* 4 per row */
+  const double* point;         /* 12 per row */
+  const double* shift;         /* 12 per row */
+  /* read and written: warm-start impulses in, the step's impulses out */
+  double* normal_impulse;      /* 4 per row */
+  double* tangent_impulse1;
+  double* tangent_impulse2;
+  double* roll_impulse1;
+  double* roll_impulse2;
+  double* spin_impulse;
+  double* drift1;              /* carried slip in, slipped() slip out */
+  double* drift2;
+  /* written */
+  double* gap;                 /* least separation as the last pass saw it */
+  double* max_normal_impulse;  /* 4 per row */
+  double* relative_velocity;   /* 4 per row */
+  uint8_t* sliding;
+  double* anchor_a;            /* 3 per row, may be NULL */
+  double* anchor_b;            /* 3 per row, may be NULL */
+} bg_rows;
+
+typedef struct bg_step {
+  double dt;                   /* World.step(dt) */
+  int32_t substeps;            /* World._substeps (8 by default) */
+  double gravity[3];           /* World._gravity */
+} bg_step;
+
+/*
+ * A batch of independent worlds solved in one launch.  bg_bodies and bg_rows then hold every
+ * world's arrays end to end; these offsets say where each world's are.  Row columns' a and b,
+ * awake_list entries and row[] entries are local to their world.
+ */
+typedef struct bg_worlds {
+  int32_t count;               /* worlds */
+  const int32_t* body_offset;  /* count+1: world w's slots are [body_offset[w], body_offset[w+1]) */
+  const int32_t* awake_offset; /* count+1: into bodies.awake_list */
+  const int32_t* row_offset;   /* count+1: into the row columns */
+  const int32_t* starts;       /* BG_STARTS per world, local row numbers */
+  const double* gravity;       /* 3 per world, or NULL for bg_step.gravity */
+} bg_worlds;
+
+/* Creates a context on CUDA device `device`.  NULL on failure (no device, no memory). */
+bg_ctx* bg_create(int32_t device, uint32_t flags);
+/* Frees every device buffer, stream and graph of the context. */
+void bg_destroy(bg_ctx* ctx);
+/* The last error's text for this context ("" if none).  Valid until the next call on ctx. */
+const char* bg_last_error(const bg_ctx* ctx);
+/* Version of the ABI: (major << 16) | minor. */
+uint32_t bg_version(void);
+
+/*
+ * One solve stage end to end: uploads the bodies and rows, runs the solve stage on the device,
+ * and downloads every written column.  Replaces src/world.js:962-1032 (inertias .. restitution,
+ * plus the drift half of store()).  Synchronous.
+ */
+int32_t bg_solve_step(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows, const bg_step* step);
+
+/* The same three parts, separately.  bg_upload and bg_solve are asynchronous on the context's
+ * stream; bg_download synchronises.  bg_solve may be called again after bg_restore without a new
+ * upload: bg_upload keeps a pristine device copy of what it uploaded. */
+int32_t bg_upload(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows);
+int32_t bg_restore(bg_ctx* ctx);
+int32_t bg_solve(bg_ctx* ctx, const bg_step* step);
+int32_t bg_download(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows);
+
+/* Batched worlds: one CTA per small world, the same solve stage, one launch for all. */
+int32_t bg_batch_solve_step(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows,
+                            const bg_worlds* worlds, const bg_step* step);
+int32_t bg_batch_upload(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows, const bg_worlds* worlds);
+int32_t bg_batch_solve(bg_ctx* ctx, const bg_step* step);
+int32_t bg_batch_download(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
+void* bg_stream(bg_ctx* ctx);
+/* Kernel launches issued by the last bg_solve / bg_batch_solve (for launch accounting). */
+int32_t bg_last_launches(const bg_ctx* ctx);
+/* Grid barriers each colour pass waits at, and the spin budget (iterations) of each wait.
+ * 0 restores the default.  A wait past its budget makes the step return BG_ETIMEOUT. */
+int32_t bg_set_wait_budget(bg_ctx* ctx, int64_t iterations);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEARING_GPU_H */

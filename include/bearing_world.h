@@ -1,0 +1,103 @@
+/*
+ * bearing_world.h - the host side of World.step, around the solve stage (libbearing_host.so).
+ *
+ * Bearing's World (src/world.js) runs its broadphase, narrowphase and colouring on the CPU and
+ * hands the solve stage (src/world.js:962-1032) to whatever runs it.  This library is that
+ * host side for worlds of boxes, spheres and capsules: bodies by slot as World keeps them,
+ * fat-box pair finding, the pair list with its warm-start memory (src/pairs.js), the
+ * narrowphase (src/collide.js), emit/carry (src/contact.js:889-1036), the colouring and row
+ * layout (src/graph.js:105-214), then store/keep (src/contact.js:1067-1115) and the transforms
+ * (src/world.js:1040-1057) after the solve.  The solve stage itself is a pluggable function
+ * with the signature of bg_solve_step (bearing_gpu.h): the GPU library, or any other.
+ *
+ * Not covered (a world using them is refused): hulls, compounds, meshes, heightfields, joints,
+ * characters, sensors, sleeping islands, the time-of-impact sweep and the contact-reuse cache.
+ */
+#ifndef BEARING_WORLD_H
+#define BEARING_WORLD_H
+
+#include <stdint.h>
+
+#include "bearing_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bw_world bw_world;
+
+/* World options (src/world.js:82, 314-395): gravity, substeps. */
+typedef struct bw_options {
+  double gravity[3];
+  int32_t substeps;
+} bw_options;
+
+/* addBody's spec for a box, sphere or capsule (src/world.js:190-221 defaults). */
+typedef struct bw_body {
+  int32_t type;          /* BG_DYNAMIC or BG_STATIC (kinematic: 2) */
+  int32_t shape;         /* BG_BOX, BG_SPHERE, BG_CAPSULE */
+  double size[3];        /* box */
+  double radius;         /* sphere, capsule */
+  double height;         /* capsule, caps included */
+  double density;        /* kg/m^3, used unless mass > 0 */
+  double mass;           /* kg, 0: from density */
+  double friction;
+  double restitution;
+  double damping;
+  double angular_damping;
+  double gravity_scale;
+  double position[3];
+  double rotation[4];    /* x y z w, normalised on the way in (src/core/check.js:106-117) */
+  double velocity[3];
+  double angular[3];
+} bw_body;
+
+/* The solve stage the world calls each step: bg_solve_step's signature with a user pointer. */
+typedef int32_t (*bw_solver)(void* user, const bg_bodies* bodies, const bg_rows* rows, const bg_step* step);
+
+/* Counters of the last step (for benchmarks and tests). */
+typedef struct bw_stats {
+  int32_t bodies;        /* slots in use */
+  int32_t awake;
+  int32_t pairs;
+  int32_t rows;          /* manifolds (Contacts.count) */
+  int32_t solved;        /* rows before the resting run */
+  int32_t points;        /* contact points over the solved rows */
+  int32_t colours;       /* colours used (non-empty), overflow excluded */
+  int32_t overflow;      /* rows in the overflow colour */
+  int64_t step;          /* steps taken */
+} bw_stats;
+
+bw_world* bw_create(const bw_options* options);
+void bw_destroy(bw_world* world);
+const char* bw_last_error(const bw_world* world);
+
+/* Adds a body; returns its slot, or a negative BG_E* code. */
+int32_t bw_add_body(bw_world* world, const bw_body* body);
+
+/* The solve stage to call; NULL restores none (bw_step then fails with BG_EUNSUPPORTED). */
+int32_t bw_set_solver(bw_world* world, bw_solver solver, void* user);
+
+/* A whole World.step(dt): bw_begin_step, the solver, bw_end_step. */
+int32_t bw_step(bw_world* world, double dt);
+
+/* The step up to the solve stage: bounds, pairs, narrowphase, emit/carry, colour, rest.
+ * After it, bw_bodies_view / bw_rows_view describe the solve stage's input. */
+int32_t bw_begin_step(bw_world* world, double dt);
+/* The step after the solve stage: store/keep, touching, transforms. */
+int32_t bw_end_step(bw_world* world);
+
+/* Views of the world's own columns (valid until the next bw_* call that changes sizes). */
+int32_t bw_bodies_view(bw_world* world, bg_bodies* out);
+int32_t bw_rows_view(bw_world* world, bg_rows* out);
+int32_t bw_step_params(const bw_world* world, bg_step* out);
+
+/* World.transforms: 7 floats per slot (position, rotation x y z w). */
+const float* bw_transforms(const bw_world* world);
+int32_t bw_stats_get(const bw_world* world, bw_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEARING_WORLD_H */
