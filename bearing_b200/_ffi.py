@@ -26,6 +26,8 @@ BG_ENOMEM = -4
 BG_EUNSUPPORTED = -5
 BG_EFAULT = -6
 
+BG_FLAG_PIN_HOST, BG_FLAG_GRID, BG_FLAG_BLOCK = 1, 2, 4
+
 BG_DYNAMIC, BG_STATIC, BG_KINEMATIC = 0, 1, 2
 BG_BOX, BG_SPHERE, BG_CAPSULE = 0, 1, 2
 

@@ -1,0 +1,791 @@
+// libbearing_gpu.so: the C ABI of include/bearing_gpu.h over the device solve stage in
+// stage.cuh.  Per context: one CUDA stream, device buffers grown by doubling (the rule
+// src/contact.js:250-255 uses for its columns), a staging copy of each input column in the
+// caller's layout (so bg_restore can run the same input again), and the packed device layout.
+//
+// A step is: copy the caller's columns in (one cudaMemcpyAsync per column), unpack them into
+// the device layout, run the solve stage (a persistent cooperative grid for a large world, one
+// CTA per world otherwise), pack the written columns and copy them out.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/bearing_gpu.h"
+#include "layout.cuh"
+#include "stage.cuh"
+
+namespace {
+
+constexpr int kGridThreads = 256;
+constexpr int kBlockThreads = 256;
+constexpr int kUnpackThreads = 256;
+// A world with at least this many solved rows is run by the whole grid; smaller ones by one CTA.
+constexpr int kGridRows = 3000;
+constexpr long long kDefaultBudget = 1LL << 24;
+
+// ---- kernels: stage the caller's layout in and out of the device layout ----
+
+struct BodyStage {
+  const double* position; const double* rotation; const double* velocity; const double* angular;
+  const double* tumbled; const double* ceiling; const double* start; const double* inv_mass;
+  const double* inertia; const double* inv_inertia; const double* dims; const double* damping;
+  const double* angular_damping; const double* gravity_scale;
+  const uint8_t* type; const uint8_t* shape; const uint8_t* frozen; const uint8_t* framed;
+  const uint8_t* lock; const int32_t* joint_head; const uint8_t* awake; const double* inv_i;
+};
+
+struct BodyOut {
+  double* position; double* rotation; double* velocity; double* angular; double* tumbled;
+  double* ceiling; double* start; double* start_q; double* inv_i;
+};
+
+struct RowStage {
+  const int32_t* row; const int32_t* a; const int32_t* b; const uint8_t* points;
+  const double* normal; const double* t1; const double* t2; const double* friction;
+  const double* restitution; const double* tolerance; const double* patch; const double* separation;
+  const double* point; const double* shift; const double* normal_impulse; const double* ti1;
+  const double* ti2; const double* ri1; const double* ri2; const double* si; const double* drift1;
+  const double* drift2;
+};
+
+struct RowOut {
+  double* normal_impulse; double* ti1; double* ti2; double* ri1; double* ri2; double* si;
+  double* drift1; double* drift2; double* gap; double* maxni; double* relvel; uint8_t* sliding;
+  double* anchor_a; double* anchor_b;
+};
+
+// Which world index i (a row or an awake entry) belongs to, from a (count+1) prefix table.
+__device__ __forceinline__ int world_of(const int32_t* offset, int count, int i) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (offset[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void unpack_bodies(BodyStage in, bg::BodiesDev B, int n, const int32_t* awake_in, int nawake,
+                              const int32_t* body_offset, const int32_t* awake_offset, int nworlds) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
+    for (int k = 0; k < 3; k++) {
+      B.vw[8 * s + k] = in.velocity[3 * s + k];
+      B.vw[8 * s + 3 + k] = in.angular[3 * s + k];
+      B.pq[8 * s + k] = in.position[3 * s + k];
+      B.st[4 * s + k] = in.start[3 * s + k];
+      B.tc[4 * s + k] = in.tumbled[3 * s + k];
+      B.pr[12 * s + k] = in.inertia[3 * s + k];
+      B.pr[12 * s + 3 + k] = in.inv_inertia[3 * s + k];
+      B.pr[12 * s + 6 + k] = in.dims[3 * s + k];
+    }
+    B.vw[8 * s + 6] = 0; B.vw[8 * s + 7] = 0;
+    B.pq[8 * s + 3] = 0;
+    B.st[4 * s + 3] = 0;
+    for (int k = 0; k < 4; k++) { B.pq[8 * s + 4 + k] = in.rotation[4 * s + k]; B.sq[4 * s + k] = 0; }
+    B.tc[4 * s + 3] = in.ceiling[s];
+    B.pr[12 * s + 9] = in.damping[s];
+    B.pr[12 * s + 10] = in.angular_damping[s];
+    B.pr[12 * s + 11] = in.gravity_scale[s];
+    B.mi[8 * s] = in.inv_mass[s];
+    for (int k = 0; k < 6; k++) B.mi[8 * s + 1 + k] = in.inv_i[6 * s + k];
+    B.mi[8 * s + 7] = 0;
+    uint32_t f = static_cast<uint32_t>(in.type[s]) & bg::F_TYPE;
+    f |= (static_cast<uint32_t>(in.shape[s]) & 3u) << bg::F_SHAPE_SHIFT;
+    if (in.frozen[s]) f |= bg::F_FROZEN;
+    if (in.framed[s]) f |= bg::F_FRAMED;
+    f |= (static_cast<uint32_t>(in.lock[s]) & 7u) << bg::F_LOCK_SHIFT;
+    if (in.joint_head[s] != 0) f |= bg::F_JOINTED;
+    if (in.awake[s]) f |= bg::F_AWAKE;
+    B.fl[s] = f;
+    B.head[s] = 0x7fffffff;
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nawake; i += stride) {
+    const int w = nworlds > 1 ? world_of(awake_offset, nworlds, i) : 0;
+    B.awake_list[i] = awake_in[i] + (nworlds > 1 ? body_offset[w] : 0);
+  }
+}
+
+__global__ void unpack_rows(RowStage in, bg::RowsDev R, int n, const int32_t* row_offset, const int32_t* body_offset,
+                            int nworlds, const double* maxni_in, const double* relvel_in, const double* gap_in) {
+  const int64_t cap = R.cap;
+  const int stride = gridDim.x * blockDim.x;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += stride) {
+    int r0 = 0, b0 = 0;
+    if (nworlds > 1) {
+      const int w = world_of(row_offset, nworlds, m);
+      r0 = row_offset[w];
+      b0 = body_offset[w];
+    }
+    R.row[m] = in.row[m] + r0;
+    R.a[m] = in.a[m] + b0;
+    R.b[m] = in.b[m] + b0;
+    R.points[m] = in.points[m];
+    for (int c = 0; c < 3; c++) {
+      R.n[c * cap + m] = in.normal[3 * m + c];
+      R.t1[c * cap + m] = in.t1[3 * m + c];
+      R.t2[c * cap + m] = in.t2[3 * m + c];
+    }
+    R.friction[m] = in.friction[m];
+    R.restitution[m] = in.restitution[m];
+    R.tolerance[m] = in.tolerance[m];
+    R.patch[m] = in.patch[m];
+    // What the stage does not write (the resting run, and point slots past a row's count) is
+    // handed back as the caller gave it.
+    R.gap[m] = gap_in[m];
+    R.sliding[m] = 0;
+    for (int c = 0; c < 3; c++) { R.anchorA[c * cap + m] = 0; R.anchorB[c * cap + m] = 0; }
+    for (int k = 0; k < bg::P; k++) {
+      R.maxni[k * cap + m] = maxni_in[bg::P * m + k];
+      R.relvel[k * cap + m] = relvel_in[bg::P * m + k];
+      R.separation[k * cap + m] = in.separation[bg::P * m + k];
+      R.ni[k * cap + m] = in.normal_impulse[bg::P * m + k];
+      for (int c = 0; c < 3; c++) {
+        R.point[(k * 3 + c) * cap + m] = in.point[12 * m + 3 * k + c];
+        R.shift[(k * 3 + c) * cap + m] = in.shift[12 * m + 3 * k + c];
+      }
+    }
+    R.ti1[m] = in.ti1[m]; R.ti2[m] = in.ti2[m]; R.ri1[m] = in.ri1[m]; R.ri2[m] = in.ri2[m];
+    R.si[m] = in.si[m]; R.drift1[m] = in.drift1[m]; R.drift2[m] = in.drift2[m];
+  }
+}
+
+__global__ void pack_bodies(bg::BodiesDev B, BodyOut out, int n) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
+    for (int k = 0; k < 3; k++) {
+      out.velocity[3 * s + k] = B.vw[8 * s + k];
+      out.angular[3 * s + k] = B.vw[8 * s + 3 + k];
+      out.position[3 * s + k] = B.pq[8 * s + k];
+      out.start[3 * s + k] = B.st[4 * s + k];
+      out.tumbled[3 * s + k] = B.tc[4 * s + k];
+    }
+    for (int k = 0; k < 4; k++) { out.rotation[4 * s + k] = B.pq[8 * s + 4 + k]; out.start_q[4 * s + k] = B.sq[4 * s + k]; }
+    out.ceiling[s] = B.tc[4 * s + 3];
+    for (int k = 0; k < 6; k++) out.inv_i[6 * s + k] = B.mi[8 * s + 1 + k];
+  }
+}
+
+__global__ void pack_rows(bg::RowsDev R, RowOut out, int n) {
+  const int64_t cap = R.cap;
+  const int stride = gridDim.x * blockDim.x;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += stride) {
+    for (int k = 0; k < bg::P; k++) {
+      out.normal_impulse[bg::P * m + k] = R.ni[k * cap + m];
+      out.maxni[bg::P * m + k] = R.maxni[k * cap + m];
+      out.relvel[bg::P * m + k] = R.relvel[k * cap + m];
+    }
+    out.ti1[m] = R.ti1[m]; out.ti2[m] = R.ti2[m]; out.ri1[m] = R.ri1[m]; out.ri2[m] = R.ri2[m];
+    out.si[m] = R.si[m]; out.drift1[m] = R.drift1[m]; out.drift2[m] = R.drift2[m];
+    out.gap[m] = R.gap[m];
+    out.sliding[m] = R.sliding[m];
+    for (int c = 0; c < 3; c++) {
+      out.anchor_a[3 * m + c] = R.anchorA[c * cap + m];
+      out.anchor_b[3 * m + c] = R.anchorB[c * cap + m];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kGridThreads) stage_grid(bg::StageParams p) {
+  bg::GridTeam t;
+  const bg::WorldDesc w = p.worlds[0];
+  bg::solve_stage(p, w, t);
+}
+
+__global__ void __launch_bounds__(kBlockThreads) stage_block(bg::StageParams p) {
+  bg::BlockTeam t;
+  for (int wi = blockIdx.x; wi < p.nworlds; wi += gridDim.x) {
+    const bg::WorldDesc w = p.worlds[wi];
+    if (!bg::solve_stage(p, w, t)) return;
+    __syncthreads();
+  }
+}
+
+
+// ---- device buffers ----
+
+template <class T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t n = 0;
+};
+
+}  // namespace
+
+struct bg_ctx {
+  int device = 0;
+  uint32_t flags = 0;
+  cudaStream_t stream = nullptr;
+  std::string error;
+  int sms = 0;
+  int grid_blocks = 0;
+  long long budget = kDefaultBudget;
+  int last_launches = 0;
+  // capacities
+  int body_cap = 0, row_cap = 0, awake_cap = 0, world_cap = 0;
+  // device allocations, all freed in bg_destroy
+  std::vector<void*> allocs;
+  // body records
+  bg::BodiesDev B = {};
+  bg::RowsDev R = {};
+  // staging in (caller layout)
+  BodyStage bin = {};
+  int32_t* awake_in = nullptr;
+  RowStage rin = {};
+  double* maxni_in = nullptr;
+  double* relvel_in = nullptr;
+  double* gap_in = nullptr;
+  // staging out
+  BodyOut bout = {};
+  RowOut rout = {};
+  // worlds
+  bg::WorldDesc* worlds_dev = nullptr;
+  int32_t* body_offset_dev = nullptr;
+  int32_t* awake_offset_dev = nullptr;
+  int32_t* row_offset_dev = nullptr;
+  std::vector<bg::WorldDesc> worlds;
+  // barrier and status
+  unsigned int* bar = nullptr;   // [0] count, [1] generation
+  int32_t* status = nullptr;
+  int32_t* block_counts = nullptr;
+  // what was uploaded
+  int nbodies = 0, nrows = 0, nawake = 0, nworlds = 0;
+  bool uploaded = false;
+  bool batch = false;
+};
+
+namespace {
+
+void set_error(bg_ctx* c, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  c->error = buf;
+}
+
+bool cuda_ok(bg_ctx* c, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  set_error(c, "%s: %s", what, cudaGetErrorString(e));
+  return false;
+}
+
+template <class T>
+bool dev_alloc(bg_ctx* c, T** p, size_t n) {
+  void* q = nullptr;
+  if (n == 0) n = 1;
+  if (!cuda_ok(c, cudaMalloc(&q, n * sizeof(T)), "cudaMalloc")) return false;
+  c->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return true;
+}
+
+void free_all(bg_ctx* c) {
+  for (void* p : c->allocs) cudaFree(p);
+  c->allocs.clear();
+}
+
+size_t grown(size_t have, size_t want) {
+  size_t c = have > 0 ? have : 64;
+  while (c < want) c *= 2;
+  return c;
+}
+
+// (Re)allocates every buffer for at least the given sizes.  Everything is reallocated together,
+// so a resize never leaves a stale pointer behind.
+bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
+  if (nbodies <= c->body_cap && nrows <= c->row_cap && nawake <= c->awake_cap && nworlds <= c->world_cap && c->bar)
+    return true;
+  cudaStreamSynchronize(c->stream);
+  free_all(c);
+  const size_t nb = grown(c->body_cap, static_cast<size_t>(nbodies));
+  const size_t nr = grown(c->row_cap, static_cast<size_t>(nrows));
+  const size_t na = grown(c->awake_cap, static_cast<size_t>(nawake));
+  const size_t nw = grown(c->world_cap, static_cast<size_t>(nworlds));
+  bool ok = true;
+  bg::BodiesDev& B = c->B;
+  ok = ok && dev_alloc(c, &B.vw, 8 * nb) && dev_alloc(c, &B.mi, 8 * nb) && dev_alloc(c, &B.pq, 8 * nb) &&
+       dev_alloc(c, &B.st, 4 * nb) && dev_alloc(c, &B.sq, 4 * nb) && dev_alloc(c, &B.tc, 4 * nb) &&
+       dev_alloc(c, &B.pr, 12 * nb) && dev_alloc(c, &B.fl, nb) && dev_alloc(c, &B.awake_list, na) &&
+       dev_alloc(c, &B.head, nb);
+  BodyStage& bi = c->bin;
+  double *position, *rotation, *velocity, *angular, *tumbled, *ceiling, *start, *inv_mass, *inertia, *inv_inertia,
+      *dims, *damping, *angular_damping, *gravity_scale, *inv_i;
+  uint8_t *type, *shape, *frozen, *framed, *lock, *awake;
+  int32_t* joint_head;
+  ok = ok && dev_alloc(c, &position, 3 * nb) && dev_alloc(c, &rotation, 4 * nb) && dev_alloc(c, &velocity, 3 * nb) &&
+       dev_alloc(c, &angular, 3 * nb) && dev_alloc(c, &tumbled, 3 * nb) && dev_alloc(c, &ceiling, nb) &&
+       dev_alloc(c, &start, 3 * nb) && dev_alloc(c, &inv_mass, nb) && dev_alloc(c, &inertia, 3 * nb) &&
+       dev_alloc(c, &inv_inertia, 3 * nb) && dev_alloc(c, &dims, 3 * nb) && dev_alloc(c, &damping, nb) &&
+       dev_alloc(c, &angular_damping, nb) && dev_alloc(c, &gravity_scale, nb) && dev_alloc(c, &type, nb) &&
+       dev_alloc(c, &shape, nb) && dev_alloc(c, &frozen, nb) && dev_alloc(c, &framed, nb) && dev_alloc(c, &lock, nb) &&
+       dev_alloc(c, &joint_head, nb) && dev_alloc(c, &awake, nb) && dev_alloc(c, &c->awake_in, na) &&
+       dev_alloc(c, &inv_i, 6 * nb);
+  if (!ok) return false;
+  bi = BodyStage{position, rotation, velocity, angular, tumbled, ceiling, start, inv_mass, inertia, inv_inertia, dims,
+                 damping, angular_damping, gravity_scale, type, shape, frozen, framed, lock, joint_head, awake, inv_i};
+  BodyOut& bo = c->bout;
+  ok = ok && dev_alloc(c, &bo.position, 3 * nb) && dev_alloc(c, &bo.rotation, 4 * nb) &&
+       dev_alloc(c, &bo.velocity, 3 * nb) && dev_alloc(c, &bo.angular, 3 * nb) && dev_alloc(c, &bo.tumbled, 3 * nb) &&
+       dev_alloc(c, &bo.ceiling, nb) && dev_alloc(c, &bo.start, 3 * nb) && dev_alloc(c, &bo.start_q, 4 * nb) &&
+       dev_alloc(c, &bo.inv_i, 6 * nb);
+  // rows
+  bg::RowsDev& R = c->R;
+  R.cap = static_cast<int64_t>(nr);
+  ok = ok && dev_alloc(c, &R.a, nr) && dev_alloc(c, &R.b, nr) && dev_alloc(c, &R.points, nr) && dev_alloc(c, &R.row, nr) &&
+       dev_alloc(c, &R.n, 3 * nr) && dev_alloc(c, &R.t1, 3 * nr) && dev_alloc(c, &R.t2, 3 * nr) &&
+       dev_alloc(c, &R.friction, nr) && dev_alloc(c, &R.restitution, nr) && dev_alloc(c, &R.tolerance, nr) &&
+       dev_alloc(c, &R.patch, nr) && dev_alloc(c, &R.separation, 4 * nr) && dev_alloc(c, &R.point, 12 * nr) &&
+       dev_alloc(c, &R.shift, 12 * nr) && dev_alloc(c, &R.ni, 4 * nr) && dev_alloc(c, &R.ti1, nr) &&
+       dev_alloc(c, &R.ti2, nr) && dev_alloc(c, &R.ri1, nr) && dev_alloc(c, &R.ri2, nr) && dev_alloc(c, &R.si, nr) &&
+       dev_alloc(c, &R.drift1, nr) && dev_alloc(c, &R.drift2, nr) && dev_alloc(c, &R.gap, nr) &&
+       dev_alloc(c, &R.maxni, 4 * nr) && dev_alloc(c, &R.relvel, 4 * nr) && dev_alloc(c, &R.sliding, nr) &&
+       dev_alloc(c, &R.anchorA, 3 * nr) && dev_alloc(c, &R.anchorB, 3 * nr) && dev_alloc(c, &R.la, 12 * nr) &&
+       dev_alloc(c, &R.lb, 12 * nr) && dev_alloc(c, &R.adjusted, 4 * nr) && dev_alloc(c, &R.now, 4 * nr) &&
+       dev_alloc(c, &R.normalMass, 4 * nr) && dev_alloc(c, &R.lever, 4 * nr) && dev_alloc(c, &R.jac, 48 * nr) &&
+       dev_alloc(c, &R.K, 16 * nr) && dev_alloc(c, &R.fjac, 24 * nr) && dev_alloc(c, &R.tm, 3 * nr) &&
+       dev_alloc(c, &R.rm1, nr) && dev_alloc(c, &R.rm2, nr) && dev_alloc(c, &R.sm, nr) &&
+       dev_alloc(c, &R.active, nr) && dev_alloc(c, &R.pending, nr);
+  RowStage& ri = c->rin;
+  int32_t *row, *a, *b;
+  uint8_t* points;
+  double *normal, *t1, *t2, *friction, *restitution, *tolerance, *patch, *separation, *point, *shift, *ni, *ti1, *ti2,
+      *ri1, *ri2, *si, *drift1, *drift2;
+  ok = ok && dev_alloc(c, &row, nr) && dev_alloc(c, &a, nr) && dev_alloc(c, &b, nr) && dev_alloc(c, &points, nr) &&
+       dev_alloc(c, &normal, 3 * nr) && dev_alloc(c, &t1, 3 * nr) && dev_alloc(c, &t2, 3 * nr) &&
+       dev_alloc(c, &friction, nr) && dev_alloc(c, &restitution, nr) && dev_alloc(c, &tolerance, nr) &&
+       dev_alloc(c, &patch, nr) && dev_alloc(c, &separation, 4 * nr) && dev_alloc(c, &point, 12 * nr) &&
+       dev_alloc(c, &shift, 12 * nr) && dev_alloc(c, &ni, 4 * nr) && dev_alloc(c, &ti1, nr) && dev_alloc(c, &ti2, nr) &&
+       dev_alloc(c, &ri1, nr) && dev_alloc(c, &ri2, nr) && dev_alloc(c, &si, nr) && dev_alloc(c, &drift1, nr) &&
+       dev_alloc(c, &drift2, nr) && dev_alloc(c, &c->maxni_in, 4 * nr) && dev_alloc(c, &c->relvel_in, 4 * nr) &&
+       dev_alloc(c, &c->gap_in, nr);
+  if (!ok) return false;
+  ri = RowStage{row, a, b, points, normal, t1, t2, friction, restitution, tolerance, patch, separation, point, shift,
+                ni, ti1, ti2, ri1, ri2, si, drift1, drift2};
+  RowOut& ro = c->rout;
+  ok = ok && dev_alloc(c, &ro.normal_impulse, 4 * nr) && dev_alloc(c, &ro.ti1, nr) && dev_alloc(c, &ro.ti2, nr) &&
+       dev_alloc(c, &ro.ri1, nr) && dev_alloc(c, &ro.ri2, nr) && dev_alloc(c, &ro.si, nr) && dev_alloc(c, &ro.drift1, nr) &&
+       dev_alloc(c, &ro.drift2, nr) && dev_alloc(c, &ro.gap, nr) && dev_alloc(c, &ro.maxni, 4 * nr) &&
+       dev_alloc(c, &ro.relvel, 4 * nr) && dev_alloc(c, &ro.sliding, nr) && dev_alloc(c, &ro.anchor_a, 3 * nr) &&
+       dev_alloc(c, &ro.anchor_b, 3 * nr);
+  // worlds
+  ok = ok && dev_alloc(c, &c->worlds_dev, nw) && dev_alloc(c, &c->body_offset_dev, nw + 1) &&
+       dev_alloc(c, &c->awake_offset_dev, nw + 1) && dev_alloc(c, &c->row_offset_dev, nw + 1);
+  ok = ok && dev_alloc(c, &c->bar, 2) && dev_alloc(c, &c->status, 1) &&
+       dev_alloc(c, &c->block_counts, static_cast<size_t>(c->grid_blocks > 0 ? c->grid_blocks : 1024));
+  if (!ok) return false;
+  if (!cuda_ok(c, cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned int), c->stream), "cudaMemset")) return false;
+  c->body_cap = static_cast<int>(nb);
+  c->row_cap = static_cast<int>(nr);
+  c->awake_cap = static_cast<int>(na);
+  c->world_cap = static_cast<int>(nw);
+  return true;
+}
+
+template <class T>
+bool put(bg_ctx* c, T* dst, const T* src, size_t n, const char* what) {
+  if (n == 0) return true;
+  if (src == nullptr) {
+    set_error(c, "upload: column %s is NULL", what);
+    return false;
+  }
+  return cuda_ok(c, cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, c->stream), what);
+}
+
+template <class T>
+bool get(bg_ctx* c, T* dst, const T* src, size_t n, const char* what) {
+  if (n == 0 || dst == nullptr) return true;
+  return cuda_ok(c, cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, c->stream), what);
+}
+
+int validate(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
+  if (B == nullptr || R == nullptr) {
+    set_error(c, "bodies and rows must not be NULL");
+    return BG_EINVAL;
+  }
+  if (B->capacity < 0 || B->awake_count < 0 || B->awake_count > B->capacity || R->count < 0) {
+    set_error(c, "negative or inconsistent counts");
+    return BG_EINVAL;
+  }
+  return BG_OK;
+}
+
+int validate_world(bg_ctx* c, int nbodies, int nrows, const int32_t* starts, int solved) {
+  if (starts[0] != 0) {
+    set_error(c, "rows.starts[0] must be 0");
+    return BG_EINVAL;
+  }
+  for (int k = 0; k < bg::NSTARTS - 1; k++)
+    if (starts[k + 1] < starts[k]) {
+      set_error(c, "rows.starts must not decrease");
+      return BG_EINVAL;
+    }
+  if (starts[bg::RESTING_RUN] != solved || solved > nrows || starts[bg::NSTARTS - 1] > nrows) {
+    set_error(c, "rows.solved must equal starts[33] and be at most count");
+    return BG_EINVAL;
+  }
+  (void)nbodies;
+  return BG_OK;
+}
+
+// Copies the caller's columns for `nb` slots / `nr` rows / `na` awake entries into staging.
+int upload_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R, int nb, int nr, int na) {
+  const size_t b = static_cast<size_t>(nb), r = static_cast<size_t>(nr);
+  BodyStage& s = c->bin;
+  bool ok = put(c, const_cast<double*>(s.position), B->position, 3 * b, "position") &&
+            put(c, const_cast<double*>(s.rotation), B->rotation, 4 * b, "rotation") &&
+            put(c, const_cast<double*>(s.velocity), B->velocity, 3 * b, "velocity") &&
+            put(c, const_cast<double*>(s.angular), B->angular, 3 * b, "angular") &&
+            put(c, const_cast<double*>(s.tumbled), B->tumbled, 3 * b, "tumbled") &&
+            put(c, const_cast<double*>(s.ceiling), B->ceiling, b, "ceiling") &&
+            put(c, const_cast<double*>(s.start), B->start, 3 * b, "start") &&
+            put(c, const_cast<double*>(s.inv_mass), B->inv_mass, b, "inv_mass") &&
+            put(c, const_cast<double*>(s.inertia), B->inertia, 3 * b, "inertia") &&
+            put(c, const_cast<double*>(s.inv_inertia), B->inv_inertia, 3 * b, "inv_inertia") &&
+            put(c, const_cast<double*>(s.dims), B->dims, 3 * b, "dims") &&
+            put(c, const_cast<double*>(s.damping), B->damping, b, "damping") &&
+            put(c, const_cast<double*>(s.angular_damping), B->angular_damping, b, "angular_damping") &&
+            put(c, const_cast<double*>(s.gravity_scale), B->gravity_scale, b, "gravity_scale") &&
+            put(c, const_cast<uint8_t*>(s.type), B->type, b, "type") &&
+            put(c, const_cast<uint8_t*>(s.shape), B->shape, b, "shape") &&
+            put(c, const_cast<uint8_t*>(s.frozen), B->frozen, b, "frozen") &&
+            put(c, const_cast<uint8_t*>(s.framed), B->framed, b, "framed") &&
+            put(c, const_cast<uint8_t*>(s.lock), B->lock, b, "lock") &&
+            put(c, const_cast<int32_t*>(s.joint_head), B->joint_head, b, "joint_head") &&
+            put(c, const_cast<uint8_t*>(s.awake), B->awake, b, "awake") &&
+            put(c, c->awake_in, B->awake_list, static_cast<size_t>(na), "awake_list") &&
+            put(c, const_cast<double*>(s.inv_i), B->inv_i, 6 * b, "inv_i");
+  RowStage& q = c->rin;
+  ok = ok && put(c, const_cast<int32_t*>(q.row), R->row, r, "row") && put(c, const_cast<int32_t*>(q.a), R->a, r, "a") &&
+       put(c, const_cast<int32_t*>(q.b), R->b, r, "b") && put(c, const_cast<uint8_t*>(q.points), R->points, r, "points") &&
+       put(c, const_cast<double*>(q.normal), R->normal, 3 * r, "normal") &&
+       put(c, const_cast<double*>(q.t1), R->t1, 3 * r, "t1") && put(c, const_cast<double*>(q.t2), R->t2, 3 * r, "t2") &&
+       put(c, const_cast<double*>(q.friction), R->friction, r, "friction") &&
+       put(c, const_cast<double*>(q.restitution), R->restitution, r, "restitution") &&
+       put(c, const_cast<double*>(q.tolerance), R->tolerance, r, "tolerance") &&
+       put(c, const_cast<double*>(q.patch), R->patch, r, "patch") &&
+       put(c, const_cast<double*>(q.separation), R->separation, 4 * r, "separation") &&
+       put(c, const_cast<double*>(q.point), R->point, 12 * r, "point") &&
+       put(c, const_cast<double*>(q.shift), R->shift, 12 * r, "shift") &&
+       put(c, const_cast<double*>(q.normal_impulse), R->normal_impulse, 4 * r, "normal_impulse") &&
+       put(c, const_cast<double*>(q.ti1), R->tangent_impulse1, r, "tangent_impulse1") &&
+       put(c, const_cast<double*>(q.ti2), R->tangent_impulse2, r, "tangent_impulse2") &&
+       put(c, const_cast<double*>(q.ri1), R->roll_impulse1, r, "roll_impulse1") &&
+       put(c, const_cast<double*>(q.ri2), R->roll_impulse2, r, "roll_impulse2") &&
+       put(c, const_cast<double*>(q.si), R->spin_impulse, r, "spin_impulse") &&
+       put(c, const_cast<double*>(q.drift1), R->drift1, r, "drift1") &&
+       put(c, const_cast<double*>(q.drift2), R->drift2, r, "drift2") &&
+       put(c, c->maxni_in, R->max_normal_impulse, 4 * r, "max_normal_impulse") &&
+       put(c, c->relvel_in, R->relative_velocity, 4 * r, "relative_velocity") && put(c, c->gap_in, R->gap, r, "gap");
+  return ok ? BG_OK : BG_ECUDA;
+}
+
+int unpack(bg_ctx* c) {
+  const int nb = c->nbodies, nr = c->nrows, na = c->nawake;
+  const int blocks = std::max(1, std::min(4 * c->sms, (std::max(nb, std::max(nr, na)) + kUnpackThreads - 1) / kUnpackThreads));
+  unpack_bodies<<<blocks, kUnpackThreads, 0, c->stream>>>(c->bin, c->B, nb, c->awake_in, na, c->body_offset_dev,
+                                                         c->awake_offset_dev, c->nworlds);
+  unpack_rows<<<blocks, kUnpackThreads, 0, c->stream>>>(c->rin, c->R, nr, c->row_offset_dev, c->body_offset_dev, c->nworlds,
+                                                       c->maxni_in, c->relvel_in, c->gap_in);
+  c->last_launches += 2;
+  return cuda_ok(c, cudaGetLastError(), "unpack") ? BG_OK : BG_ECUDA;
+}
+
+int upload_worlds(bg_ctx* c, const std::vector<int32_t>& body_off, const std::vector<int32_t>& awake_off,
+                  const std::vector<int32_t>& row_off) {
+  const size_t nw = c->worlds.size();
+  bool ok = put(c, c->worlds_dev, c->worlds.data(), nw, "worlds") &&
+            put(c, c->body_offset_dev, body_off.data(), nw + 1, "body_offset") &&
+            put(c, c->awake_offset_dev, awake_off.data(), nw + 1, "awake_offset") &&
+            put(c, c->row_offset_dev, row_off.data(), nw + 1, "row_offset");
+  // The host vectors must outlive the asynchronous copies.
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(c->stream), "upload worlds");
+  return ok ? BG_OK : BG_ECUDA;
+}
+
+// makeSoft: src/contact.js:1591-1597, for STIFFNESS / h and DAMPING_RATIO (src/world.js:115-118).
+bg::Soft make_soft(double h) {
+  const double hertz = (1.0 / 8.0) / h, zeta = 10;
+  const double omega = 2 * 3.141592653589793 * hertz;
+  const double a1 = 2 * zeta + h * omega, a2 = h * omega * a1, a3 = 1 / (1 + a2);
+  return bg::Soft{omega / a1, a2 * a3, a3};
+}
+
+int launch_stage(bg_ctx* c, const bg_step* step) {
+  if (step == nullptr || !(step->dt > 0) || step->substeps < 1) {
+    set_error(c, "step: dt must be positive and substeps at least 1");
+    return BG_EINVAL;
+  }
+  bg::StageParams p;
+  p.B = c->B;
+  p.R = c->R;
+  p.worlds = c->worlds_dev;
+  p.nworlds = c->nworlds;
+  p.dt = step->dt;
+  p.substeps = step->substeps;
+  p.soft = make_soft(step->dt / step->substeps);
+  p.bar_count = c->bar;
+  p.bar_gen = c->bar + 1;
+  p.status = c->status;
+  p.block_counts = c->block_counts;
+  p.budget = c->budget;
+  if (!cuda_ok(c, cudaMemsetAsync(c->status, 0, sizeof(int32_t), c->stream), "status")) return BG_ECUDA;
+  c->last_launches += 1;
+  bool big = !c->batch && c->nworlds == 1 && c->worlds[0].solved >= kGridRows;
+  if (!c->batch && (c->flags & BG_FLAG_GRID)) big = true;
+  if (!c->batch && (c->flags & BG_FLAG_BLOCK)) big = false;
+  if (big) {
+    void* args[] = {&p};
+    const cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(stage_grid), dim3(c->grid_blocks),
+                                                      dim3(kGridThreads), args, 0, c->stream);
+    if (!cuda_ok(c, e, "stage_grid launch")) return BG_ECUDA;
+  } else {
+    const int blocks = std::min(c->nworlds, 64 * c->sms);
+    stage_block<<<blocks, kBlockThreads, 0, c->stream>>>(p);
+    if (!cuda_ok(c, cudaGetLastError(), "stage_block launch")) return BG_ECUDA;
+  }
+  return BG_OK;
+}
+
+int finish(bg_ctx* c) {
+  const int nb = c->nbodies, nr = c->nrows;
+  const int blocks = std::max(1, std::min(4 * c->sms, (std::max(nb, nr) + kUnpackThreads - 1) / kUnpackThreads));
+  pack_bodies<<<blocks, kUnpackThreads, 0, c->stream>>>(c->B, c->bout, nb);
+  pack_rows<<<blocks, kUnpackThreads, 0, c->stream>>>(c->R, c->rout, nr);
+  c->last_launches += 2;
+  return cuda_ok(c, cudaGetLastError(), "pack") ? BG_OK : BG_ECUDA;
+}
+
+int download_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
+  const size_t b = static_cast<size_t>(c->nbodies), r = static_cast<size_t>(c->nrows);
+  BodyOut& o = c->bout;
+  RowOut& q = c->rout;
+  bool ok = get(c, B->position, o.position, 3 * b, "position") && get(c, B->rotation, o.rotation, 4 * b, "rotation") &&
+            get(c, B->velocity, o.velocity, 3 * b, "velocity") && get(c, B->angular, o.angular, 3 * b, "angular") &&
+            get(c, B->tumbled, o.tumbled, 3 * b, "tumbled") && get(c, B->ceiling, o.ceiling, b, "ceiling") &&
+            get(c, B->start, o.start, 3 * b, "start") && get(c, B->start_q, o.start_q, 4 * b, "start_q") &&
+            get(c, B->inv_i, o.inv_i, 6 * b, "inv_i");
+  ok = ok && get(c, R->normal_impulse, q.normal_impulse, 4 * r, "normal_impulse") &&
+       get(c, R->tangent_impulse1, q.ti1, r, "tangent_impulse1") && get(c, R->tangent_impulse2, q.ti2, r, "tangent_impulse2") &&
+       get(c, R->roll_impulse1, q.ri1, r, "roll_impulse1") && get(c, R->roll_impulse2, q.ri2, r, "roll_impulse2") &&
+       get(c, R->spin_impulse, q.si, r, "spin_impulse") && get(c, R->drift1, q.drift1, r, "drift1") &&
+       get(c, R->drift2, q.drift2, r, "drift2") && get(c, R->gap, q.gap, r, "gap") &&
+       get(c, R->max_normal_impulse, q.maxni, 4 * r, "max_normal_impulse") &&
+       get(c, R->relative_velocity, q.relvel, 4 * r, "relative_velocity") && get(c, R->sliding, q.sliding, r, "sliding") &&
+       get(c, R->anchor_a, q.anchor_a, 3 * r, "anchor_a") && get(c, R->anchor_b, q.anchor_b, 3 * r, "anchor_b");
+  int32_t status = 0;
+  ok = ok && cuda_ok(c, cudaMemcpyAsync(&status, c->status, sizeof status, cudaMemcpyDeviceToHost, c->stream), "status") &&
+       cuda_ok(c, cudaStreamSynchronize(c->stream), "synchronize");
+  if (!ok) return BG_ECUDA;
+  if (status != 0) {
+    set_error(c, "a grid barrier waited past its budget; the step is lost");
+    return BG_ETIMEOUT;
+  }
+  return BG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t bg_version(void) { return (1u << 16) | 0u; }
+
+bg_ctx* bg_create(int32_t device, uint32_t flags) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) return nullptr;
+  bg_ctx* c = new bg_ctx();
+  c->device = device;
+  c->flags = flags;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return nullptr;
+  }
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_grid, kGridThreads, 0);
+  if (per_sm < 1) per_sm = 1;
+  c->grid_blocks = c->sms * per_sm;
+  if (c->grid_blocks > 1024) c->grid_blocks = 1024;
+  return c;
+}
+
+void bg_destroy(bg_ctx* c) {
+  if (c == nullptr) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_all(c);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* bg_last_error(const bg_ctx* c) { return c == nullptr ? "no context" : c->error.c_str(); }
+
+void* bg_stream(bg_ctx* c) { return c == nullptr ? nullptr : static_cast<void*>(c->stream); }
+
+int32_t bg_last_launches(const bg_ctx* c) { return c == nullptr ? 0 : c->last_launches; }
+
+int32_t bg_set_wait_budget(bg_ctx* c, int64_t iterations) {
+  if (c == nullptr || iterations < 0) return BG_EINVAL;
+  c->budget = iterations == 0 ? kDefaultBudget : iterations;
+  return BG_OK;
+}
+
+int32_t bg_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
+  if (c == nullptr) return BG_EINVAL;
+  cudaSetDevice(c->device);
+  int rc = validate(c, B, R);
+  if (rc != BG_OK) return rc;
+  rc = validate_world(c, B->capacity, R->count, R->starts, R->solved);
+  if (rc != BG_OK) return rc;
+  c->last_launches = 0;
+  if (!ensure(c, B->capacity, R->count, B->awake_count, 1)) return BG_ENOMEM;
+  c->nbodies = B->capacity;
+  c->nrows = R->count;
+  c->nawake = B->awake_count;
+  c->nworlds = 1;
+  c->batch = false;
+  bg::WorldDesc w = {};
+  w.body0 = 0; w.nbodies = B->capacity; w.awake0 = 0; w.nawake = B->awake_count;
+  w.row0 = 0; w.nrows = R->count; w.solved = R->solved;
+  for (int k = 0; k < bg::NSTARTS; k++) w.starts[k] = R->starts[k];
+  w.gravity[0] = 0; w.gravity[1] = 0; w.gravity[2] = 0;
+  c->worlds.assign(1, w);
+  rc = upload_columns(c, B, R, c->nbodies, c->nrows, c->nawake);
+  if (rc != BG_OK) return rc;
+  std::vector<int32_t> bo = {0, c->nbodies}, ao = {0, c->nawake}, ro = {0, c->nrows};
+  rc = upload_worlds(c, bo, ao, ro);
+  if (rc != BG_OK) return rc;
+  c->uploaded = true;
+  return unpack(c);
+}
+
+int32_t bg_restore(bg_ctx* c) {
+  if (c == nullptr || !c->uploaded) return BG_EINVAL;
+  cudaSetDevice(c->device);
+  c->last_launches = 0;
+  return unpack(c);
+}
+
+int32_t bg_solve(bg_ctx* c, const bg_step* step) {
+  if (c == nullptr || !c->uploaded) {
+    if (c) set_error(c, "solve: nothing uploaded");
+    return BG_EINVAL;
+  }
+  if (step == nullptr) return BG_EINVAL;
+  cudaSetDevice(c->device);
+  // The world's gravity is the step's (unless a batch gave each world its own).
+  if (!c->batch) {
+    for (int k = 0; k < 3; k++) c->worlds[0].gravity[k] = step->gravity[k];
+    if (!put(c, c->worlds_dev, c->worlds.data(), 1, "worlds")) return BG_ECUDA;
+  }
+  int rc = launch_stage(c, step);
+  if (rc != BG_OK) return rc;
+  return finish(c);
+}
+
+int32_t bg_download(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
+  if (c == nullptr || B == nullptr || R == nullptr) return BG_EINVAL;
+  cudaSetDevice(c->device);
+  return download_columns(c, B, R);
+}
+
+int32_t bg_solve_step(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_step* step) {
+  int rc = bg_upload(c, B, R);
+  if (rc != BG_OK) return rc;
+  rc = bg_solve(c, step);
+  if (rc != BG_OK) return rc;
+  return bg_download(c, B, R);
+}
+
+int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_worlds* W) {
+  if (c == nullptr) return BG_EINVAL;
+  cudaSetDevice(c->device);
+  int rc = validate(c, B, R);
+  if (rc != BG_OK) return rc;
+  if (W == nullptr || W->count < 1 || W->body_offset == nullptr || W->awake_offset == nullptr ||
+      W->row_offset == nullptr || W->starts == nullptr) {
+    set_error(c, "batch: worlds and their offsets must be given");
+    return BG_EINVAL;
+  }
+  const int nw = W->count;
+  if (W->body_offset[0] != 0 || W->awake_offset[0] != 0 || W->row_offset[0] != 0 || W->body_offset[nw] != B->capacity ||
+      W->awake_offset[nw] != B->awake_count || W->row_offset[nw] != R->count) {
+    set_error(c, "batch: offsets must start at 0 and end at the arrays' lengths");
+    return BG_EINVAL;
+  }
+  std::vector<bg::WorldDesc> worlds(static_cast<size_t>(nw));
+  for (int i = 0; i < nw; i++) {
+    bg::WorldDesc& w = worlds[static_cast<size_t>(i)];
+    w.body0 = W->body_offset[i];
+    w.nbodies = W->body_offset[i + 1] - W->body_offset[i];
+    w.awake0 = W->awake_offset[i];
+    w.nawake = W->awake_offset[i + 1] - W->awake_offset[i];
+    w.row0 = W->row_offset[i];
+    w.nrows = W->row_offset[i + 1] - W->row_offset[i];
+    if (w.nbodies < 0 || w.nawake < 0 || w.nrows < 0) {
+      set_error(c, "batch: offsets must not decrease");
+      return BG_EINVAL;
+    }
+    for (int k = 0; k < bg::NSTARTS; k++) w.starts[k] = W->starts[bg::NSTARTS * i + k];
+    w.solved = w.starts[bg::RESTING_RUN];
+    rc = validate_world(c, w.nbodies, w.nrows, w.starts, w.solved);
+    if (rc != BG_OK) return rc;
+    for (int k = 0; k < 3; k++) w.gravity[k] = W->gravity != nullptr ? W->gravity[3 * i + k] : NAN;
+  }
+  c->last_launches = 0;
+  if (!ensure(c, B->capacity, R->count, B->awake_count, nw)) return BG_ENOMEM;
+  c->nbodies = B->capacity;
+  c->nrows = R->count;
+  c->nawake = B->awake_count;
+  c->nworlds = nw;
+  c->batch = true;
+  c->worlds = worlds;
+  rc = upload_columns(c, B, R, c->nbodies, c->nrows, c->nawake);
+  if (rc != BG_OK) return rc;
+  std::vector<int32_t> bo(W->body_offset, W->body_offset + nw + 1), ao(W->awake_offset, W->awake_offset + nw + 1),
+      ro(W->row_offset, W->row_offset + nw + 1);
+  rc = upload_worlds(c, bo, ao, ro);
+  if (rc != BG_OK) return rc;
+  c->uploaded = true;
+  return unpack(c);
+}
+
+int32_t bg_batch_solve(bg_ctx* c, const bg_step* step) {
+  if (c == nullptr || !c->uploaded || !c->batch) {
+    if (c) set_error(c, "batch solve: no batch uploaded");
+    return BG_EINVAL;
+  }
+  if (step == nullptr) return BG_EINVAL;
+  cudaSetDevice(c->device);
+  bool changed = false;
+  for (auto& w : c->worlds)
+    if (w.gravity[0] != w.gravity[0]) {
+      for (int k = 0; k < 3; k++) w.gravity[k] = step->gravity[k];
+      changed = true;
+    }
+  if (changed) {
+    if (!put(c, c->worlds_dev, c->worlds.data(), c->worlds.size(), "worlds")) return BG_ECUDA;
+    if (!cuda_ok(c, cudaStreamSynchronize(c->stream), "worlds")) return BG_ECUDA;
+  }
+  int rc = launch_stage(c, step);
+  if (rc != BG_OK) return rc;
+  return finish(c);
+}
+
+int32_t bg_batch_download(bg_ctx* c, const bg_bodies* B, const bg_rows* R) { return bg_download(c, B, R); }
+
+int32_t bg_batch_solve_step(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_worlds* W, const bg_step* step) {
+  int rc = bg_batch_upload(c, B, R, W);
+  if (rc != BG_OK) return rc;
+  rc = bg_batch_solve(c, step);
+  if (rc != BG_OK) return rc;
+  return bg_batch_download(c, B, R);
+}
+
+}  // extern "C"

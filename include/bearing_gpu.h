@@ -60,6 +60,10 @@ extern "C" {
 #define BG_FLAG_NONE 0u
 /* Register the caller's host arrays as pinned on first use (cudaHostRegister) and keep them so. */
 #define BG_FLAG_PIN_HOST 1u
+/* Run every single world on the persistent grid (the path large worlds take), whatever its size. */
+#define BG_FLAG_GRID 2u
+/* Run every single world on one CTA (the path small and batched worlds take), whatever its size. */
+#define BG_FLAG_BLOCK 4u
 
 /* World body type codes: src/world.js TYPES (dynamic 0, static 1, kinematic 2, character 3). */
 #define BG_DYNAMIC 0

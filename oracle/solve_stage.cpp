@@ -200,15 +200,18 @@ class Pool {
     }
     const int chunks = (workers_ + 1) * 4;
     const int chunk = (n + chunks - 1) / chunks;
+    uint64_t epoch;
     {
       std::lock_guard<std::mutex> g(mu_);
       job_ = &job;
       from_ = from;
       count_ = n;
       chunk_ = chunk;
-      cursor_.store(0);
       completed_.store(0);
-      epoch_++;
+      epoch = ++epoch_;
+      // The cursor carries the dispatch's epoch (src/core/jobs.js:80-83): a worker still holding
+      // an earlier dispatch's arguments can never claim a chunk of this one.
+      cursor_.store(epoch << 32);
     }
     cv_.notify_all();
     claim();
@@ -221,18 +224,23 @@ class Pool {
   void claim() {
     const std::function<void(int, int)>* job;
     int from, count, chunk;
+    uint64_t epoch;
     {
       std::lock_guard<std::mutex> g(mu_);
       job = job_;
       from = from_;
       count = count_;
       chunk = chunk_;
+      epoch = epoch_;
     }
     if (job == nullptr) return;
     for (;;) {
-      const int index = cursor_.fetch_add(1);
+      uint64_t cursor = cursor_.load();
+      if ((cursor >> 32) != epoch) return;
+      const int index = static_cast<int>(cursor & 0xffffffffu);
       const int start = index * chunk;
       if (start >= count) return;
+      if (!cursor_.compare_exchange_weak(cursor, cursor + 1)) continue;
       const int end = start + chunk < count ? start + chunk : count;
       (*job)(from + start, from + end);
       completed_.fetch_add(end - start, std::memory_order_release);
@@ -258,7 +266,7 @@ class Pool {
   bool shutdown_ = false;
   const std::function<void(int, int)>* job_ = nullptr;
   int from_ = 0, count_ = 0, chunk_ = 1;
-  std::atomic<int> cursor_{0};
+  std::atomic<uint64_t> cursor_{0};
   std::atomic<int> completed_{0};
 };
 

@@ -1,0 +1,134 @@
+"""Copies of a solve stage's input, for running the same step through two solvers.
+
+``StageCopy(world)`` takes the solve stage's input as the world's host side left it (after
+``world.begin_step``) into numpy arrays of its own; ``views()`` gives bg_bodies / bg_rows /
+bg_step structures over those arrays, which the CUDA library and the oracle both accept.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from bearing_b200 import _ffi
+
+# (field, numpy dtype, numbers per slot)
+BODY_COLUMNS = [
+    ("position", np.float64, 3), ("rotation", np.float64, 4), ("velocity", np.float64, 3),
+    ("angular", np.float64, 3), ("tumbled", np.float64, 3), ("ceiling", np.float64, 1),
+    ("start", np.float64, 3), ("start_q", np.float64, 4), ("inv_i", np.float64, 6),
+    ("inv_mass", np.float64, 1), ("inertia", np.float64, 3), ("inv_inertia", np.float64, 3),
+    ("dims", np.float64, 3), ("damping", np.float64, 1), ("angular_damping", np.float64, 1),
+    ("gravity_scale", np.float64, 1), ("type", np.uint8, 1), ("shape", np.uint8, 1),
+    ("frozen", np.uint8, 1), ("framed", np.uint8, 1), ("lock", np.uint8, 1), ("joint_head", np.int32, 1),
+    ("awake", np.uint8, 1),
+]
+# (field, numpy dtype, numbers per row)
+ROW_COLUMNS = [
+    ("row", np.int32, 1), ("a", np.int32, 1), ("b", np.int32, 1), ("points", np.uint8, 1),
+    ("normal", np.float64, 3), ("t1", np.float64, 3), ("t2", np.float64, 3), ("friction", np.float64, 1),
+    ("restitution", np.float64, 1), ("tolerance", np.float64, 1), ("patch", np.float64, 1),
+    ("separation", np.float64, 4), ("point", np.float64, 12), ("shift", np.float64, 12),
+    ("normal_impulse", np.float64, 4), ("tangent_impulse1", np.float64, 1), ("tangent_impulse2", np.float64, 1),
+    ("roll_impulse1", np.float64, 1), ("roll_impulse2", np.float64, 1), ("spin_impulse", np.float64, 1),
+    ("drift1", np.float64, 1), ("drift2", np.float64, 1), ("gap", np.float64, 1),
+    ("max_normal_impulse", np.float64, 4), ("relative_velocity", np.float64, 4), ("sliding", np.uint8, 1),
+    ("anchor_a", np.float64, 3), ("anchor_b", np.float64, 3),
+]
+# What the solve stage writes.
+BODY_OUT = ["position", "rotation", "velocity", "angular", "tumbled", "ceiling", "start", "inv_i"]
+ROW_OUT = ["normal_impulse", "tangent_impulse1", "tangent_impulse2", "roll_impulse1", "roll_impulse2",
+           "spin_impulse", "drift1", "drift2", "gap", "max_normal_impulse", "relative_velocity"]
+# Written for solved rows only.
+ROW_OUT_SOLVED = ["sliding", "anchor_a", "anchor_b"]
+
+_CT = {np.float64: C.c_double, np.uint8: C.c_uint8, np.int32: C.c_int32}
+
+
+def _ptr(arr, dtype):
+    return arr.ctypes.data_as(C.POINTER(_CT[dtype]))
+
+
+def _read(ptr, n, dtype):
+    if n == 0:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True)
+
+
+class StageCopy:
+    """A solve stage's input, in arrays of its own."""
+
+    def __init__(self, world=None, *, arrays=None):
+        if arrays is not None:
+            self.__dict__.update(arrays)
+            return
+        B, R, S = world.views()
+        self.capacity = B.capacity
+        self.awake_count = B.awake_count
+        self.awake_list = _read(B.awake_list, B.awake_count, np.int32)
+        self.body = {f: _read(getattr(B, f), per * B.capacity, dt) for f, dt, per in BODY_COLUMNS}
+        self.count = R.count
+        self.solved = R.solved
+        self.starts = np.array(list(R.starts), dtype=np.int32)
+        self.rows = {f: _read(getattr(R, f), per * R.count, dt) for f, dt, per in ROW_COLUMNS}
+        self.dt = S.dt
+        self.substeps = S.substeps
+        self.gravity = tuple(S.gravity)
+
+    def copy(self):
+        return StageCopy(arrays=dict(
+            capacity=self.capacity, awake_count=self.awake_count, awake_list=self.awake_list.copy(),
+            body={k: v.copy() for k, v in self.body.items()}, count=self.count, solved=self.solved,
+            starts=self.starts.copy(), rows={k: v.copy() for k, v in self.rows.items()}, dt=self.dt,
+            substeps=self.substeps, gravity=self.gravity))
+
+    def views(self):
+        B = _ffi.Bodies()
+        B.capacity = self.capacity
+        B.awake_count = self.awake_count
+        B.awake_list = _ptr(self.awake_list, np.int32)
+        for f, dt, _ in BODY_COLUMNS:
+            setattr(B, f, _ptr(self.body[f], dt))
+        R = _ffi.Rows()
+        R.count = self.count
+        R.solved = self.solved
+        R.starts = (C.c_int32 * _ffi.BG_STARTS)(*[int(x) for x in self.starts])
+        for f, dt, _ in ROW_COLUMNS:
+            setattr(R, f, _ptr(self.rows[f], dt))
+        S = _ffi.Step(self.dt, self.substeps, (C.c_double * 3)(*self.gravity))
+        self._keep = (B, R, S)
+        return B, R, S
+
+
+def first_difference(a: StageCopy, b: StageCopy):
+    """None if every column the solve stage writes is bit-identical; else a description."""
+    for f in BODY_OUT:
+        x, y = a.body[f], b.body[f]
+        if x.tobytes() != y.tobytes():
+            i = int(np.flatnonzero(x.view(np.uint64) != y.view(np.uint64))[0])
+            return f"body {f}[{i}]: {x[i]!r} vs {y[i]!r}"
+    per = dict((f, p) for f, _, p in ROW_COLUMNS)
+    for f in ROW_OUT:
+        x, y = a.rows[f], b.rows[f]
+        if x.tobytes() != y.tobytes():
+            i = int(np.flatnonzero(x.view(np.uint64) != y.view(np.uint64))[0])
+            return f"row {f}[{i}] (row {i // per[f]}): {x[i]!r} vs {y[i]!r}"
+    n = a.solved
+    for f in ROW_OUT_SOLVED:
+        k = per[f]
+        x, y = a.rows[f][: k * n], b.rows[f][: k * n]
+        if x.tobytes() != y.tobytes():
+            i = int(np.flatnonzero(x.view(np.uint8 if x.dtype == np.uint8 else np.uint64)
+                                   != y.view(np.uint8 if y.dtype == np.uint8 else np.uint64))[0])
+            return f"row {f}[{i}] (row {i // k}): {x[i]!r} vs {y[i]!r}"
+    return None
+
+
+def max_relative_difference(a: StageCopy, b: StageCopy) -> float:
+    worst = 0.0
+    for f in BODY_OUT:
+        x, y = a.body[f], b.body[f]
+        d = np.abs(x - y) / np.maximum(1.0, np.maximum(np.abs(x), np.abs(y)))
+        if d.size:
+            worst = max(worst, float(np.nanmax(d)))
+    return worst
