@@ -225,6 +225,8 @@ struct bg_ctx {
   int grid_blocks = 0;
   long long budget = kDefaultBudget;
   int last_launches = 0;
+  cudaEvent_t stage_begin = nullptr, stage_end = nullptr;
+  bool stage_timed = false;
   // capacities
   int body_cap = 0, row_cap = 0, awake_cap = 0, world_cap = 0;
   // device allocations, all freed in bg_destroy
@@ -536,6 +538,7 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
   p.budget = c->budget;
   if (!cuda_ok(c, cudaMemsetAsync(c->status, 0, sizeof(int32_t), c->stream), "status")) return BG_ECUDA;
   c->last_launches += 1;
+  cudaEventRecord(c->stage_begin, c->stream);
   bool big = !c->batch && c->nworlds == 1 && c->worlds[0].solved >= kGridRows;
   if (!c->batch && (c->flags & BG_FLAG_GRID)) big = true;
   if (!c->batch && (c->flags & BG_FLAG_BLOCK)) big = false;
@@ -549,6 +552,8 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
     stage_block<<<blocks, kBlockThreads, 0, c->stream>>>(p);
     if (!cuda_ok(c, cudaGetLastError(), "stage_block launch")) return BG_ECUDA;
   }
+  cudaEventRecord(c->stage_end, c->stream);
+  c->stage_timed = true;
   return BG_OK;
 }
 
@@ -607,6 +612,8 @@ bg_ctx* bg_create(int32_t device, uint32_t flags) {
     return nullptr;
   }
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  cudaEventCreate(&c->stage_begin);
+  cudaEventCreate(&c->stage_end);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_grid, kGridThreads, 0);
   if (per_sm < 1) per_sm = 1;
@@ -620,6 +627,8 @@ void bg_destroy(bg_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_all(c);
+  if (c->stage_begin) cudaEventDestroy(c->stage_begin);
+  if (c->stage_end) cudaEventDestroy(c->stage_end);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -629,6 +638,15 @@ const char* bg_last_error(const bg_ctx* c) { return c == nullptr ? "no context" 
 void* bg_stream(bg_ctx* c) { return c == nullptr ? nullptr : static_cast<void*>(c->stream); }
 
 int32_t bg_last_launches(const bg_ctx* c) { return c == nullptr ? 0 : c->last_launches; }
+
+double bg_last_stage_ms(bg_ctx* c) {
+  if (c == nullptr || !c->stage_timed) return -1.0;
+  cudaSetDevice(c->device);
+  if (cudaEventSynchronize(c->stage_end) != cudaSuccess) return -1.0;
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, c->stage_begin, c->stage_end) != cudaSuccess) return -1.0;
+  return static_cast<double>(ms);
+}
 
 int32_t bg_set_wait_budget(bg_ctx* c, int64_t iterations) {
   if (c == nullptr || iterations < 0) return BG_EINVAL;

@@ -1,0 +1,352 @@
+"""Benchmark: the contact solve stage of a 50,000-body mixed pile at step 300, on one B200.
+
+A "step" here is one solve stage (src/world.js:962-1032: inertias, prepare, 8 substeps of
+accelerate / warm / solve / move / relax, restitution, slipped) over the pile's manifolds at
+step 301, the pile having been stepped 300 times first (host side of the step on the CPU, solve
+stage on the GPU).  Metric: contact rows/s = solved rows x substeps x 3 (warm, solve and relax
+row visits) / solve-stage seconds.
+
+  value     the solve stage with its input resident in HBM: bg_restore (untimed), an L2 flush
+            (untimed), then CUDA events around bg_solve on the library's stream
+  e2e       the same solve stage through bg_solve_step with host arrays: upload, solve and
+            download inside the timed region, events on the same stream
+  roofline  algorithmic bytes of one solve-stage kernel (counted from the rows' point counts by
+            the rule in algorithmic_bytes()) / that kernel's event-timed duration, against the
+            measured HBM copy bandwidth
+  cpu_baseline  the CPU restatement of the reference's solve stage on this box's host cores
+            (rank 0, N=1), on a bounded sample of the same input
+
+--impl reference times that CPU solve stage alone, with every host thread, as the reference arm.
+Under torchrun each rank solves its own replica of the pile (the solve stage of one world does
+not shard: replicas only); value is the sum over ranks, time the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT = 1 / 60
+SUBSTEPS = 8
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--bodies", type=int, default=50_000)
+    p.add_argument("--at", type=int, default=300, help="steps taken before the timed solve stage")
+    p.add_argument("--cpu-sample", type=int, default=2, help="solve stages the CPU baseline times")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+# ---- the workload -------------------------------------------------------------------------
+
+def build_pile(solver, bodies, at, log=None):
+    """The pile stepped `at` times with `solver`, then the host side of step at+1."""
+    from bearing_b200 import scenes
+    from bearing_b200.world import World
+    w = World({}, solver=solver)
+    scenes.pile(w, count=bodies, seed=50_000)
+    t0 = time.time()
+    for i in range(at):
+        w.step(DT)
+        if log and (i + 1) % 50 == 0:
+            log(f"step {i + 1}: {w.stats()} ({time.time() - t0:.0f} s)")
+    w.begin_step(DT)
+    return w
+
+
+def algorithmic_bytes(copy):
+    """Bytes one solve stage must move at least: each column a pass needs read once and each
+    column it writes written once, per row per pass, at the widths the rows are kept in, plus the
+    two bodies' records each row reads and writes, plus the per-body passes.  FP64 = 8 bytes.
+
+      warm    per row 521 + 56 n        (n = the row's points)
+      solve   per row 754 + 160 n + 8 n^2, and 160 + 48 n more where the separation is not
+              known (first substep) and in relax, which writes it (8 n)
+      prepare per row 560 + 256 n + 8 n^2
+      bodies  per awake body: 200 once, then 124 (accelerate) + 300 (move) a substep
+      slipped per row 289 + 32 n
+    """
+    import numpy as np
+    pts = copy.rows["points"][: copy.solved].astype(np.int64)
+    n1 = int(pts.sum())
+    n2 = int((pts * pts).sum())
+    rows = copy.solved
+    warm = 521 * rows + 56 * n1
+    solve_known = 754 * rows + 160 * n1 + 8 * n2
+    solve_fresh = solve_known + 160 * rows + 48 * n1
+    relax = solve_fresh + 8 * n1
+    prepare = 560 * rows + 256 * n1 + 8 * n2
+    slipped = 289 * rows + 32 * n1
+    body = copy.awake_count * (200 + SUBSTEPS * (124 + 300))
+    total = prepare + SUBSTEPS * (warm + relax) + solve_fresh + (SUBSTEPS - 1) * solve_known + slipped + body
+    return int(total)
+
+
+# ---- clocks -------------------------------------------------------------------------------
+
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples if len(s) >= 9 for k in range(4)
+                          if s[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---- timing -------------------------------------------------------------------------------
+
+def time_resident(lib, ctx, copy, steps, warmup, torch):
+    """bg_solve over the uploaded input: restore and flush untimed, events around the solve."""
+    from bearing_b200 import _ffi
+    B, R, S = copy.views()
+    rc = lib.bg_upload(ctx, C.byref(B), C.byref(R))
+    assert rc == 0, lib.bg_last_error(ctx)
+    stream = torch.cuda.ExternalStream(lib.bg_stream(ctx))
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
+    times, stage, launches = [], [], 0
+    for i in range(warmup + steps):
+        assert lib.bg_restore(ctx) == 0
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        before = lib.bg_last_launches(ctx)
+        e0.record(stream)
+        rc = lib.bg_solve(ctx, C.byref(S))
+        e1.record(stream)
+        assert rc == 0, lib.bg_last_error(ctx)
+        e1.synchronize()
+        if i >= warmup:
+            times.append(e0.elapsed_time(e1))
+            stage.append(lib.bg_last_stage_ms(ctx))
+            launches += lib.bg_last_launches(ctx) - before
+    # The result of the last timed solve, checked for completion (a lost step raises).
+    out = copy.copy()
+    Bo, Ro, _ = out.views()
+    rc = lib.bg_download(ctx, C.byref(Bo), C.byref(Ro))
+    assert rc == 0, lib.bg_last_error(ctx)
+    return times, stage, launches, out
+
+
+def time_e2e(lib, ctx, copy, steps, warmup, torch):
+    """bg_solve_step with host arrays: uploads, solve and downloads inside the timed region."""
+    stream = torch.cuda.ExternalStream(lib.bg_stream(ctx))
+    times = []
+    for i in range(warmup + steps):
+        work = copy.copy()
+        B, R, S = work.views()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = lib.bg_solve_step(ctx, C.byref(B), C.byref(R), C.byref(S))
+        e1.record(stream)
+        assert rc == 0, lib.bg_last_error(ctx)
+        e1.synchronize()
+        if i >= warmup:
+            times.append(e0.elapsed_time(e1))
+    return times
+
+
+def io_bytes(copy):
+    """Bytes bg_solve_step copies in and out per step, from the columns it moves."""
+    from stage_io import BODY_COLUMNS, ROW_COLUMNS, BODY_OUT, ROW_OUT, ROW_OUT_SOLVED
+    import numpy as np
+    h2d_body = [f for f, _, _ in BODY_COLUMNS if f not in ("start_q",)]
+    h2d_row = [f for f, _, _ in ROW_COLUMNS if f not in ("sliding", "anchor_a", "anchor_b")]
+    h2d = sum(copy.body[f].nbytes for f in h2d_body) + copy.awake_list.nbytes + sum(copy.rows[f].nbytes for f in h2d_row)
+    d2h_body = BODY_OUT + ["start_q"]
+    d2h = sum(copy.body[f].nbytes for f in d2h_body) + sum(copy.rows[f].nbytes for f in ROW_OUT + ROW_OUT_SOLVED)
+    return int(h2d), int(d2h)
+
+
+def cpu_solve_times(copy, workers, sample):
+    """The CPU restatement of the reference's solve stage, timed on `sample` solve stages."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_io
+    times = []
+    for _ in range(sample):
+        work = copy.copy()
+        t0 = time.perf_counter()
+        oracle_io.solve(work, workers)
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---- main ---------------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    log = (lambda s: print(f"[bench] {s}", file=sys.stderr, flush=True)) if rank == 0 else None
+
+    config = {"workload": f"{args.bodies}-body mixed pile (60% boxes, 25% spheres, 15% capsules), solve stage "
+                          f"at step {args.at + 1}", "bodies": args.bodies, "at_step": args.at + 1,
+              "substeps": SUBSTEPS, "dt": DT, "l2": "flushed between timed iterations (256 MB write)",
+              "parallelism": f"replicas x{args.gpus}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from stage_io import StageCopy
+        import oracle_io
+        threads = host_threads()
+        workers = max(0, threads - 1)
+        w = build_pile(oracle_io.solver(workers), args.bodies, args.at, log)
+        copy = StageCopy(w)
+        rows_per_stage = copy.solved * SUBSTEPS * 3
+        cpu_solve_times(copy, workers, 1)
+        times = []
+        for _ in range(args.warmup):
+            cpu_solve_times(copy, workers, 1)
+        for _ in range(args.steps):
+            times += cpu_solve_times(copy, workers, 1)
+        sec = statistics.mean(times)
+        value = rows_per_stage / sec
+        line = {"metric": "contact rows/s", "value": value, "unit": "rows/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1000, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                "impl": "reference", "config": dict(config, rows=copy.solved, cpu_threads=threads),
+                "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
+                                 "sample": f"{args.steps} solve stages of the step-{args.at + 1} input, "
+                                           f"{workers} workers + the calling thread (src/core/jobs.js split)"},
+                "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world_size > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    from bearing_b200 import _ffi
+    from bearing_b200.world import GpuSolver
+    from stage_io import StageCopy
+    lib = _ffi.gpu()
+    solver = GpuSolver(local)
+    t0 = time.time()
+    w = build_pile(solver, args.bodies, args.at, log)
+    if log:
+        log(f"pile built to step {args.at} in {time.time() - t0:.0f} s: {w.stats()}")
+    copy = StageCopy(w)
+    ctx = lib.bg_create(local, 0)
+    assert ctx, "bg_create failed"
+    h2d, d2h = io_bytes(copy)
+    algo = algorithmic_bytes(copy)
+    clocks = Clocks(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    times, stage, launches, out = time_resident(lib, ctx, copy, args.steps, args.warmup, torch)
+    clock = clocks.stop()
+    e2e_times = time_e2e(lib, ctx, copy, args.steps, args.warmup, torch)
+    torch.cuda.synchronize()
+    ms = statistics.mean(times)
+    ms_e2e = statistics.mean(e2e_times)
+    ms_stage = statistics.mean(stage)
+    if dist:
+        t = torch.tensor([ms, ms_e2e, ms_stage], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e, ms_stage = (float(x) for x in t.tolist())
+    rows_per_stage = copy.solved * SUBSTEPS * 3
+    value = world_size * rows_per_stage / (ms / 1000)
+    e2e = world_size * rows_per_stage / (ms_e2e / 1000)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = algo / (ms_stage / 1000) / 1e9
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu:
+        threads = host_threads()
+        t1 = cpu_solve_times(copy, 0, args.cpu_sample)
+        cpu = {"value": rows_per_stage / statistics.mean(t1), "unit": "rows/s", "cores": 1, "kind": "port",
+               "sample": f"{args.cpu_sample} solve stages of the step-{args.at + 1} input "
+                         f"({copy.solved} rows), 1 thread",
+               "threads_available": threads}
+        if threads > 1:
+            tn = cpu_solve_times(copy, threads - 1, args.cpu_sample)
+            cpu["all_threads"] = {"value": rows_per_stage / statistics.mean(tn), "cores": threads}
+    if rank == 0:
+        line = {"metric": "contact rows/s", "value": value, "unit": "rows/s", "n_gpus": world_size,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                "config": dict(config, rows=copy.solved, points=int(copy.rows["points"][:copy.solved].sum()),
+                               colours=int(sum(1 for k in range(32) if copy.starts[k + 1] > copy.starts[k])),
+                               overflow=int(copy.starts[33] - copy.starts[32]), awake=copy.awake_count),
+                "e2e": {"value": e2e, "unit": "rows/s", "ms_per_step": ms_e2e, "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                             "frac": achieved / hbm, "traffic": None, "kernel_ms": ms_stage,
+                             "algorithmic_bytes": algo, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    lib.bg_destroy(ctx)
+    solver.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

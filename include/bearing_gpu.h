@@ -206,8 +206,11 @@ int32_t bg_batch_download(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* r
 
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
 void* bg_stream(bg_ctx* ctx);
-/* Kernel launches issued by the last bg_solve / bg_batch_solve (for launch accounting). */
+/* Kernel launches issued since the last bg_upload / bg_restore (for launch accounting). */
 int32_t bg_last_launches(const bg_ctx* ctx);
+/* Device time, in milliseconds, of the last solve-stage kernel (CUDA events recorded around it
+ * on the context's stream); synchronises.  Negative if none has run. */
+double bg_last_stage_ms(bg_ctx* ctx);
 /* Grid barriers each colour pass waits at, and the spin budget (iterations) of each wait.
  * 0 restores the default.  A wait past its budget makes the step return BG_ETIMEOUT. */
 int32_t bg_set_wait_budget(bg_ctx* ctx, int64_t iterations);
