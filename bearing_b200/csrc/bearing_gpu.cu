@@ -110,47 +110,49 @@ __global__ void unpack_bodies(BodyStage in, bg::BodiesDev B, int n, const int32_
   }
 }
 
+// Device row m holds the caller's row perm[m] (rows of one colour sorted by point count, see
+// order_rows()); the found-order list maps to device rows through iperm.
 __global__ void unpack_rows(RowStage in, bg::RowsDev R, int n, const int32_t* row_offset, const int32_t* body_offset,
-                            int nworlds, const double* maxni_in, const double* relvel_in, const double* gap_in) {
+                            int nworlds, const double* maxni_in, const double* relvel_in, const double* gap_in,
+                            const int32_t* perm, const int32_t* iperm) {
   const int64_t cap = R.cap;
   const int stride = gridDim.x * blockDim.x;
-  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += stride) {
-    int r0 = 0, b0 = 0;
-    if (nworlds > 1) {
-      const int w = world_of(row_offset, nworlds, m);
-      r0 = row_offset[w];
-      b0 = body_offset[w];
-    }
-    R.row[m] = in.row[m] + r0;
-    R.a[m] = in.a[m] + b0;
-    R.b[m] = in.b[m] + b0;
-    R.points[m] = in.points[m];
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < n; f += stride) {
+    int r0 = 0;
+    if (nworlds > 1) r0 = row_offset[world_of(row_offset, nworlds, f)];
+    R.row[f] = iperm[in.row[f] + r0];
+  }
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += stride) {
+    const int m = perm[d];
+    int b0 = 0;
+    if (nworlds > 1) b0 = body_offset[world_of(row_offset, nworlds, m)];
+    R.a[d] = in.a[m] + b0;
+    R.b[d] = in.b[m] + b0;
+    R.points[d] = in.points[m];
     for (int c = 0; c < 3; c++) {
-      R.n[c * cap + m] = in.normal[3 * m + c];
-      R.t1[c * cap + m] = in.t1[3 * m + c];
-      R.t2[c * cap + m] = in.t2[3 * m + c];
+      R.n[c * cap + d] = in.normal[3 * m + c];
+      R.t1[c * cap + d] = in.t1[3 * m + c];
+      R.t2[c * cap + d] = in.t2[3 * m + c];
     }
-    R.friction[m] = in.friction[m];
-    R.restitution[m] = in.restitution[m];
-    R.tolerance[m] = in.tolerance[m];
-    R.patch[m] = in.patch[m];
-    // What the stage does not write (the resting run, and point slots past a row's count) is
-    // handed back as the caller gave it.
-    R.gap[m] = gap_in[m];
-    R.sliding[m] = 0;
-    for (int c = 0; c < 3; c++) { R.anchorA[c * cap + m] = 0; R.anchorB[c * cap + m] = 0; }
+    R.friction[d] = in.friction[m];
+    R.restitution[d] = in.restitution[m];
+    R.tolerance[d] = in.tolerance[m];
+    R.patch[d] = in.patch[m];
+    R.gap[d] = gap_in[m];
+    R.sliding[d] = 0;
+    for (int c = 0; c < 3; c++) { R.anchorA[c * cap + d] = 0; R.anchorB[c * cap + d] = 0; }
     for (int k = 0; k < bg::P; k++) {
-      R.maxni[k * cap + m] = maxni_in[bg::P * m + k];
-      R.relvel[k * cap + m] = relvel_in[bg::P * m + k];
-      R.separation[k * cap + m] = in.separation[bg::P * m + k];
-      R.ni[k * cap + m] = in.normal_impulse[bg::P * m + k];
+      R.maxni[k * cap + d] = maxni_in[bg::P * m + k];
+      R.relvel[k * cap + d] = relvel_in[bg::P * m + k];
+      R.separation[k * cap + d] = in.separation[bg::P * m + k];
+      R.ni[k * cap + d] = in.normal_impulse[bg::P * m + k];
       for (int c = 0; c < 3; c++) {
-        R.point[(k * 3 + c) * cap + m] = in.point[12 * m + 3 * k + c];
-        R.shift[(k * 3 + c) * cap + m] = in.shift[12 * m + 3 * k + c];
+        R.point[(k * 3 + c) * cap + d] = in.point[12 * m + 3 * k + c];
+        R.shift[(k * 3 + c) * cap + d] = in.shift[12 * m + 3 * k + c];
       }
     }
-    R.ti1[m] = in.ti1[m]; R.ti2[m] = in.ti2[m]; R.ri1[m] = in.ri1[m]; R.ri2[m] = in.ri2[m];
-    R.si[m] = in.si[m]; R.drift1[m] = in.drift1[m]; R.drift2[m] = in.drift2[m];
+    R.ti1[d] = in.ti1[m]; R.ti2[d] = in.ti2[m]; R.ri1[d] = in.ri1[m]; R.ri2[d] = in.ri2[m];
+    R.si[d] = in.si[m]; R.drift1[d] = in.drift1[m]; R.drift2[d] = in.drift2[m];
   }
 }
 
@@ -170,22 +172,23 @@ __global__ void pack_bodies(bg::BodiesDev B, BodyOut out, int n) {
   }
 }
 
-__global__ void pack_rows(bg::RowsDev R, RowOut out, int n) {
+__global__ void pack_rows(bg::RowsDev R, RowOut out, int n, const int32_t* perm) {
   const int64_t cap = R.cap;
   const int stride = gridDim.x * blockDim.x;
-  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += stride) {
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += stride) {
+    const int m = perm[d];
     for (int k = 0; k < bg::P; k++) {
-      out.normal_impulse[bg::P * m + k] = R.ni[k * cap + m];
-      out.maxni[bg::P * m + k] = R.maxni[k * cap + m];
-      out.relvel[bg::P * m + k] = R.relvel[k * cap + m];
+      out.normal_impulse[bg::P * m + k] = R.ni[k * cap + d];
+      out.maxni[bg::P * m + k] = R.maxni[k * cap + d];
+      out.relvel[bg::P * m + k] = R.relvel[k * cap + d];
     }
-    out.ti1[m] = R.ti1[m]; out.ti2[m] = R.ti2[m]; out.ri1[m] = R.ri1[m]; out.ri2[m] = R.ri2[m];
-    out.si[m] = R.si[m]; out.drift1[m] = R.drift1[m]; out.drift2[m] = R.drift2[m];
-    out.gap[m] = R.gap[m];
-    out.sliding[m] = R.sliding[m];
+    out.ti1[m] = R.ti1[d]; out.ti2[m] = R.ti2[d]; out.ri1[m] = R.ri1[d]; out.ri2[m] = R.ri2[d];
+    out.si[m] = R.si[d]; out.drift1[m] = R.drift1[d]; out.drift2[m] = R.drift2[d];
+    out.gap[m] = R.gap[d];
+    out.sliding[m] = R.sliding[d];
     for (int c = 0; c < 3; c++) {
-      out.anchor_a[3 * m + c] = R.anchorA[c * cap + m];
-      out.anchor_b[3 * m + c] = R.anchorB[c * cap + m];
+      out.anchor_a[3 * m + c] = R.anchorA[c * cap + d];
+      out.anchor_b[3 * m + c] = R.anchorB[c * cap + d];
     }
   }
 }
@@ -241,6 +244,10 @@ struct bg_ctx {
   double* maxni_in = nullptr;
   double* relvel_in = nullptr;
   double* gap_in = nullptr;
+  // device row d holds the caller's row perm[d]; iperm the other way (see order_rows)
+  int32_t* perm_dev = nullptr;
+  int32_t* iperm_dev = nullptr;
+  std::vector<int32_t> perm, iperm;
   // staging out
   BodyOut bout = {};
   RowOut rout = {};
@@ -365,7 +372,7 @@ bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
        dev_alloc(c, &shift, 12 * nr) && dev_alloc(c, &ni, 4 * nr) && dev_alloc(c, &ti1, nr) && dev_alloc(c, &ti2, nr) &&
        dev_alloc(c, &ri1, nr) && dev_alloc(c, &ri2, nr) && dev_alloc(c, &si, nr) && dev_alloc(c, &drift1, nr) &&
        dev_alloc(c, &drift2, nr) && dev_alloc(c, &c->maxni_in, 4 * nr) && dev_alloc(c, &c->relvel_in, 4 * nr) &&
-       dev_alloc(c, &c->gap_in, nr);
+       dev_alloc(c, &c->gap_in, nr) && dev_alloc(c, &c->perm_dev, nr) && dev_alloc(c, &c->iperm_dev, nr);
   if (!ok) return false;
   ri = RowStage{row, a, b, points, normal, t1, t2, friction, restitution, tolerance, patch, separation, point, shift,
                 ni, ti1, ti2, ri1, ri2, si, drift1, drift2};
@@ -487,13 +494,43 @@ int upload_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R, int nb, int 
   return ok ? BG_OK : BG_ECUDA;
 }
 
+// The order rows are solved in on the device: within each colour, rows by point count (a
+// colour's rows share no body the solve moves, so their order changes no result, src/graph.js:1-33),
+// which keeps a warp's 32 rows on one code path.  The overflow and resting runs keep their order
+// (the overflow is solved in row order, src/contact.js:1794-1795).
+int order_rows(bg_ctx* c, const uint8_t* points) {
+  const int n = c->nrows;
+  c->perm.resize(static_cast<size_t>(n));
+  c->iperm.resize(static_cast<size_t>(n));
+  for (const bg::WorldDesc& w : c->worlds) {
+    for (int k = 0; k < bg::NSTARTS - 1; k++) {
+      const int from = w.starts[k], to = k < bg::RESTING_RUN ? w.starts[k + 1] : w.nrows;
+      if (to <= from) continue;
+      if (k >= bg::OVERFLOW_RUN) {
+        for (int m = from; m < to; m++) c->perm[static_cast<size_t>(w.row0 + m)] = w.row0 + m;
+        continue;
+      }
+      int at = from;
+      for (int count = 1; count <= bg::P; count++)
+        for (int m = from; m < to; m++) {
+          const int pc = points[w.row0 + m] < 1 ? 1 : points[w.row0 + m] > bg::P ? bg::P : points[w.row0 + m];
+          if (pc == count) c->perm[static_cast<size_t>(w.row0 + at++)] = w.row0 + m;
+        }
+    }
+  }
+  for (int d = 0; d < n; d++) c->iperm[static_cast<size_t>(c->perm[static_cast<size_t>(d)])] = d;
+  bool ok = put(c, c->perm_dev, c->perm.data(), static_cast<size_t>(n), "perm") &&
+            put(c, c->iperm_dev, c->iperm.data(), static_cast<size_t>(n), "iperm");
+  return ok ? BG_OK : BG_ECUDA;
+}
+
 int unpack(bg_ctx* c) {
   const int nb = c->nbodies, nr = c->nrows, na = c->nawake;
   const int blocks = std::max(1, std::min(4 * c->sms, (std::max(nb, std::max(nr, na)) + kUnpackThreads - 1) / kUnpackThreads));
   unpack_bodies<<<blocks, kUnpackThreads, 0, c->stream>>>(c->bin, c->B, nb, c->awake_in, na, c->body_offset_dev,
                                                          c->awake_offset_dev, c->nworlds);
   unpack_rows<<<blocks, kUnpackThreads, 0, c->stream>>>(c->rin, c->R, nr, c->row_offset_dev, c->body_offset_dev, c->nworlds,
-                                                       c->maxni_in, c->relvel_in, c->gap_in);
+                                                       c->maxni_in, c->relvel_in, c->gap_in, c->perm_dev, c->iperm_dev);
   c->last_launches += 2;
   return cuda_ok(c, cudaGetLastError(), "unpack") ? BG_OK : BG_ECUDA;
 }
@@ -561,7 +598,7 @@ int finish(bg_ctx* c) {
   const int nb = c->nbodies, nr = c->nrows;
   const int blocks = std::max(1, std::min(4 * c->sms, (std::max(nb, nr) + kUnpackThreads - 1) / kUnpackThreads));
   pack_bodies<<<blocks, kUnpackThreads, 0, c->stream>>>(c->B, c->bout, nb);
-  pack_rows<<<blocks, kUnpackThreads, 0, c->stream>>>(c->R, c->rout, nr);
+  pack_rows<<<blocks, kUnpackThreads, 0, c->stream>>>(c->R, c->rout, nr, c->perm_dev);
   c->last_launches += 2;
   return cuda_ok(c, cudaGetLastError(), "pack") ? BG_OK : BG_ECUDA;
 }
@@ -617,7 +654,10 @@ bg_ctx* bg_create(int32_t device, uint32_t flags) {
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_grid, kGridThreads, 0);
   if (per_sm < 1) per_sm = 1;
-  c->grid_blocks = c->sms * per_sm;
+  // One block an SM: every colour's rows are spread over all of them (GridTeam::each), and fewer
+  // blocks make each grid barrier cheaper.
+  (void)per_sm;
+  c->grid_blocks = c->sms;
   if (c->grid_blocks > 1024) c->grid_blocks = 1024;
   return c;
 }
@@ -675,6 +715,8 @@ int32_t bg_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
   w.gravity[0] = 0; w.gravity[1] = 0; w.gravity[2] = 0;
   c->worlds.assign(1, w);
   rc = upload_columns(c, B, R, c->nbodies, c->nrows, c->nawake);
+  if (rc != BG_OK) return rc;
+  rc = order_rows(c, R->points);
   if (rc != BG_OK) return rc;
   std::vector<int32_t> bo = {0, c->nbodies}, ao = {0, c->nawake}, ro = {0, c->nrows};
   rc = upload_worlds(c, bo, ao, ro);
@@ -765,6 +807,8 @@ int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const b
   c->batch = true;
   c->worlds = worlds;
   rc = upload_columns(c, B, R, c->nbodies, c->nrows, c->nawake);
+  if (rc != BG_OK) return rc;
+  rc = order_rows(c, R->points);
   if (rc != BG_OK) return rc;
   std::vector<int32_t> bo(W->body_offset, W->body_offset + nw + 1), ao(W->awake_offset, W->awake_offset + nw + 1),
       ro(W->row_offset, W->row_offset + nw + 1);

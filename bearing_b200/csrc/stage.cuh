@@ -179,6 +179,17 @@ struct GridTeam {
   __device__ GridTeam() : rank(blockIdx.x * blockDim.x + threadIdx.x), size(gridDim.x * blockDim.x), lead(blockIdx.x == 0) {}
   __device__ bool sync(const StageParams& p) const { return grid_barrier(p); }
   __device__ int lane_in_lead() const { return threadIdx.x; }
+  // Items from..to-1 spread over every block, each block a contiguous share, so a colour's rows
+  // reach every SM however few there are.
+  template <class F>
+  __device__ void each(int from, int to, F f) const {
+    const int n = to - from;
+    if (n <= 0) return;
+    const int per = (n + static_cast<int>(gridDim.x) - 1) / static_cast<int>(gridDim.x);
+    const int lo = from + static_cast<int>(blockIdx.x) * per;
+    const int hi = min(to, lo + per);
+    for (int m = lo + static_cast<int>(threadIdx.x); m < hi; m += blockDim.x) f(m);
+  }
 };
 
 struct BlockTeam {
@@ -188,6 +199,10 @@ struct BlockTeam {
   __device__ BlockTeam() : rank(threadIdx.x), size(blockDim.x), lead(true) {}
   __device__ bool sync(const StageParams&) const { __syncthreads(); return true; }
   __device__ int lane_in_lead() const { return threadIdx.x; }
+  template <class F>
+  __device__ void each(int from, int to, F f) const {
+    for (int m = from + static_cast<int>(threadIdx.x); m < to; m += blockDim.x) f(m);
+  }
 };
 
 // ---- bodies ----
@@ -564,50 +579,64 @@ __device__ __forceinline__ void write_back(const BodiesDev& B, double im, int s,
   stm(vw, vx); stm(vw + 1, vy); stm(vw + 2, vz); stm(vw + 3, wx); stm(vw + 4, wy); stm(vw + 5, wz);
 }
 
-// warmRows for row m: src/contact.js:1616-1663.
-__device__ void warm_row(const StageParams& p, int m) {
+// warmRows for row m: src/contact.js:1616-1663, for a row of N points.  Every array index below
+// is known at compile time, so nothing goes to local memory.
+template <int N>
+__device__ __forceinline__ void warm_row_n(const StageParams& p, int m) {
   const RowsDev& R = p.R;
   const BodiesDev& B = p.B;
   const int64_t cap = R.cap;
   const int a = ldi(R.a + m), b = ldi(R.b + m);
+  // every load first: the row's own columns, then its two bodies
+  const double nx = ldi(R.n + m), ny = ldi(R.n + cap + m), nz = ldi(R.n + 2 * cap + m);
+  const double t1x = ldi(R.t1 + m), t1y = ldi(R.t1 + cap + m), t1z = ldi(R.t1 + 2 * cap + m);
+  const double t2x = ldi(R.t2 + m), t2y = ldi(R.t2 + cap + m), t2z = ldi(R.t2 + 2 * cap + m);
+  double ln[N], ia[N][3], ib[N][3];
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    ln[k] = ldm(R.ni + k * cap + m);
+    const double* jac = R.jac + (k * J) * cap + m;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      ia[k][c] = ldm(jac + (6 + c) * cap);
+      ib[k][c] = ldm(jac + (9 + c) * cap);
+    }
+  }
+  double fa[6], fb[6];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    fa[c] = ldm(R.fjac + (6 + c) * cap + m);
+    fa[3 + c] = ldm(R.fjac + (18 + c) * cap + m);
+    fb[c] = ldm(R.fjac + (9 + c) * cap + m);
+    fb[3 + c] = ldm(R.fjac + (21 + c) * cap + m);
+  }
+  const double l1 = ldm(R.ti1 + m), l2 = ldm(R.ti2 + m);
+  const double r1 = ldm(R.ri1 + m), r2 = ldm(R.ri2 + m), sp = ldm(R.si + m);
   BodyLoad A, Bb;
   load_mass(B, a, A);
   load_mass(B, b, Bb);
   const double ima = A.im, imb = Bb.im;
-  const double nx = ldi(R.n + m), ny = ldi(R.n + cap + m), nz = ldi(R.n + 2 * cap + m);
-  const double t1x = ldi(R.t1 + m), t1y = ldi(R.t1 + cap + m), t1z = ldi(R.t1 + 2 * cap + m);
-  const double t2x = ldi(R.t2 + m), t2y = ldi(R.t2 + cap + m), t2z = ldi(R.t2 + 2 * cap + m);
   const double* va = B.vw + 8 * a;
   const double* vb = B.vw + 8 * b;
   double vax = ldm(va), vay = ldm(va + 1), vaz = ldm(va + 2), wax = ldm(va + 3), way = ldm(va + 4), waz = ldm(va + 5);
   double vbx = ldm(vb), vby = ldm(vb + 1), vbz = ldm(vb + 2), wbx = ldm(vb + 3), wby = ldm(vb + 4), wbz = ldm(vb + 5);
-  const int count = ldi(R.points + m);
 #pragma unroll
-  for (int k = 0; k < P; k++) {
-    if (k >= count) break;
-    const double ln = ldm(R.ni + k * cap + m);
-    const double* jac = R.jac + (k * J) * cap + m;
-    const double px = nx * ln, py = ny * ln, pz = nz * ln;
+  for (int k = 0; k < N; k++) {
+    const double l = ln[k];
+    const double px = nx * l, py = ny * l, pz = nz * l;
     vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
     vbx += imb * px; vby += imb * py; vbz += imb * pz;
-    wax -= ldm(jac + 6 * cap) * ln; way -= ldm(jac + 7 * cap) * ln; waz -= ldm(jac + 8 * cap) * ln;
-    wbx += ldm(jac + 9 * cap) * ln; wby += ldm(jac + 10 * cap) * ln; wbz += ldm(jac + 11 * cap) * ln;
+    wax -= ia[k][0] * l; way -= ia[k][1] * l; waz -= ia[k][2] * l;
+    wbx += ib[k][0] * l; wby += ib[k][1] * l; wbz += ib[k][2] * l;
   }
   {
-    const double* fj = R.fjac + m;
-    const double l1 = ldm(R.ti1 + m), l2 = ldm(R.ti2 + m);
     const double px = t1x * l1 + t2x * l2, py = t1y * l1 + t2y * l2, pz = t1z * l1 + t2z * l2;
     vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
     vbx += imb * px; vby += imb * py; vbz += imb * pz;
-    wax -= ldm(fj + 6 * cap) * l1 + ldm(fj + 18 * cap) * l2;
-    way -= ldm(fj + 7 * cap) * l1 + ldm(fj + 19 * cap) * l2;
-    waz -= ldm(fj + 8 * cap) * l1 + ldm(fj + 20 * cap) * l2;
-    wbx += ldm(fj + 9 * cap) * l1 + ldm(fj + 21 * cap) * l2;
-    wby += ldm(fj + 10 * cap) * l1 + ldm(fj + 22 * cap) * l2;
-    wbz += ldm(fj + 11 * cap) * l1 + ldm(fj + 23 * cap) * l2;
+    wax -= fa[0] * l1 + fa[3] * l2; way -= fa[1] * l1 + fa[4] * l2; waz -= fa[2] * l1 + fa[5] * l2;
+    wbx += fb[0] * l1 + fb[3] * l2; wby += fb[1] * l1 + fb[4] * l2; wbz += fb[2] * l1 + fb[5] * l2;
   }
   {
-    const double r1 = ldm(R.ri1 + m), r2 = ldm(R.ri2 + m), sp = ldm(R.si + m);
     const double* Ia = A.I;
     const double* Ib = Bb.I;
     const double lx = t1x * r1 + t2x * r2 + nx * sp, ly = t1y * r1 + t2y * r2 + ny * sp, lz = t1z * r1 + t2z * r2 + nz * sp;
@@ -622,60 +651,81 @@ __device__ void warm_row(const StageParams& p, int m) {
   write_back(B, imb, b, vbx, vby, vbz, wbx, wby, wbz);
 }
 
-// pushes: src/contact.js:1672-1724.
-__device__ __forceinline__ void pushes(const double* K, int count, int set, const double* give, const double* wanted,
-                                       double* solved) {
-  if (set == 15) {
-    const double g0 = 1 + give[0], g1 = 1 + give[1], g2 = 1 + give[2], g3 = 1 + give[3];
-    double a00 = K[0] * g0, a01 = K[1], a02 = K[2], a03 = K[3];
-    double a10 = K[4], a11 = K[5] * g1, a12 = K[6], a13 = K[7];
-    double a20 = K[8], a21 = K[9], a22 = K[10] * g2, a23 = K[11];
-    double a30 = K[12], a31 = K[13], a32 = K[14], a33 = K[15] * g3;
-    double r0 = wanted[0], r1 = wanted[1], r2 = wanted[2], r3 = wanted[3], f;
-    f = a10 / a00; a11 -= f * a01; a12 -= f * a02; a13 -= f * a03; r1 -= f * r0;
-    f = a20 / a00; a21 -= f * a01; a22 -= f * a02; a23 -= f * a03; r2 -= f * r0;
-    f = a30 / a00; a31 -= f * a01; a32 -= f * a02; a33 -= f * a03; r3 -= f * r0;
-    f = a21 / a11; a22 -= f * a12; a23 -= f * a13; r2 -= f * r1;
-    f = a31 / a11; a32 -= f * a12; a33 -= f * a13; r3 -= f * r1;
-    f = a32 / a22; a33 -= f * a23; r3 -= f * r2;
-    const double x3 = r3 / a33;
-    const double x2 = (r2 - a23 * x3) / a22;
-    const double x1 = (r1 - a12 * x2 - a13 * x3) / a11;
-    const double x0 = (r0 - a01 * x1 - a02 * x2 - a03 * x3) / a00;
-    solved[0] = x0; solved[1] = x1; solved[2] = x2; solved[3] = x3;
-    return;
-  }
-  double AS[P * P], RS[P], XS[P];
-  int IN[P];
-  int n = 0;
-  for (int k = 0; k < count; k++) {
-    solved[k] = 0;
-    if (set >> k & 1) IN[n++] = k;
-  }
-  for (int r = 0; r < n; r++) {
-    const int kr = IN[r];
-    for (int s = 0; s < n; s++) AS[r * P + s] = K[P * kr + IN[s]];
-    AS[r * P + r] *= 1 + give[kr];
-    RS[r] = wanted[kr];
-  }
-  for (int col = 0; col < n; col++) {
-    const double pivot = AS[col * P + col];
-    for (int r = col + 1; r < n; r++) {
-      const double f = AS[r * P + col] / pivot;
-      for (int s = col + 1; s < n; s++) AS[r * P + s] -= f * AS[col * P + s];
-      RS[r] -= f * RS[col];
-    }
-  }
-  for (int r = n - 1; r >= 0; r--) {
-    double x = RS[r];
-    for (int s = r + 1; s < n; s++) x -= AS[r * P + s] * XS[s];
-    XS[r] = x / AS[r * P + r];
-    solved[IN[r]] = XS[r];
+__device__ __forceinline__ void warm_row(const StageParams& p, int m) {
+  switch (ldi(p.R.points + m)) {
+    case 1: warm_row_n<1>(p, m); break;
+    case 2: warm_row_n<2>(p, m); break;
+    case 3: warm_row_n<3>(p, m); break;
+    default: warm_row_n<4>(p, m); break;
   }
 }
 
-// solveRows for row m, one pass: src/contact.js:1805-2090.
-__device__ void solve_row(const StageParams& p, int m, double h, bool bias, bool known) {
+// pushes: src/contact.js:1672-1724.  One instance per point count N and point set SET, so
+// the points taken, and every index below, are compile-time constants: the reference's subset
+// Gaussian elimination, in its operation order, on registers.  (For N = 4 and SET = 15 this is
+// exactly the written-out path of src/contact.js:1673-1698, which does the same operations.)
+__host__ __device__ constexpr int set_size(int set, int n) {
+  return n == 0 ? 0 : ((set & 1) + set_size(set >> 1, n - 1));
+}
+// The r-th point of SET (the reference's IN[r]).
+__host__ __device__ constexpr int set_point(int set, int r, int k = 0) {
+  return (set & 1) ? (r == 0 ? k : set_point(set >> 1, r - 1, k + 1)) : set_point(set >> 1, r, k + 1);
+}
+
+template <int N, int SET>
+__device__ __forceinline__ void solve_set(const double (&K)[N][N], const double (&give)[N], const double (&wanted)[N],
+                                          double (&solved)[N]) {
+  constexpr int n = set_size(SET, N);
+#pragma unroll
+  for (int k = 0; k < N; k++) solved[k] = 0;
+  if (n == 0) return;
+  double AS[n > 0 ? n : 1][n > 0 ? n : 1], RS[n > 0 ? n : 1], XS[n > 0 ? n : 1];
+#pragma unroll
+  for (int r = 0; r < n; r++) {
+#pragma unroll
+    for (int s = 0; s < n; s++) AS[r][s] = K[set_point(SET, r)][set_point(SET, s)];
+    AS[r][r] *= 1 + give[set_point(SET, r)];
+    RS[r] = wanted[set_point(SET, r)];
+  }
+#pragma unroll
+  for (int col = 0; col < n; col++) {
+    const double pivot = AS[col][col];
+#pragma unroll
+    for (int r = col + 1; r < n; r++) {
+      const double f = AS[r][col] / pivot;
+#pragma unroll
+      for (int s = col + 1; s < n; s++) AS[r][s] -= f * AS[col][s];
+      RS[r] -= f * RS[col];
+    }
+  }
+#pragma unroll
+  for (int r = n - 1; r >= 0; r--) {
+    double x = RS[r];
+#pragma unroll
+    for (int s = r + 1; s < n; s++) x -= AS[r][s] * XS[s];
+    XS[r] = x / AS[r][r];
+    solved[set_point(SET, r)] = XS[r];
+  }
+}
+
+template <int N>
+__device__ __forceinline__ void pushes_n(const double (&K)[N][N], int set, const double (&give)[N],
+                                         const double (&wanted)[N], double (&solved)[N]) {
+#define BG_SET(S) \
+  case S:         \
+    if (S < (1 << N)) solve_set<N, (S < (1 << N) ? S : 0)>(K, give, wanted, solved); \
+    break;
+  switch (set) {
+    BG_SET(0) BG_SET(1) BG_SET(2) BG_SET(3) BG_SET(4) BG_SET(5) BG_SET(6) BG_SET(7)
+    BG_SET(8) BG_SET(9) BG_SET(10) BG_SET(11) BG_SET(12) BG_SET(13) BG_SET(14) BG_SET(15)
+    default: break;
+  }
+#undef BG_SET
+}
+
+// solveRows for row m, one pass, a row of N points: src/contact.js:1805-2090.
+template <int N>
+__device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bool known) {
   const RowsDev& R = p.R;
   const BodiesDev& B = p.B;
   const int64_t cap = R.cap;
@@ -683,10 +733,47 @@ __device__ void solve_row(const StageParams& p, int m, double h, bool bias, bool
   const double inv = 1 / h;
   const double springy = soft.impulseScale / soft.massScale + COMPLIANCE;
   const int a = ldi(R.a + m), b = ldi(R.b + m);
+  // The row's own columns first, so their loads are in flight together.
   const double nx = ldi(R.n + m), ny = ldi(R.n + cap + m), nz = ldi(R.n + 2 * cap + m);
   const double maxBias = ldi(R.tolerance + m) * inv;
-  const int count = ldi(R.points + m);
-  double target[P], massScale[P], impulseScale[P], give[P], closingNow[P], wanted[P], solved[P];
+  double sep[N];
+  double la[N][3], lb[N][3];
+  if (known) {
+#pragma unroll
+    for (int k = 0; k < N; k++) sep[k] = ldm(R.now + k * cap + m);
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      sep[k] = ldm(R.adjusted + k * cap + m);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        la[k][c] = ldm(R.la + (k * 3 + c) * cap + m);
+        lb[k][c] = ldm(R.lb + (k * 3 + c) * cap + m);
+      }
+    }
+  }
+  double ni[N], jn[N][6];
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    ni[k] = ldm(R.ni + k * cap + m);
+#pragma unroll
+    for (int c = 0; c < 6; c++) jn[k][c] = ldm(R.jac + (k * J + c) * cap + m);
+  }
+  double Kb[N][N];
+  if (N >= 2) {
+#pragma unroll
+    for (int k = 0; k < N; k++)
+#pragma unroll
+      for (int l = 0; l < N; l++) Kb[k][l] = ldm(R.K + (P * k + l) * cap + m);
+  }
+  // The two bodies.
+  BodyLoad A, Bb;
+  load_mass(B, a, A);
+  load_mass(B, b, Bb);
+  const double* va = B.vw + 8 * a;
+  const double* vb = B.vw + 8 * b;
+  double vax = ldm(va), vay = ldm(va + 1), vaz = ldm(va + 2), wax = ldm(va + 3), way = ldm(va + 4), waz = ldm(va + 5);
+  double vbx = ldm(vb), vby = ldm(vb + 1), vbz = ldm(vb + 2), wbx = ldm(vb + 3), wby = ldm(vb + 4), wbz = ldm(vb + 5);
   double dn = 0, nax = 0, nay = 0, naz = 0, nbx = 0, nby = 0, nbz = 0;
   if (!known) {
     const double* pqa = B.pq + 8 * a;
@@ -698,24 +785,23 @@ __device__ void solve_row(const StageParams& p, int m, double h, bool bias, bool
     const double dz = (ldm(pqb + 2) - ldm(stb + 2)) - (ldm(pqa + 2) - ldm(sta + 2));
     dn = dx * nx + dy * ny + dz * nz;
     double qa[4], qb[4], v3[3];
+#pragma unroll
     for (int k = 0; k < 4; k++) { qa[k] = ldm(pqa + 4 + k); qb[k] = ldm(pqb + 4 + k); }
     rotate(qa, nx, ny, nz, true, v3);
     nax = v3[0]; nay = v3[1]; naz = v3[2];
     rotate(qb, nx, ny, nz, true, v3);
     nbx = v3[0]; nby = v3[1]; nbz = v3[2];
   }
+  double target[N], massScale[N], impulseScale[N], give[N];
   double least = INFINITY;
 #pragma unroll
-  for (int k = 0; k < P; k++) {
-    if (k >= count) break;
+  for (int k = 0; k < N; k++) {
     double s;
     if (known) {
-      s = ldm(R.now + k * cap + m);
+      s = sep[k];
     } else {
-      const double* lb = R.lb + (k * 3) * cap + m;
-      const double* la = R.la + (k * 3) * cap + m;
-      s = dn + (ldm(lb) * nbx + ldm(lb + cap) * nby + ldm(lb + 2 * cap) * nbz)
-        - (ldm(la) * nax + ldm(la + cap) * nay + ldm(la + 2 * cap) * naz) + ldm(R.adjusted + k * cap + m);
+      s = dn + (lb[k][0] * nbx + lb[k][1] * nby + lb[k][2] * nbz) - (la[k][0] * nax + la[k][1] * nay + la[k][2] * naz)
+        + sep[k];
       if (!bias) stm(R.now + k * cap + m, s);
     }
     if (s < least) least = s;
@@ -729,28 +815,12 @@ __device__ void solve_row(const StageParams& p, int m, double h, bool bias, bool
     }
   }
   stm(R.gap + m, least);
-  BodyLoad A, Bb;
-  load_mass(B, a, A);
-  load_mass(B, b, Bb);
   const double ima = A.im, imb = Bb.im;
-  const double* va = B.vw + 8 * a;
-  const double* vb = B.vw + 8 * b;
-  double vax = ldm(va), vay = ldm(va + 1), vaz = ldm(va + 2), wax = ldm(va + 3), way = ldm(va + 4), waz = ldm(va + 5);
-  double vbx = ldm(vb), vby = ldm(vb + 1), vbz = ldm(vb + 2), wbx = ldm(vb + 3), wby = ldm(vb + 4), wbz = ldm(vb + 5);
-  double ni[P], jk[P][J];
+  double closingNow[N], solved[N];
+  if (N == 1 || !(Kb[0][0] > 0)) {
 #pragma unroll
-  for (int k = 0; k < P; k++) {
-    if (k >= count) break;
-    ni[k] = ldm(R.ni + k * cap + m);
-    for (int c = 0; c < J; c++) jk[k][c] = ldm(R.jac + (k * J + c) * cap + m);
-  }
-  double K[P * P];
-  const double K00 = count >= 2 ? ldm(R.K + m) : 0.0;
-  if (count == 1 || !(K00 > 0)) {
-#pragma unroll
-    for (int k = 0; k < P; k++) {
-      if (k >= count) break;
-      const double* jac = jk[k];
+    for (int k = 0; k < N; k++) {
+      const double* jac = jn[k];
       const double vn = (vbx - vax) * nx + (vby - vay) * ny + (vbz - vaz) * nz
         + wbx * jac[3] + wby * jac[4] + wbz * jac[5] - wax * jac[0] - way * jac[1] - waz * jac[2];
       const double old = ni[k];
@@ -759,42 +829,45 @@ __device__ void solve_row(const StageParams& p, int m, double h, bool bias, bool
       closingNow[k] = vn; solved[k] = next;
     }
   } else {
-    for (int k = 0; k < count; k++)
-      for (int l = 0; l < count; l++) K[P * k + l] = ldm(R.K + (P * k + l) * cap + m);
 #pragma unroll
-    for (int k = 0; k < P; k++) {
-      if (k >= count) break;
-      const double* jac = jk[k];
+    for (int k = 0; k < N; k++) {
+      const double* jac = jn[k];
       closingNow[k] = (vbx - vax) * nx + (vby - vay) * ny + (vbz - vaz) * nz
         + wbx * jac[3] + wby * jac[4] + wbz * jac[5] - wax * jac[0] - way * jac[1] - waz * jac[2];
     }
+    double wanted[N];
     int set = 0;
-    for (int k = 0; k < count; k++) {
+#pragma unroll
+    for (int k = 0; k < N; k++) {
       double r = -closingNow[k] - target[k];
-      for (int l = 0; l < count; l++) r += K[P * k + l] * ni[l];
+#pragma unroll
+      for (int l = 0; l < N; l++) r += Kb[k][l] * ni[l];
       wanted[k] = r;
       if (r > 0) set |= 1 << k;
     }
     for (int round = 0;; round++) {
-      pushes(K, count, set, give, wanted, solved);
+      pushes_n<N>(Kb, set, give, wanted, solved);
       int flip = -1;
-      for (int k = 0; k < count && flip < 0; k++) {
-        if (set >> k & 1) {
-          if (solved[k] < 0) flip = k;
-        } else {
-          double r = -wanted[k];
-          for (int l = 0; l < count; l++) r += K[P * k + l] * solved[l];
-          if (r < 0) flip = k;
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        if (flip < 0) {
+          if (set >> k & 1) {
+            if (solved[k] < 0) flip = k;
+          } else {
+            double r = -wanted[k];
+#pragma unroll
+            for (int l = 0; l < N; l++) r += Kb[k][l] * solved[l];
+            if (r < 0) flip = k;
+          }
         }
       }
-      if (flip < 0 || round == 1 << count) break;
+      if (flip < 0 || round == 1 << N) break;
       set ^= 1 << flip;
     }
   }
 #pragma unroll
-  for (int k = 0; k < P; k++) {
-    if (k >= count) break;
-    const double* jac = jk[k];
+  for (int k = 0; k < N; k++) {
+    const double* jac = R.jac + (k * J) * cap + m;
     const double old = ni[k], next = solved[k] > 0 ? solved[k] : 0;
     const double d = next - old;
     ni[k] = next;
@@ -805,21 +878,21 @@ __device__ void solve_row(const StageParams& p, int m, double h, bool bias, bool
     const double px = nx * d, py = ny * d, pz = nz * d;
     vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
     vbx += imb * px; vby += imb * py; vbz += imb * pz;
-    wax -= jac[6] * d; way -= jac[7] * d; waz -= jac[8] * d;
-    wbx += jac[9] * d; wby += jac[10] * d; wbz += jac[11] * d;
+    wax -= ldm(jac + 6 * cap) * d; way -= ldm(jac + 7 * cap) * d; waz -= ldm(jac + 8 * cap) * d;
+    wbx += ldm(jac + 9 * cap) * d; wby += ldm(jac + 10 * cap) * d; wbz += ldm(jac + 11 * cap) * d;
   }
   const double mu = ldi(R.friction + m);
   const double t1x = ldi(R.t1 + m), t1y = ldi(R.t1 + cap + m), t1z = ldi(R.t1 + 2 * cap + m);
   const double t2x = ldi(R.t2 + m), t2y = ldi(R.t2 + cap + m), t2z = ldi(R.t2 + 2 * cap + m);
   double pressed = 0, twisted = 0;
 #pragma unroll
-  for (int k = 0; k < P; k++) {
-    if (k >= count) break;
+  for (int k = 0; k < N; k++) {
     pressed += ni[k];
     twisted += ldm(R.lever + k * cap + m) * ni[k];
   }
   {
     double fj[FJ];
+#pragma unroll
     for (int c = 0; c < FJ; c++) fj[c] = ldm(R.fjac + c * cap + m);
     const double* g = fj + 12;
     const double dvx = vbx - vax, dvy = vby - vay, dvz = vbz - vaz;
@@ -872,7 +945,7 @@ __device__ void solve_row(const StageParams& p, int m, double h, bool bias, bool
   }
   const double* Ia = A.I;
   const double* Ib = Bb.I;
-  if (count <= 2) {
+  if (N <= 2) {
     const double most = ldi(R.patch + m) * pressed;
     const double ux = wbx - wax, uy = wby - way, uz = wbz - waz;
     const double r1 = ldm(R.ri1 + m), r2 = ldm(R.ri2 + m);
@@ -894,7 +967,7 @@ __device__ void solve_row(const StageParams& p, int m, double h, bool bias, bool
     wbz += Ib[2] * lx + Ib[4] * ly + Ib[5] * lz;
   }
   {
-    const double limit = count == 1 ? SPIN_DISC * mu * ldi(R.patch + m) * pressed : mu * twisted;
+    const double limit = N == 1 ? SPIN_DISC * mu * ldi(R.patch + m) * pressed : mu * twisted;
     const double s0 = ldm(R.si + m);
     double s1 = s0 - ldm(R.sm + m) * ((wbx - wax) * nx + (wby - way) * ny + (wbz - waz) * nz);
     if (s1 > limit) s1 = limit; else if (s1 < -limit) s1 = -limit;
@@ -909,6 +982,15 @@ __device__ void solve_row(const StageParams& p, int m, double h, bool bias, bool
   }
   write_back(B, ima, a, vax, vay, vaz, wax, way, waz);
   write_back(B, imb, b, vbx, vby, vbz, wbx, wby, wbz);
+}
+
+__device__ __forceinline__ void solve_row(const StageParams& p, int m, double h, bool bias, bool known) {
+  switch (ldi(p.R.points + m)) {
+    case 1: solve_row_n<1>(p, m, h, bias, known); break;
+    case 2: solve_row_n<2>(p, m, h, bias, known); break;
+    case 3: solve_row_n<3>(p, m, h, bias, known); break;
+    default: solve_row_n<4>(p, m, h, bias, known); break;
+  }
 }
 
 // Whether row m has a point restitution() works on: src/contact.js:2233-2241.  What it reads
@@ -1166,19 +1248,19 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
   const double h = p.dt / substeps;
   const int* starts = w.starts;
   const int r0 = w.row0;
-  for (int i = t.rank; i < w.nawake; i += t.size) body_begin(p, ldi(p.B.awake_list + w.awake0 + i), touching);
+  t.each(0, w.nawake, [&](int i) { body_begin(p, ldi(p.B.awake_list + w.awake0 + i), touching); });
   if (!t.sync(p)) return false;
   if (touching) {
-    for (int m = t.rank; m < w.solved; m += t.size) prepare_row(p, r0 + m);
+    t.each(0, w.solved, [&](int m) { prepare_row(p, r0 + m); });
     if (!t.sync(p)) return false;
   }
   for (int sub = 0; sub < substeps; sub++) {
-    for (int i = t.rank; i < w.nawake; i += t.size) accelerate_body(p, ldi(p.B.awake_list + w.awake0 + i), h, w.gravity);
+    t.each(0, w.nawake, [&](int i) { accelerate_body(p, ldi(p.B.awake_list + w.awake0 + i), h, w.gravity); });
     if (!t.sync(p)) return false;
     if (touching) {
       for (int k = 0; k < NCOLOURS; k++) {
         if (starts[k + 1] <= starts[k]) continue;
-        for (int m = starts[k] + t.rank; m < starts[k + 1]; m += t.size) warm_row(p, r0 + m);
+        t.each(starts[k], starts[k + 1], [&](int m) { warm_row(p, r0 + m); });
         if (!t.sync(p)) return false;
       }
       if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
@@ -1188,7 +1270,7 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
       }
       for (int k = 0; k < NCOLOURS; k++) {
         if (starts[k + 1] <= starts[k]) continue;
-        for (int m = starts[k] + t.rank; m < starts[k + 1]; m += t.size) solve_row(p, r0 + m, h, true, sub > 0);
+        t.each(starts[k], starts[k + 1], [&](int m) { solve_row(p, r0 + m, h, true, sub > 0); });
         if (!t.sync(p)) return false;
       }
       if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
@@ -1197,12 +1279,12 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
         if (!t.sync(p)) return false;
       }
     }
-    for (int i = t.rank; i < w.nawake; i += t.size) move_body(p, ldi(p.B.awake_list + w.awake0 + i), h);
+    t.each(0, w.nawake, [&](int i) { move_body(p, ldi(p.B.awake_list + w.awake0 + i), h); });
     if (!t.sync(p)) return false;
     if (touching) {
       for (int k = 0; k < NCOLOURS; k++) {
         if (starts[k + 1] <= starts[k]) continue;
-        for (int m = starts[k] + t.rank; m < starts[k + 1]; m += t.size) solve_row(p, r0 + m, h, false, false);
+        t.each(starts[k], starts[k + 1], [&](int m) { solve_row(p, r0 + m, h, false, false); });
         if (!t.sync(p)) return false;
       }
       if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
@@ -1216,7 +1298,7 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
     const double* g = w.gravity;
     const double gravity = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
     if (!restitution_stage(p, w, t, gravity)) return false;
-    for (int m = t.rank; m < w.solved; m += t.size) slipped_row(p, r0 + m);
+    t.each(0, w.solved, [&](int m) { slipped_row(p, r0 + m); });
   }
   return true;
 }

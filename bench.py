@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--at", type=int, default=300, help="steps taken before the timed solve stage")
     p.add_argument("--cpu-sample", type=int, default=2, help="solve stages the CPU baseline times")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--resident-only", action="store_true", help="time the resident solve only (for profiling)")
     return p.parse_args()
 
 
@@ -157,9 +158,11 @@ def time_resident(lib, ctx, copy, steps, warmup, torch):
             flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         before = lib.bg_last_launches(ctx)
+        torch.cuda.nvtx.range_push("timed" if i >= warmup else "warmup")
         e0.record(stream)
         rc = lib.bg_solve(ctx, C.byref(S))
         e1.record(stream)
+        torch.cuda.nvtx.range_pop()
         assert rc == 0, lib.bg_last_error(ctx)
         e1.synchronize()
         if i >= warmup:
@@ -297,7 +300,7 @@ def main():
     clocks.start()
     times, stage, launches, out = time_resident(lib, ctx, copy, args.steps, args.warmup, torch)
     clock = clocks.stop()
-    e2e_times = time_e2e(lib, ctx, copy, args.steps, args.warmup, torch)
+    e2e_times = times if args.resident_only else time_e2e(lib, ctx, copy, args.steps, args.warmup, torch)
     torch.cuda.synchronize()
     ms = statistics.mean(times)
     ms_e2e = statistics.mean(e2e_times)
@@ -317,7 +320,7 @@ def main():
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = algo / (ms_stage / 1000) / 1e9
     cpu = None
-    if rank == 0 and world_size == 1 and not args.no_cpu:
+    if rank == 0 and world_size == 1 and not args.no_cpu and not args.resident_only:
         threads = host_threads()
         t1 = cpu_solve_times(copy, 0, args.cpu_sample)
         cpu = {"value": rows_per_stage / statistics.mean(t1), "unit": "rows/s", "cores": 1, "kind": "port",
