@@ -248,6 +248,13 @@ struct bg_ctx {
   int32_t* perm_dev = nullptr;
   int32_t* iperm_dev = nullptr;
   std::vector<int32_t> perm, iperm;
+  // the grid's dataflow schedule (see stage.cuh, flow_pass)
+  int32_t* rank_dev = nullptr;     // rank_a then rank_b, by device row
+  int32_t* deg_dev = nullptr;
+  unsigned int* done_dev = nullptr;
+  int2* chunks_dev = nullptr;
+  std::vector<int32_t> rank, deg;
+  std::vector<int2> chunks;
   // staging out
   BodyOut bout = {};
   RowOut rout = {};
@@ -318,6 +325,8 @@ bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
   const size_t nw = grown(c->world_cap, static_cast<size_t>(nworlds));
   bool ok = true;
   bg::BodiesDev& B = c->B;
+  B.deg = nullptr;
+  B.done = nullptr;
   ok = ok && dev_alloc(c, &B.vw, 8 * nb) && dev_alloc(c, &B.mi, 8 * nb) && dev_alloc(c, &B.pq, 8 * nb) &&
        dev_alloc(c, &B.st, 4 * nb) && dev_alloc(c, &B.sq, 4 * nb) && dev_alloc(c, &B.tc, 4 * nb) &&
        dev_alloc(c, &B.pr, 12 * nb) && dev_alloc(c, &B.fl, nb) && dev_alloc(c, &B.awake_list, na) &&
@@ -372,7 +381,9 @@ bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
        dev_alloc(c, &shift, 12 * nr) && dev_alloc(c, &ni, 4 * nr) && dev_alloc(c, &ti1, nr) && dev_alloc(c, &ti2, nr) &&
        dev_alloc(c, &ri1, nr) && dev_alloc(c, &ri2, nr) && dev_alloc(c, &si, nr) && dev_alloc(c, &drift1, nr) &&
        dev_alloc(c, &drift2, nr) && dev_alloc(c, &c->maxni_in, 4 * nr) && dev_alloc(c, &c->relvel_in, 4 * nr) &&
-       dev_alloc(c, &c->gap_in, nr) && dev_alloc(c, &c->perm_dev, nr) && dev_alloc(c, &c->iperm_dev, nr);
+       dev_alloc(c, &c->gap_in, nr) && dev_alloc(c, &c->perm_dev, nr) && dev_alloc(c, &c->iperm_dev, nr) &&
+       dev_alloc(c, &c->rank_dev, 2 * nr) && dev_alloc(c, &c->deg_dev, nb) && dev_alloc(c, &c->done_dev, nb) &&
+       dev_alloc(c, &c->chunks_dev, nr + 64);
   if (!ok) return false;
   ri = RowStage{row, a, b, points, normal, t1, t2, friction, restitution, tolerance, patch, separation, point, shift,
                 ni, ti1, ti2, ri1, ri2, si, drift1, drift2};
@@ -498,7 +509,7 @@ int upload_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R, int nb, int 
 // colour's rows share no body the solve moves, so their order changes no result, src/graph.js:1-33),
 // which keeps a warp's 32 rows on one code path.  The overflow and resting runs keep their order
 // (the overflow is solved in row order, src/contact.js:1794-1795).
-int order_rows(bg_ctx* c, const uint8_t* points) {
+int order_rows(bg_ctx* c, const uint8_t* points, const int32_t* a, const int32_t* b, const double* inv_mass) {
   const int n = c->nrows;
   c->perm.resize(static_cast<size_t>(n));
   c->iperm.resize(static_cast<size_t>(n));
@@ -519,8 +530,32 @@ int order_rows(bg_ctx* c, const uint8_t* points) {
     }
   }
   for (int d = 0; d < n; d++) c->iperm[static_cast<size_t>(c->perm[static_cast<size_t>(d)])] = d;
+  // Each solved row's place among the rows on each body it moves, in device (solve) order, and
+  // each body's count of them: what the grid's dataflow waits on.
+  c->rank.assign(2 * static_cast<size_t>(n), -1);
+  c->deg.assign(static_cast<size_t>(c->nbodies), 0);
+  for (const bg::WorldDesc& w : c->worlds) {
+    for (int d = w.row0; d < w.row0 + w.solved; d++) {
+      const int m = c->perm[static_cast<size_t>(d)];
+      const int x = a[m] + w.body0, y = b[m] + w.body0;
+      if (inv_mass[x] != 0) c->rank[static_cast<size_t>(d)] = c->deg[static_cast<size_t>(x)]++;
+      if (inv_mass[y] != 0) c->rank[static_cast<size_t>(n) + d] = c->deg[static_cast<size_t>(y)]++;
+    }
+  }
+  // The grid's runs: each colour's rows in runs of 32, then the overflow's one row a run.
+  c->chunks.clear();
+  if (c->nworlds == 1) {
+    const bg::WorldDesc& w = c->worlds[0];
+    for (int k = 0; k < bg::NCOLOURS; k++)
+      for (int m = w.starts[k]; m < w.starts[k + 1]; m += 32)
+        c->chunks.push_back(make_int2(m, std::min(32, w.starts[k + 1] - m)));
+    for (int m = w.starts[bg::OVERFLOW_RUN]; m < w.starts[bg::OVERFLOW_RUN + 1]; m++) c->chunks.push_back(make_int2(m, 1));
+  }
   bool ok = put(c, c->perm_dev, c->perm.data(), static_cast<size_t>(n), "perm") &&
-            put(c, c->iperm_dev, c->iperm.data(), static_cast<size_t>(n), "iperm");
+            put(c, c->iperm_dev, c->iperm.data(), static_cast<size_t>(n), "iperm") &&
+            put(c, c->rank_dev, c->rank.data(), 2 * static_cast<size_t>(n), "rank") &&
+            put(c, c->deg_dev, c->deg.data(), static_cast<size_t>(c->nbodies), "deg") &&
+            put(c, c->chunks_dev, c->chunks.data(), c->chunks.size(), "chunks");
   return ok ? BG_OK : BG_ECUDA;
 }
 
@@ -573,6 +608,14 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
   p.status = c->status;
   p.block_counts = c->block_counts;
   p.budget = c->budget;
+  p.B.deg = c->deg_dev;
+  p.B.done = c->done_dev;
+  p.R.rank_a = c->rank_dev;
+  p.R.rank_b = c->rank_dev + c->nrows;
+  p.chunks = c->chunks_dev;
+  p.nchunks = static_cast<int32_t>(c->chunks.size());
+  if (!cuda_ok(c, cudaMemsetAsync(c->done_dev, 0, sizeof(unsigned int) * static_cast<size_t>(c->nbodies > 0 ? c->nbodies : 1),
+                                  c->stream), "done")) return BG_ECUDA;
   if (!cuda_ok(c, cudaMemsetAsync(c->status, 0, sizeof(int32_t), c->stream), "status")) return BG_ECUDA;
   c->last_launches += 1;
   cudaEventRecord(c->stage_begin, c->stream);
@@ -716,7 +759,7 @@ int32_t bg_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
   c->worlds.assign(1, w);
   rc = upload_columns(c, B, R, c->nbodies, c->nrows, c->nawake);
   if (rc != BG_OK) return rc;
-  rc = order_rows(c, R->points);
+  rc = order_rows(c, R->points, R->a, R->b, B->inv_mass);
   if (rc != BG_OK) return rc;
   std::vector<int32_t> bo = {0, c->nbodies}, ao = {0, c->nawake}, ro = {0, c->nrows};
   rc = upload_worlds(c, bo, ao, ro);
@@ -808,7 +851,7 @@ int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const b
   c->worlds = worlds;
   rc = upload_columns(c, B, R, c->nbodies, c->nrows, c->nawake);
   if (rc != BG_OK) return rc;
-  rc = order_rows(c, R->points);
+  rc = order_rows(c, R->points, R->a, R->b, B->inv_mass);
   if (rc != BG_OK) return rc;
   std::vector<int32_t> bo(W->body_offset, W->body_offset + nw + 1), ao(W->awake_offset, W->awake_offset + nw + 1),
       ro(W->row_offset, W->row_offset + nw + 1);

@@ -48,6 +48,8 @@ struct BodiesDev {
   uint32_t* fl;
   int32_t* awake_list;   // global slots of the awake bodies, world after world
   int32_t* head;         // restitution's per-body scratch (see restitution())
+  int32_t* deg;          // rows that move this body in a pass (0 for a body the solve never moves)
+  unsigned int* done;    // rows done on this body so far in the stage (the grid's dataflow)
 };
 
 struct RowsDev {
@@ -97,6 +99,10 @@ struct RowsDev {
   // restitution's work lists
   int32_t* active;       // found indices of bouncy rows, compacted
   int32_t* pending;
+  // the row's place among the rows on each of its bodies, in solve order (-1: a body the solve
+  // never moves, so nothing to wait for)
+  int32_t* rank_a;
+  int32_t* rank_b;
 };
 
 // One world's share of the arrays.
@@ -130,6 +136,10 @@ struct StageParams {
   int32_t* status;
   int32_t* block_counts;  // per-block counts for restitution's compaction
   long long budget;
+  // The grid's pass schedule: runs of rows (start, length), colour after colour, each within
+  // one colour (or one row of the overflow); warp w takes runs w, w + warps, ... in order.
+  const int2* chunks;
+  int32_t nchunks;
 };
 
 }  // namespace bg

@@ -192,6 +192,69 @@ struct GridTeam {
   }
 };
 
+// ---- the grid's dataflow passes ----
+//
+// A pass over every solved row with no barrier between colours: a row waits only until the rows
+// before it (in solve order) on each body it moves are done, which is all that colour order
+// guarantees and all the reference's order depends on (src/graph.js:1-33).  Each body's counter
+// counts its rows done in the stage; row m of pass `pass` on body X may start when it reaches
+// pass * deg[X] + rank, and moves it on by one when its writes are out (release / acquire).
+// Work goes to warps as runs of rows in solve order, each warp taking its runs in ascending
+// order, so the earliest waiting row always has every predecessor done or running: no cycle.
+// Every wait is bounded by the step's budget; past it the status word is set and all waits end.
+
+__device__ __forceinline__ unsigned int load_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void store_release(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ bool wait_body(const StageParams& p, int x, int rank, int pass) {
+  if (rank < 0) return true;
+  const unsigned int target = static_cast<unsigned int>(pass) * static_cast<unsigned int>(ldi(p.B.deg + x)) +
+                              static_cast<unsigned int>(rank);
+  long long it = 0;
+  while (load_acquire(p.B.done + x) < target) {
+    if (++it > p.budget || ((it & 255) == 0 && *(volatile int32_t*)p.status != 0)) {
+      atomicExch(p.status, 1);
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void signal_body(const StageParams& p, int x, int rank, int pass) {
+  if (rank < 0) return;
+  const unsigned int next = static_cast<unsigned int>(pass) * static_cast<unsigned int>(ldi(p.B.deg + x)) +
+                            static_cast<unsigned int>(rank) + 1u;
+  store_release(p.B.done + x, next);
+}
+
+template <class F>
+__device__ __forceinline__ void flow_pass(const StageParams& p, int pass, F row) {
+  const int lane = static_cast<int>(threadIdx.x) & 31;
+  const int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int warps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+  for (int c = warp; c < p.nchunks; c += warps) {
+    const int2 run = p.chunks[c];
+    if (lane < run.y) {
+      const int m = run.x + lane;
+      const int a = ldi(p.R.a + m), b = ldi(p.R.b + m);
+      const int ra = ldi(p.R.rank_a + m), rb = ldi(p.R.rank_b + m);
+      bool open = false;
+      row(m, [&]() { open = wait_body(p, a, ra, pass) && wait_body(p, b, rb, pass); return open; });
+      if (open) {
+        signal_body(p, a, ra, pass);
+        signal_body(p, b, rb, pass);
+      }
+    }
+    __syncwarp();
+  }
+}
+
 struct BlockTeam {
   static constexpr bool kGrid = false;
   int rank, size;
@@ -579,10 +642,14 @@ __device__ __forceinline__ void write_back(const BodiesDev& B, double im, int s,
   stm(vw, vx); stm(vw + 1, vy); stm(vw + 2, vz); stm(vw + 3, wx); stm(vw + 4, wy); stm(vw + 5, wz);
 }
 
+struct OpenGate {
+  __device__ __forceinline__ bool operator()() const { return true; }
+};
+
 // warmRows for row m: src/contact.js:1616-1663, for a row of N points.  Every array index below
 // is known at compile time, so nothing goes to local memory.
-template <int N>
-__device__ __forceinline__ void warm_row_n(const StageParams& p, int m) {
+template <int N, class Gate>
+__device__ __forceinline__ void warm_row_n(const StageParams& p, int m, Gate gate) {
   const RowsDev& R = p.R;
   const BodiesDev& B = p.B;
   const int64_t cap = R.cap;
@@ -612,6 +679,7 @@ __device__ __forceinline__ void warm_row_n(const StageParams& p, int m) {
   }
   const double l1 = ldm(R.ti1 + m), l2 = ldm(R.ti2 + m);
   const double r1 = ldm(R.ri1 + m), r2 = ldm(R.ri2 + m), sp = ldm(R.si + m);
+  if (!gate()) return;
   BodyLoad A, Bb;
   load_mass(B, a, A);
   load_mass(B, b, Bb);
@@ -651,12 +719,13 @@ __device__ __forceinline__ void warm_row_n(const StageParams& p, int m) {
   write_back(B, imb, b, vbx, vby, vbz, wbx, wby, wbz);
 }
 
-__device__ __forceinline__ void warm_row(const StageParams& p, int m) {
+template <class Gate>
+__device__ __forceinline__ void warm_row(const StageParams& p, int m, Gate gate) {
   switch (ldi(p.R.points + m)) {
-    case 1: warm_row_n<1>(p, m); break;
-    case 2: warm_row_n<2>(p, m); break;
-    case 3: warm_row_n<3>(p, m); break;
-    default: warm_row_n<4>(p, m); break;
+    case 1: warm_row_n<1>(p, m, gate); break;
+    case 2: warm_row_n<2>(p, m, gate); break;
+    case 3: warm_row_n<3>(p, m, gate); break;
+    default: warm_row_n<4>(p, m, gate); break;
   }
 }
 
@@ -723,17 +792,20 @@ __device__ __forceinline__ void pushes_n(const double (&K)[N][N], int set, const
 #undef BG_SET
 }
 
-// solveRows for row m, one pass, a row of N points: src/contact.js:1805-2090.
-template <int N>
-__device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bool known) {
+// solveRows for row m, one pass, a row of N points: src/contact.js:1805-2090.  The row's own
+// columns are read first, then `gate` (the grid's wait for the rows before it on its bodies; nothing
+// for a CTA), then its two bodies; every store is held to the end.  So once the gate opens, the
+// row costs one trip to memory (its bodies' records) and its arithmetic.
+template <int N, class Gate>
+__device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bool known, Gate gate) {
   const RowsDev& R = p.R;
   const BodiesDev& B = p.B;
   const int64_t cap = R.cap;
   const Soft soft = p.soft;
   const double inv = 1 / h;
   const double springy = soft.impulseScale / soft.massScale + COMPLIANCE;
+  // ---- the row's own columns ----
   const int a = ldi(R.a + m), b = ldi(R.b + m);
-  // The row's own columns first, so their loads are in flight together.
   const double nx = ldi(R.n + m), ny = ldi(R.n + cap + m), nz = ldi(R.n + 2 * cap + m);
   const double maxBias = ldi(R.tolerance + m) * inv;
   double sep[N];
@@ -752,12 +824,18 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
       }
     }
   }
-  double ni[N], jn[N][6];
+  double ni[N], jn[N][6], jw[N][6], mx[N], nmass[N], lev[N];
 #pragma unroll
   for (int k = 0; k < N; k++) {
     ni[k] = ldm(R.ni + k * cap + m);
+    mx[k] = ldm(R.maxni + k * cap + m);
+    nmass[k] = ldm(R.normalMass + k * cap + m);
+    lev[k] = ldm(R.lever + k * cap + m);
 #pragma unroll
-    for (int c = 0; c < 6; c++) jn[k][c] = ldm(R.jac + (k * J + c) * cap + m);
+    for (int c = 0; c < 6; c++) {
+      jn[k][c] = ldm(R.jac + (k * J + c) * cap + m);
+      jw[k][c] = ldm(R.jac + (k * J + 6 + c) * cap + m);
+    }
   }
   double Kb[N][N];
   if (N >= 2) {
@@ -766,7 +844,24 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
 #pragma unroll
       for (int l = 0; l < N; l++) Kb[k][l] = ldm(R.K + (P * k + l) * cap + m);
   }
-  // The two bodies.
+  const double mu = ldi(R.friction + m), patch = ldi(R.patch + m);
+  const double t1x = ldi(R.t1 + m), t1y = ldi(R.t1 + cap + m), t1z = ldi(R.t1 + 2 * cap + m);
+  const double t2x = ldi(R.t2 + m), t2y = ldi(R.t2 + cap + m), t2z = ldi(R.t2 + 2 * cap + m);
+  double fj[FJ];
+#pragma unroll
+  for (int c = 0; c < FJ; c++) fj[c] = ldm(R.fjac + c * cap + m);
+  const double s1 = ldm(R.drift1 + m), s2 = ldm(R.drift2 + m);
+  const double tm0 = ldm(R.tm + m), tm1 = ldm(R.tm + cap + m), tm2 = ldm(R.tm + 2 * cap + m);
+  const double o1 = ldm(R.ti1 + m), o2 = ldm(R.ti2 + m);
+  double r1 = 0, r2 = 0, rm1 = 0, rm2 = 0;
+  if (N <= 2) {
+    r1 = ldm(R.ri1 + m); r2 = ldm(R.ri2 + m);
+    rm1 = ldm(R.rm1 + m); rm2 = ldm(R.rm2 + m);
+  }
+  const double s0 = ldm(R.si + m), smass = ldm(R.sm + m);
+  // ---- the rows before this one on its bodies ----
+  if (!gate()) return;
+  // ---- its bodies ----
   BodyLoad A, Bb;
   load_mass(B, a, A);
   load_mass(B, b, Bb);
@@ -792,7 +887,8 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
     rotate(qb, nx, ny, nz, true, v3);
     nbx = v3[0]; nby = v3[1]; nbz = v3[2];
   }
-  double target[N], massScale[N], impulseScale[N], give[N];
+  // ---- the arithmetic, in the reference's order ----
+  double target[N], massScale[N], impulseScale[N], give[N], nowv[N];
   double least = INFINITY;
 #pragma unroll
   for (int k = 0; k < N; k++) {
@@ -802,8 +898,8 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
     } else {
       s = dn + (lb[k][0] * nbx + lb[k][1] * nby + lb[k][2] * nbz) - (la[k][0] * nax + la[k][1] * nay + la[k][2] * naz)
         + sep[k];
-      if (!bias) stm(R.now + k * cap + m, s);
     }
+    nowv[k] = s;
     if (s < least) least = s;
     if (s > 0) {
       target[k] = s * inv; massScale[k] = 1; impulseScale[k] = 0; give[k] = COMPLIANCE;
@@ -814,7 +910,6 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
       target[k] = 0; massScale[k] = 1; impulseScale[k] = 0; give[k] = COMPLIANCE;
     }
   }
-  stm(R.gap + m, least);
   const double ima = A.im, imb = Bb.im;
   double closingNow[N], solved[N];
   if (N == 1 || !(Kb[0][0] > 0)) {
@@ -824,7 +919,7 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
       const double vn = (vbx - vax) * nx + (vby - vay) * ny + (vbz - vaz) * nz
         + wbx * jac[3] + wby * jac[4] + wbz * jac[5] - wax * jac[0] - way * jac[1] - waz * jac[2];
       const double old = ni[k];
-      double next = old - ldm(R.normalMass + k * cap + m) * massScale[k] * (vn + target[k]) - impulseScale[k] * old;
+      double next = old - nmass[k] * massScale[k] * (vn + target[k]) - impulseScale[k] * old;
       if (next < 0) next = 0;
       closingNow[k] = vn; solved[k] = next;
     }
@@ -865,40 +960,35 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
       set ^= 1 << flip;
     }
   }
+  double rv[N];
+  bool rvset[N];
 #pragma unroll
   for (int k = 0; k < N; k++) {
-    const double* jac = R.jac + (k * J) * cap + m;
     const double old = ni[k], next = solved[k] > 0 ? solved[k] : 0;
     const double d = next - old;
     ni[k] = next;
-    stm(R.ni + k * cap + m, next);
-    const double mx = ldm(R.maxni + k * cap + m);
-    if (d > 0 && mx == 0) stm(R.relvel + k * cap + m, closingNow[k]);
-    if (d > mx) stm(R.maxni + k * cap + m, d);
+    rvset[k] = d > 0 && mx[k] == 0;
+    rv[k] = closingNow[k];
+    if (d > mx[k]) mx[k] = d;
     const double px = nx * d, py = ny * d, pz = nz * d;
     vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
     vbx += imb * px; vby += imb * py; vbz += imb * pz;
-    wax -= ldm(jac + 6 * cap) * d; way -= ldm(jac + 7 * cap) * d; waz -= ldm(jac + 8 * cap) * d;
-    wbx += ldm(jac + 9 * cap) * d; wby += ldm(jac + 10 * cap) * d; wbz += ldm(jac + 11 * cap) * d;
+    wax -= jw[k][0] * d; way -= jw[k][1] * d; waz -= jw[k][2] * d;
+    wbx += jw[k][3] * d; wby += jw[k][4] * d; wbz += jw[k][5] * d;
   }
-  const double mu = ldi(R.friction + m);
-  const double t1x = ldi(R.t1 + m), t1y = ldi(R.t1 + cap + m), t1z = ldi(R.t1 + 2 * cap + m);
-  const double t2x = ldi(R.t2 + m), t2y = ldi(R.t2 + cap + m), t2z = ldi(R.t2 + 2 * cap + m);
   double pressed = 0, twisted = 0;
 #pragma unroll
   for (int k = 0; k < N; k++) {
     pressed += ni[k];
-    twisted += ldm(R.lever + k * cap + m) * ni[k];
+    twisted += lev[k] * ni[k];
   }
+  double n1f, n2f;
+  uint8_t sliding;
   {
-    double fj[FJ];
-#pragma unroll
-    for (int c = 0; c < FJ; c++) fj[c] = ldm(R.fjac + c * cap + m);
     const double* g = fj + 12;
     const double dvx = vbx - vax, dvy = vby - vay, dvz = vbz - vaz;
     double v1 = dvx * t1x + dvy * t1y + dvz * t1z + wbx * fj[3] + wby * fj[4] + wbz * fj[5] - wax * fj[0] - way * fj[1] - waz * fj[2];
     double v2 = dvx * t2x + dvy * t2y + dvz * t2z + wbx * g[3] + wby * g[4] + wbz * g[5] - wax * g[0] - way * g[1] - waz * g[2];
-    const double s1 = ldm(R.drift1 + m), s2 = ldm(R.drift2 + m);
     if (bias && (s1 != 0 || s2 != 0)) {
       double b1 = soft.biasRate * s1, b2 = soft.biasRate * s2;
       const double bb = b1 * b1 + b2 * b2;
@@ -908,8 +998,6 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
       }
       v1 += b1; v2 += b2;
     }
-    const double tm0 = ldm(R.tm + m), tm1 = ldm(R.tm + cap + m), tm2 = ldm(R.tm + 2 * cap + m);
-    const double o1 = ldm(R.ti1 + m), o2 = ldm(R.ti2 + m);
     double n1 = o1 - (tm0 * v1 + tm1 * v2), n2 = o2 - (tm1 * v1 + tm2 * v2);
     const double limit = mu * pressed, l2 = n1 * n1 + n2 * n2;
     if (l2 > limit * limit) {
@@ -931,11 +1019,11 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
       }
       const double scale = limit / sqrt(ll);
       n1 = x * scale; n2 = y * scale;
-      stm(R.sliding + m, static_cast<uint8_t>(1));
+      sliding = 1;
     } else {
-      stm(R.sliding + m, static_cast<uint8_t>(0));
+      sliding = 0;
     }
-    stm(R.ti1 + m, n1); stm(R.ti2 + m, n2);
+    n1f = n1; n2f = n2;
     const double d1 = n1 - o1, d2 = n2 - o2;
     const double px = t1x * d1 + t2x * d2, py = t1y * d1 + t2y * d2, pz = t1z * d1 + t2z * d2;
     vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
@@ -945,18 +1033,18 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
   }
   const double* Ia = A.I;
   const double* Ib = Bb.I;
+  double r1f = 0, r2f = 0;
   if (N <= 2) {
-    const double most = ldi(R.patch + m) * pressed;
+    const double most = patch * pressed;
     const double ux = wbx - wax, uy = wby - way, uz = wbz - waz;
-    const double r1 = ldm(R.ri1 + m), r2 = ldm(R.ri2 + m);
-    double n1 = r1 - ldm(R.rm1 + m) * (ux * t1x + uy * t1y + uz * t1z);
-    double n2 = r2 - ldm(R.rm2 + m) * (ux * t2x + uy * t2y + uz * t2z);
+    double n1 = r1 - rm1 * (ux * t1x + uy * t1y + uz * t1z);
+    double n2 = r2 - rm2 * (ux * t2x + uy * t2y + uz * t2z);
     const double l2 = n1 * n1 + n2 * n2;
     if (l2 > most * most) {
       const double scale = most / sqrt(l2);
       n1 *= scale; n2 *= scale;
     }
-    stm(R.ri1 + m, n1); stm(R.ri2 + m, n2);
+    r1f = n1; r2f = n2;
     const double d1 = n1 - r1, d2 = n2 - r2;
     const double lx = t1x * d1 + t2x * d2, ly = t1y * d1 + t2y * d2, lz = t1z * d1 + t2z * d2;
     wax -= Ia[0] * lx + Ia[1] * ly + Ia[2] * lz;
@@ -966,13 +1054,13 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
     wby += Ib[1] * lx + Ib[3] * ly + Ib[4] * lz;
     wbz += Ib[2] * lx + Ib[4] * ly + Ib[5] * lz;
   }
+  double s1f;
   {
-    const double limit = N == 1 ? SPIN_DISC * mu * ldi(R.patch + m) * pressed : mu * twisted;
-    const double s0 = ldm(R.si + m);
-    double s1 = s0 - ldm(R.sm + m) * ((wbx - wax) * nx + (wby - way) * ny + (wbz - waz) * nz);
-    if (s1 > limit) s1 = limit; else if (s1 < -limit) s1 = -limit;
-    stm(R.si + m, s1);
-    const double ds = s1 - s0, lx = nx * ds, ly = ny * ds, lz = nz * ds;
+    const double limit = N == 1 ? SPIN_DISC * mu * patch * pressed : mu * twisted;
+    double sv = s0 - smass * ((wbx - wax) * nx + (wby - way) * ny + (wbz - waz) * nz);
+    if (sv > limit) sv = limit; else if (sv < -limit) sv = -limit;
+    s1f = sv;
+    const double ds = sv - s0, lx = nx * ds, ly = ny * ds, lz = nz * ds;
     wax -= Ia[0] * lx + Ia[1] * ly + Ia[2] * lz;
     way -= Ia[1] * lx + Ia[3] * ly + Ia[4] * lz;
     waz -= Ia[2] * lx + Ia[4] * ly + Ia[5] * lz;
@@ -980,17 +1068,35 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
     wby += Ib[1] * lx + Ib[3] * ly + Ib[4] * lz;
     wbz += Ib[2] * lx + Ib[4] * ly + Ib[5] * lz;
   }
+  // ---- every store, last: the bodies first, which the rows after this one wait for ----
   write_back(B, ima, a, vax, vay, vaz, wax, way, waz);
   write_back(B, imb, b, vbx, vby, vbz, wbx, wby, wbz);
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    if (!known && !bias) stm(R.now + k * cap + m, nowv[k]);
+    stm(R.ni + k * cap + m, ni[k]);
+    if (rvset[k]) stm(R.relvel + k * cap + m, rv[k]);
+    stm(R.maxni + k * cap + m, mx[k]);
+  }
+  stm(R.gap + m, least);
+  stm(R.sliding + m, sliding);
+  stm(R.ti1 + m, n1f); stm(R.ti2 + m, n2f);
+  if (N <= 2) { stm(R.ri1 + m, r1f); stm(R.ri2 + m, r2f); }
+  stm(R.si + m, s1f);
+}
+
+template <class Gate>
+__device__ __forceinline__ void solve_row(const StageParams& p, int m, double h, bool bias, bool known, Gate gate) {
+  switch (ldi(p.R.points + m)) {
+    case 1: solve_row_n<1>(p, m, h, bias, known, gate); break;
+    case 2: solve_row_n<2>(p, m, h, bias, known, gate); break;
+    case 3: solve_row_n<3>(p, m, h, bias, known, gate); break;
+    default: solve_row_n<4>(p, m, h, bias, known, gate); break;
+  }
 }
 
 __device__ __forceinline__ void solve_row(const StageParams& p, int m, double h, bool bias, bool known) {
-  switch (ldi(p.R.points + m)) {
-    case 1: solve_row_n<1>(p, m, h, bias, known); break;
-    case 2: solve_row_n<2>(p, m, h, bias, known); break;
-    case 3: solve_row_n<3>(p, m, h, bias, known); break;
-    default: solve_row_n<4>(p, m, h, bias, known); break;
-  }
+  solve_row(p, m, h, bias, known, OpenGate());
 }
 
 // Whether row m has a point restitution() works on: src/contact.js:2233-2241.  What it reads
@@ -1254,43 +1360,56 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
     t.each(0, w.solved, [&](int m) { prepare_row(p, r0 + m); });
     if (!t.sync(p)) return false;
   }
+  int pass = 0;   // row passes so far: the dataflow counters' epoch
   for (int sub = 0; sub < substeps; sub++) {
     t.each(0, w.nawake, [&](int i) { accelerate_body(p, ldi(p.B.awake_list + w.awake0 + i), h, w.gravity); });
     if (!t.sync(p)) return false;
     if (touching) {
-      for (int k = 0; k < NCOLOURS; k++) {
-        if (starts[k + 1] <= starts[k]) continue;
-        t.each(starts[k], starts[k + 1], [&](int m) { warm_row(p, r0 + m); });
+      if (Team::kGrid && p.nchunks > 0) {
+        // warm and solve flow into each other: a solve row waits for its bodies' warm rows
+        flow_pass(p, pass++, [&](int m, auto gate) { warm_row(p, m, gate); });
+        flow_pass(p, pass++, [&](int m, auto gate) { solve_row(p, m, h, true, sub > 0, gate); });
         if (!t.sync(p)) return false;
-      }
-      if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
-        if (t.rank == 0)
-          for (int m = starts[OVERFLOW_RUN]; m < starts[OVERFLOW_RUN + 1]; m++) warm_row(p, r0 + m);
-        if (!t.sync(p)) return false;
-      }
-      for (int k = 0; k < NCOLOURS; k++) {
-        if (starts[k + 1] <= starts[k]) continue;
-        t.each(starts[k], starts[k + 1], [&](int m) { solve_row(p, r0 + m, h, true, sub > 0); });
-        if (!t.sync(p)) return false;
-      }
-      if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
-        if (t.rank == 0)
-          for (int m = starts[OVERFLOW_RUN]; m < starts[OVERFLOW_RUN + 1]; m++) solve_row(p, r0 + m, h, true, sub > 0);
-        if (!t.sync(p)) return false;
+      } else {
+        for (int k = 0; k < NCOLOURS; k++) {
+          if (starts[k + 1] <= starts[k]) continue;
+          t.each(starts[k], starts[k + 1], [&](int m) { warm_row(p, r0 + m, OpenGate()); });
+          if (!t.sync(p)) return false;
+        }
+        if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
+          if (t.rank == 0)
+            for (int m = starts[OVERFLOW_RUN]; m < starts[OVERFLOW_RUN + 1]; m++) warm_row(p, r0 + m, OpenGate());
+          if (!t.sync(p)) return false;
+        }
+        for (int k = 0; k < NCOLOURS; k++) {
+          if (starts[k + 1] <= starts[k]) continue;
+          t.each(starts[k], starts[k + 1], [&](int m) { solve_row(p, r0 + m, h, true, sub > 0); });
+          if (!t.sync(p)) return false;
+        }
+        if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
+          if (t.rank == 0)
+            for (int m = starts[OVERFLOW_RUN]; m < starts[OVERFLOW_RUN + 1]; m++) solve_row(p, r0 + m, h, true, sub > 0);
+          if (!t.sync(p)) return false;
+        }
       }
     }
     t.each(0, w.nawake, [&](int i) { move_body(p, ldi(p.B.awake_list + w.awake0 + i), h); });
     if (!t.sync(p)) return false;
     if (touching) {
-      for (int k = 0; k < NCOLOURS; k++) {
-        if (starts[k + 1] <= starts[k]) continue;
-        t.each(starts[k], starts[k + 1], [&](int m) { solve_row(p, r0 + m, h, false, false); });
+      if (Team::kGrid && p.nchunks > 0) {
+        flow_pass(p, pass++, [&](int m, auto gate) { solve_row(p, m, h, false, false, gate); });
         if (!t.sync(p)) return false;
-      }
-      if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
-        if (t.rank == 0)
-          for (int m = starts[OVERFLOW_RUN]; m < starts[OVERFLOW_RUN + 1]; m++) solve_row(p, r0 + m, h, false, false);
-        if (!t.sync(p)) return false;
+      } else {
+        for (int k = 0; k < NCOLOURS; k++) {
+          if (starts[k + 1] <= starts[k]) continue;
+          t.each(starts[k], starts[k + 1], [&](int m) { solve_row(p, r0 + m, h, false, false); });
+          if (!t.sync(p)) return false;
+        }
+        if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
+          if (t.rank == 0)
+            for (int m = starts[OVERFLOW_RUN]; m < starts[OVERFLOW_RUN + 1]; m++) solve_row(p, r0 + m, h, false, false);
+          if (!t.sync(p)) return false;
+        }
       }
     }
   }
