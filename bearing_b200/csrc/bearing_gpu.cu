@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cstdarg>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -894,3 +895,230 @@ int32_t bg_batch_solve_step(bg_ctx* c, const bg_bodies* B, const bg_rows* R, con
 }
 
 }  // extern "C"
+
+// ---- the solve stage without allocation --------------------------------------------------
+//
+// bg_solve_step_static: for callers that may not allocate device memory themselves, such as a
+// host runtime (a game engine's or a JavaScript embedding's) that owns every device buffer in a
+// pool of its own and hands this library only pointers into it, or a per-frame loop that cannot
+// take the device-wide synchronisation a cudaMalloc may cause.  Its working memory is one
+// file-scope device array, sized for a world of at most BG_STATIC_MAX_BODIES slots and
+// BG_STATIC_MAX_ROWS rows, which every GPU that loads this library holds until the process ends.
+
+namespace {
+
+constexpr int kStaticBodies = BG_STATIC_MAX_BODIES;
+constexpr int kStaticRows = BG_STATIC_MAX_ROWS;
+// Per slot: vw 8, mi 8, pq 8, st 4, sq 4, tc 4, pr 12 doubles, then fl, awake, head, deg, done.
+constexpr size_t kStaticBodyDoubles = 48;
+// Per row, doubles: n 3, t1 3, t2 3, friction, restitution, tolerance, patch, separation 4,
+// point 12, shift 12, ni 4, ti1, ti2, ri1, ri2, si, drift1, drift2, gap, maxni 4, relvel 4,
+// anchorA 3, anchorB 3, la 12, lb 12, adjusted 4, now 4, normalMass 4, lever 4, jac 48, K 16,
+// fjac 24, tm 3, rm1, rm2, sm; then ints a, b, row, active, pending, rank_a, rank_b; bytes
+// points, sliding.
+constexpr size_t kStaticRowDoubles = 3 + 3 + 3 + 4 + 4 + 12 + 12 + 4 + 7 + 1 + 4 + 4 + 3 + 3 + 12 + 12 + 4 + 4 + 4 + 4 + 48 +
+                                     16 + 24 + 3 + 3;
+constexpr size_t kStaticBytes =
+    256 + kStaticBodies * (kStaticBodyDoubles * 8 + 5 * 4) + kStaticRows * (kStaticRowDoubles * 8 + 7 * 4 + 2) + 4096;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+// The scratch array's device address, per device: set up by the first call on that device.
+void* g_static_addr[64] = {};
+std::mutex g_static_mutex;
+
+struct StaticIn {
+  bg_bodies B;
+  bg_rows R;
+};
+
+__global__ void __launch_bounds__(kBlockThreads) stage_static(StaticIn in, unsigned char* base, double dt, int substeps,
+                                                               bg::Soft soft, double gx, double gy, double gz) {
+  const bg_bodies& Bi = in.B;
+  const bg_rows& Ri = in.R;
+  const int nb = Bi.capacity, nr = Ri.count, na = Bi.awake_count;
+  const int64_t cap = kStaticRows;
+  // Carve the scratch array: status word first, then the bodies' records, then the rows' columns.
+  int32_t* status = reinterpret_cast<int32_t*>(base);
+  double* d = reinterpret_cast<double*>(base + 256);
+  bg::BodiesDev B;
+  B.vw = d; d += 8 * kStaticBodies;
+  B.mi = d; d += 8 * kStaticBodies;
+  B.pq = d; d += 8 * kStaticBodies;
+  B.st = d; d += 4 * kStaticBodies;
+  B.sq = d; d += 4 * kStaticBodies;
+  B.tc = d; d += 4 * kStaticBodies;
+  B.pr = d; d += 12 * kStaticBodies;
+  bg::RowsDev R;
+  R.cap = cap;
+  R.n = d; d += 3 * cap; R.t1 = d; d += 3 * cap; R.t2 = d; d += 3 * cap;
+  R.friction = d; d += cap; R.restitution = d; d += cap; R.tolerance = d; d += cap; R.patch = d; d += cap;
+  R.separation = d; d += 4 * cap; R.point = d; d += 12 * cap; R.shift = d; d += 12 * cap; R.ni = d; d += 4 * cap;
+  R.ti1 = d; d += cap; R.ti2 = d; d += cap; R.ri1 = d; d += cap; R.ri2 = d; d += cap; R.si = d; d += cap;
+  R.drift1 = d; d += cap; R.drift2 = d; d += cap; R.gap = d; d += cap; R.maxni = d; d += 4 * cap; R.relvel = d; d += 4 * cap;
+  R.anchorA = d; d += 3 * cap; R.anchorB = d; d += 3 * cap; R.la = d; d += 12 * cap; R.lb = d; d += 12 * cap;
+  R.adjusted = d; d += 4 * cap; R.now = d; d += 4 * cap; R.normalMass = d; d += 4 * cap; R.lever = d; d += 4 * cap;
+  R.jac = d; d += 48 * cap; R.K = d; d += 16 * cap; R.fjac = d; d += 24 * cap; R.tm = d; d += 3 * cap;
+  R.rm1 = d; d += cap; R.rm2 = d; d += cap; R.sm = d; d += cap;
+  int32_t* q = reinterpret_cast<int32_t*>(d);
+  B.fl = reinterpret_cast<uint32_t*>(q); q += kStaticBodies;
+  B.awake_list = q; q += kStaticBodies;
+  B.head = q; q += kStaticBodies;
+  B.deg = q; q += kStaticBodies;
+  B.done = reinterpret_cast<unsigned int*>(q); q += kStaticBodies;
+  R.a = q; q += cap; R.b = q; q += cap; R.row = q; q += cap; R.active = q; q += cap; R.pending = q; q += cap;
+  R.rank_a = q; q += cap; R.rank_b = q; q += cap;
+  uint8_t* u = reinterpret_cast<uint8_t*>(q);
+  R.points = u; u += cap;
+  R.sliding = u; u += cap;
+  if (threadIdx.x == 0) *status = 0;
+  // The caller's layout in: what every call must set afresh, since the array keeps the last
+  // call's contents.
+  for (int s = threadIdx.x; s < nb; s += blockDim.x) {
+    for (int k = 0; k < 3; k++) {
+      B.vw[8 * s + k] = Bi.velocity[3 * s + k];
+      B.vw[8 * s + 3 + k] = Bi.angular[3 * s + k];
+      B.pq[8 * s + k] = Bi.position[3 * s + k];
+      B.st[4 * s + k] = Bi.start[3 * s + k];
+      B.tc[4 * s + k] = Bi.tumbled[3 * s + k];
+      B.pr[12 * s + k] = Bi.inertia[3 * s + k];
+      B.pr[12 * s + 3 + k] = Bi.inv_inertia[3 * s + k];
+      B.pr[12 * s + 6 + k] = Bi.dims[3 * s + k];
+    }
+    for (int k = 0; k < 4; k++) { B.pq[8 * s + 4 + k] = Bi.rotation[4 * s + k]; B.sq[4 * s + k] = 0; }
+    B.tc[4 * s + 3] = Bi.ceiling[s];
+    B.pr[12 * s + 9] = Bi.damping[s];
+    B.pr[12 * s + 10] = Bi.angular_damping[s];
+    B.pr[12 * s + 11] = Bi.gravity_scale[s];
+    B.mi[8 * s] = Bi.inv_mass[s];
+    for (int k = 0; k < 6; k++) B.mi[8 * s + 1 + k] = Bi.inv_i[6 * s + k];
+    uint32_t f = static_cast<uint32_t>(Bi.type[s]) & bg::F_TYPE;
+    f |= (static_cast<uint32_t>(Bi.shape[s]) & 3u) << bg::F_SHAPE_SHIFT;
+    if (Bi.frozen[s]) f |= bg::F_FROZEN;
+    if (Bi.framed[s]) f |= bg::F_FRAMED;
+    f |= (static_cast<uint32_t>(Bi.lock[s]) & 7u) << bg::F_LOCK_SHIFT;
+    if (Bi.joint_head[s] != 0) f |= bg::F_JOINTED;
+    if (Bi.awake[s]) f |= bg::F_AWAKE;
+    B.fl[s] = f;
+    B.head[s] = 0x7fffffff;
+  }
+  for (int i = threadIdx.x; i < na; i += blockDim.x) B.awake_list[i] = Bi.awake_list[i];
+  for (int m = threadIdx.x; m < nr; m += blockDim.x) {
+    R.row[m] = Ri.row[m];
+    R.a[m] = Ri.a[m];
+    R.b[m] = Ri.b[m];
+    R.points[m] = Ri.points[m];
+    for (int c = 0; c < 3; c++) {
+      R.n[c * cap + m] = Ri.normal[3 * m + c];
+      R.t1[c * cap + m] = Ri.t1[3 * m + c];
+      R.t2[c * cap + m] = Ri.t2[3 * m + c];
+      R.anchorA[c * cap + m] = 0;
+      R.anchorB[c * cap + m] = 0;
+    }
+    R.friction[m] = Ri.friction[m];
+    R.restitution[m] = Ri.restitution[m];
+    R.tolerance[m] = Ri.tolerance[m];
+    R.patch[m] = Ri.patch[m];
+    R.gap[m] = Ri.gap[m];
+    R.sliding[m] = 0;
+    for (int k = 0; k < bg::P; k++) {
+      R.maxni[k * cap + m] = Ri.max_normal_impulse[bg::P * m + k];
+      R.relvel[k * cap + m] = Ri.relative_velocity[bg::P * m + k];
+      R.separation[k * cap + m] = Ri.separation[bg::P * m + k];
+      R.ni[k * cap + m] = Ri.normal_impulse[bg::P * m + k];
+      for (int c = 0; c < 3; c++) {
+        R.point[(k * 3 + c) * cap + m] = Ri.point[12 * m + 3 * k + c];
+        R.shift[(k * 3 + c) * cap + m] = Ri.shift[12 * m + 3 * k + c];
+      }
+    }
+    R.ti1[m] = Ri.tangent_impulse1[m]; R.ti2[m] = Ri.tangent_impulse2[m];
+    R.ri1[m] = Ri.roll_impulse1[m]; R.ri2[m] = Ri.roll_impulse2[m];
+    R.si[m] = Ri.spin_impulse[m]; R.drift1[m] = Ri.drift1[m]; R.drift2[m] = Ri.drift2[m];
+  }
+  __syncthreads();
+  bg::WorldDesc w = {};
+  w.nbodies = nb;
+  w.nawake = na;
+  w.nrows = nr;
+  w.solved = Ri.solved;
+  for (int k = 0; k < bg::NSTARTS; k++) w.starts[k] = Ri.starts[k];
+  w.gravity[0] = gx; w.gravity[1] = gy; w.gravity[2] = gz;
+  bg::StageParams p = {};
+  p.B = B;
+  p.R = R;
+  p.worlds = nullptr;
+  p.nworlds = 1;
+  p.dt = dt;
+  p.substeps = substeps;
+  p.soft = soft;
+  p.status = status;
+  p.budget = kDefaultBudget;
+  p.chunks = nullptr;
+  p.nchunks = 0;
+  bg::BlockTeam t;
+  bg::solve_stage(p, w, t);
+  __syncthreads();
+  // The written columns back into the caller's arrays.
+  for (int s = threadIdx.x; s < nb; s += blockDim.x) {
+    for (int k = 0; k < 3; k++) {
+      Bi.velocity[3 * s + k] = B.vw[8 * s + k];
+      Bi.angular[3 * s + k] = B.vw[8 * s + 3 + k];
+      Bi.position[3 * s + k] = B.pq[8 * s + k];
+      Bi.start[3 * s + k] = B.st[4 * s + k];
+      Bi.tumbled[3 * s + k] = B.tc[4 * s + k];
+    }
+    for (int k = 0; k < 4; k++) { Bi.rotation[4 * s + k] = B.pq[8 * s + 4 + k]; Bi.start_q[4 * s + k] = B.sq[4 * s + k]; }
+    Bi.ceiling[s] = B.tc[4 * s + 3];
+    for (int k = 0; k < 6; k++) Bi.inv_i[6 * s + k] = B.mi[8 * s + 1 + k];
+  }
+  for (int m = threadIdx.x; m < nr; m += blockDim.x) {
+    for (int k = 0; k < bg::P; k++) {
+      Ri.normal_impulse[bg::P * m + k] = R.ni[k * cap + m];
+      Ri.max_normal_impulse[bg::P * m + k] = R.maxni[k * cap + m];
+      Ri.relative_velocity[bg::P * m + k] = R.relvel[k * cap + m];
+    }
+    Ri.tangent_impulse1[m] = R.ti1[m]; Ri.tangent_impulse2[m] = R.ti2[m];
+    Ri.roll_impulse1[m] = R.ri1[m]; Ri.roll_impulse2[m] = R.ri2[m];
+    Ri.spin_impulse[m] = R.si[m]; Ri.drift1[m] = R.drift1[m]; Ri.drift2[m] = R.drift2[m];
+    Ri.gap[m] = R.gap[m];
+    Ri.sliding[m] = R.sliding[m];
+    for (int c = 0; c < 3; c++) {
+      if (Ri.anchor_a) Ri.anchor_a[3 * m + c] = R.anchorA[c * cap + m];
+      if (Ri.anchor_b) Ri.anchor_b[3 * m + c] = R.anchorB[c * cap + m];
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int32_t bg_solve_step_static(const bg_bodies* bodies, const bg_rows* rows, const bg_step* step, void* stream) {
+  if (bodies == nullptr || rows == nullptr || step == nullptr) return BG_EINVAL;
+  if (bodies->capacity < 0 || bodies->capacity > BG_STATIC_MAX_BODIES || bodies->awake_count < 0 ||
+      bodies->awake_count > bodies->capacity || rows->count < 0 || rows->count > BG_STATIC_MAX_ROWS ||
+      rows->solved < 0 || rows->solved > rows->count || rows->starts[bg::RESTING_RUN] != rows->solved ||
+      !(step->dt > 0) || step->substeps < 1)
+    return BG_EINVAL;
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return BG_ECUDA;
+  void* base = nullptr;
+  {
+    // First call on this device: the array's device address, looked up with the device current.
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (g_static_addr[device] == nullptr) {
+      void* ptr = nullptr;
+      if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || ptr == nullptr) return BG_ECUDA;
+      g_static_addr[device] = ptr;
+    }
+    base = g_static_addr[device];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  StaticIn in{*bodies, *rows};
+  stage_static<<<1, kBlockThreads, 0, s>>>(in, static_cast<unsigned char*>(base), step->dt, step->substeps,
+                                           make_soft(step->dt / step->substeps), step->gravity[0], step->gravity[1],
+                                           step->gravity[2]);
+  if (cudaGetLastError() != cudaSuccess) return BG_ECUDA;
+  int32_t status = 0;
+  if (cudaMemcpyAsync(&status, base, sizeof status, cudaMemcpyDeviceToHost, s) != cudaSuccess) return BG_ECUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return BG_ECUDA;
+  return status == 0 ? BG_OK : BG_ETIMEOUT;
+}

@@ -215,6 +215,31 @@ double bg_last_stage_ms(bg_ctx* ctx);
  * 0 restores the default.  A wait past its budget makes the step return BG_ETIMEOUT. */
 int32_t bg_set_wait_budget(bg_ctx* ctx, int64_t iterations);
 
+/*
+ * The solve stage without allocating: no counterpart in the reference.
+ *
+ * For callers that may not allocate device memory themselves: a host runtime (a game engine's,
+ * or a JavaScript embedding's) that keeps every device buffer in a pool of its own and hands
+ * this library only pointers into it, or a per-frame loop that cannot afford the device-wide
+ * synchronisation a cudaMalloc may bring.  The caller passes the same structures as
+ * bg_solve_step, but every array they point to is DEVICE memory the caller owns; the written
+ * columns are written back into those arrays.  The stage runs in one CTA on `stream` (a
+ * cudaStream_t; NULL for the default stream) and the call returns when it is done.
+ *
+ * Its working memory is one fixed device array inside this library, of about 4 MiB, which every
+ * GPU that loads the library holds until the process exits; so a world may have at most
+ * BG_STATIC_MAX_BODIES slots and BG_STATIC_MAX_ROWS rows, and larger ones are refused with
+ * BG_EINVAL (use bg_solve_step for those).  The first call on a device looks up that array's
+ * device address with the device current; make that first call before any stream capture.  All
+ * calls share the one array: calls that overlap on the GPU (other streams, other host threads)
+ * race, so run them one after another.  It calls no cudaMalloc or cudaFree.
+ * Returns BG_OK, BG_EINVAL, BG_ECUDA, or BG_ETIMEOUT as bg_solve_step does; there is no context,
+ * so no bg_last_error text.
+ */
+#define BG_STATIC_MAX_BODIES 512
+#define BG_STATIC_MAX_ROWS 2048
+int32_t bg_solve_step_static(const bg_bodies* bodies, const bg_rows* rows, const bg_step* step, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
