@@ -196,8 +196,15 @@ def host() -> C.CDLL:
         lib.bw_transforms.restype = C.POINTER(C.c_float)
         lib.bw_transforms.argtypes = [C.c_void_p]
         lib.bw_stats_get.argtypes = [C.c_void_p, C.POINTER(Stats)]
+        lib.bw_batch_create.restype = C.c_void_p
+        lib.bw_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int32]
+        lib.bw_batch_destroy.argtypes = [C.c_void_p]
+        lib.bw_batch_begin_step.argtypes = [C.c_void_p, C.c_double, C.c_int32]
+        lib.bw_batch_views.argtypes = [C.c_void_p, C.POINTER(Bodies), C.POINTER(Rows), C.POINTER(Worlds), C.POINTER(Step)]
+        lib.bw_batch_end_step.argtypes = [C.c_void_p, C.c_int32]
         for f in ("bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step", "bw_end_step",
-                  "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_stats_get"):
+                  "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_stats_get", "bw_batch_begin_step",
+                  "bw_batch_views", "bw_batch_end_step"):
             getattr(lib, f).restype = C.c_int32
         _host = lib
     return _host
@@ -253,4 +260,5 @@ GPU_SYMBOLS = [
 HOST_SYMBOLS = [
     "bw_create", "bw_destroy", "bw_last_error", "bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step",
     "bw_end_step", "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_transforms", "bw_stats_get",
+    "bw_batch_create", "bw_batch_destroy", "bw_batch_begin_step", "bw_batch_views", "bw_batch_end_step",
 ]

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -878,6 +879,217 @@ const float* bw_transforms(const bw_world* w) { return w == nullptr ? nullptr : 
 int32_t bw_stats_get(const bw_world* w, bw_stats* out) {
   if (w == nullptr || out == nullptr) return BG_EINVAL;
   *out = w->stats;
+  return BG_OK;
+}
+
+}  // extern "C"
+
+// ---- batches of worlds ----
+
+namespace {
+
+// Runs f(i) for i in [0, n) on up to `threads` threads, each taking every threads-th index.
+template <class F>
+void parallel(int n, int threads, F f) {
+  if (threads <= 1 || n <= 1) {
+    for (int i = 0; i < n; i++) f(i);
+    return;
+  }
+  const int t = threads < n ? threads : n;
+  std::vector<std::thread> pool;
+  for (int k = 0; k < t; k++)
+    pool.emplace_back([&, k] {
+      for (int i = k; i < n; i += t) f(i);
+    });
+  for (auto& th : pool) th.join();
+}
+
+template <class T>
+struct Col {
+  std::vector<T> v;
+  T* at(size_t off) { return v.data() + off; }
+};
+
+}  // namespace
+
+struct bw_batch {
+  std::vector<bw_world*> worlds;
+  std::vector<int32_t> body_off, awake_off, row_off, starts;
+  // bodies, end to end
+  std::vector<double> position, rotation, velocity, angular, tumbled, ceiling, start, startQ, invI, invMass, inertia,
+      invInertia, dims, damping, angularDamping, gravityScale;
+  std::vector<uint8_t> type, shape, frozen, framed, lock, awake;
+  std::vector<int32_t> jointHead, awakeList;
+  // rows, end to end
+  std::vector<int32_t> row, a, b;
+  std::vector<uint8_t> points, sliding;
+  std::vector<double> normal, t1, t2, friction, restitution, tolerance, patch, separation, point, shift, normalImpulse,
+      tangentImpulse1, tangentImpulse2, rollImpulse1, rollImpulse2, spinImpulse, drift1, drift2, gap, maxNormalImpulse,
+      relativeVelocity, anchorA, anchorB;
+  double dt = 0;
+  bool begun = false;
+};
+
+namespace {
+
+template <class T>
+void put(std::vector<T>& dst, size_t off, const T* src, size_t n) {
+  if (n) std::memcpy(dst.data() + off, src, n * sizeof(T));
+}
+template <class T>
+void take(const std::vector<T>& src, size_t off, T* dst, size_t n) {
+  if (n) std::memcpy(dst, src.data() + off, n * sizeof(T));
+}
+
+}  // namespace
+
+extern "C" {
+
+bw_batch* bw_batch_create(bw_world* const* worlds, int32_t count) {
+  if (worlds == nullptr || count < 1) return nullptr;
+  bw_batch* b = new bw_batch();
+  b->worlds.assign(worlds, worlds + count);
+  for (bw_world* w : b->worlds)
+    if (w == nullptr) {
+      delete b;
+      return nullptr;
+    }
+  return b;
+}
+
+void bw_batch_destroy(bw_batch* b) { delete b; }
+
+int32_t bw_batch_begin_step(bw_batch* b, double dt, int32_t threads) {
+  if (b == nullptr) return BG_EINVAL;
+  const int n = static_cast<int>(b->worlds.size());
+  std::vector<int32_t> rcs(static_cast<size_t>(n), 0);
+  parallel(n, threads, [&](int i) { rcs[static_cast<size_t>(i)] = bw_begin_step(b->worlds[static_cast<size_t>(i)], dt); });
+  for (int32_t rc : rcs)
+    if (rc != BG_OK) return rc;
+  b->body_off.assign(static_cast<size_t>(n) + 1, 0);
+  b->awake_off.assign(static_cast<size_t>(n) + 1, 0);
+  b->row_off.assign(static_cast<size_t>(n) + 1, 0);
+  b->starts.assign(static_cast<size_t>(n) * BG_STARTS, 0);
+  for (int i = 0; i < n; i++) {
+    bw_world* w = b->worlds[static_cast<size_t>(i)];
+    b->body_off[i + 1] = b->body_off[i] + w->n;
+    b->awake_off[i + 1] = b->awake_off[i] + w->awakeCount;
+    b->row_off[i + 1] = b->row_off[i] + w->c.count;
+    for (int k = 0; k < BG_STARTS; k++) b->starts[static_cast<size_t>(i) * BG_STARTS + k] = w->c.starts[k];
+  }
+  const size_t nb = static_cast<size_t>(b->body_off[n]), na = static_cast<size_t>(b->awake_off[n]),
+               nr = static_cast<size_t>(b->row_off[n]);
+  auto sz = [](auto& v, size_t k) { v.resize(k > 0 ? k : 1); };
+  sz(b->position, 3 * nb); sz(b->rotation, 4 * nb); sz(b->velocity, 3 * nb); sz(b->angular, 3 * nb);
+  sz(b->tumbled, 3 * nb); sz(b->ceiling, nb); sz(b->start, 3 * nb); sz(b->startQ, 4 * nb); sz(b->invI, 6 * nb);
+  sz(b->invMass, nb); sz(b->inertia, 3 * nb); sz(b->invInertia, 3 * nb); sz(b->dims, 3 * nb); sz(b->damping, nb);
+  sz(b->angularDamping, nb); sz(b->gravityScale, nb); sz(b->type, nb); sz(b->shape, nb); sz(b->frozen, nb);
+  sz(b->framed, nb); sz(b->lock, nb); sz(b->awake, nb); sz(b->jointHead, nb); sz(b->awakeList, na);
+  sz(b->row, nr); sz(b->a, nr); sz(b->b, nr); sz(b->points, nr); sz(b->sliding, nr); sz(b->normal, 3 * nr);
+  sz(b->t1, 3 * nr); sz(b->t2, 3 * nr); sz(b->friction, nr); sz(b->restitution, nr); sz(b->tolerance, nr);
+  sz(b->patch, nr); sz(b->separation, 4 * nr); sz(b->point, 12 * nr); sz(b->shift, 12 * nr); sz(b->normalImpulse, 4 * nr);
+  sz(b->tangentImpulse1, nr); sz(b->tangentImpulse2, nr); sz(b->rollImpulse1, nr); sz(b->rollImpulse2, nr);
+  sz(b->spinImpulse, nr); sz(b->drift1, nr); sz(b->drift2, nr); sz(b->gap, nr); sz(b->maxNormalImpulse, 4 * nr);
+  sz(b->relativeVelocity, 4 * nr); sz(b->anchorA, 3 * nr); sz(b->anchorB, 3 * nr);
+  parallel(n, threads, [&](int i) {
+    bw_world* w = b->worlds[static_cast<size_t>(i)];
+    const size_t o = static_cast<size_t>(b->body_off[i]), q = static_cast<size_t>(b->awake_off[i]),
+                 r = static_cast<size_t>(b->row_off[i]), s = static_cast<size_t>(w->n), m = static_cast<size_t>(w->c.count);
+    put(b->position, 3 * o, w->position.data(), 3 * s); put(b->rotation, 4 * o, w->rotation.data(), 4 * s);
+    put(b->velocity, 3 * o, w->velocity.data(), 3 * s); put(b->angular, 3 * o, w->angular.data(), 3 * s);
+    put(b->tumbled, 3 * o, w->tumbled.data(), 3 * s); put(b->ceiling, o, w->ceiling.data(), s);
+    put(b->start, 3 * o, w->start.data(), 3 * s); put(b->startQ, 4 * o, w->startQ.data(), 4 * s);
+    put(b->invI, 6 * o, w->invI.data(), 6 * s); put(b->invMass, o, w->invMass.data(), s);
+    put(b->inertia, 3 * o, w->inertia.data(), 3 * s); put(b->invInertia, 3 * o, w->invInertia.data(), 3 * s);
+    put(b->dims, 3 * o, w->dims.data(), 3 * s); put(b->damping, o, w->damping.data(), s);
+    put(b->angularDamping, o, w->angularDamping.data(), s); put(b->gravityScale, o, w->gravityScale.data(), s);
+    put(b->type, o, w->type.data(), s); put(b->shape, o, w->shape.data(), s); put(b->frozen, o, w->frozen.data(), s);
+    put(b->framed, o, w->framed.data(), s); put(b->lock, o, w->lock.data(), s); put(b->awake, o, w->awake.data(), s);
+    put(b->jointHead, o, w->jointHead.data(), s);
+    put(b->awakeList, q, w->awakeList.data(), static_cast<size_t>(w->awakeCount));
+    Contacts& c = w->c;
+    put(b->row, r, c.row.data(), m); put(b->a, r, c.a.data(), m); put(b->b, r, c.b.data(), m);
+    put(b->points, r, c.points.data(), m); put(b->sliding, r, c.sliding.data(), m);
+    put(b->normal, 3 * r, c.normal.data(), 3 * m); put(b->t1, 3 * r, c.t1.data(), 3 * m); put(b->t2, 3 * r, c.t2.data(), 3 * m);
+    put(b->friction, r, c.friction.data(), m); put(b->restitution, r, c.restitution.data(), m);
+    put(b->tolerance, r, c.tolerance.data(), m); put(b->patch, r, c.patch.data(), m);
+    put(b->separation, 4 * r, c.separation.data(), 4 * m); put(b->point, 12 * r, c.point.data(), 12 * m);
+    put(b->shift, 12 * r, c.shift.data(), 12 * m); put(b->normalImpulse, 4 * r, c.normalImpulse.data(), 4 * m);
+    put(b->tangentImpulse1, r, c.tangentImpulse1.data(), m); put(b->tangentImpulse2, r, c.tangentImpulse2.data(), m);
+    put(b->rollImpulse1, r, c.rollImpulse1.data(), m); put(b->rollImpulse2, r, c.rollImpulse2.data(), m);
+    put(b->spinImpulse, r, c.spinImpulse.data(), m); put(b->drift1, r, c.drift1.data(), m); put(b->drift2, r, c.drift2.data(), m);
+    put(b->gap, r, c.gap.data(), m); put(b->maxNormalImpulse, 4 * r, c.maxNormalImpulse.data(), 4 * m);
+    put(b->relativeVelocity, 4 * r, c.relativeVelocity.data(), 4 * m);
+    put(b->anchorA, 3 * r, c.anchorA.data(), 3 * m); put(b->anchorB, 3 * r, c.anchorB.data(), 3 * m);
+  });
+  b->dt = dt;
+  b->begun = true;
+  return BG_OK;
+}
+
+int32_t bw_batch_views(bw_batch* b, bg_bodies* B, bg_rows* R, bg_worlds* W, bg_step* S) {
+  if (b == nullptr || !b->begun || B == nullptr || R == nullptr || W == nullptr || S == nullptr) return BG_EINVAL;
+  const size_t n = b->worlds.size();
+  B->capacity = b->body_off[n];
+  B->awake_count = b->awake_off[n];
+  B->awake_list = b->awakeList.data(); B->awake = b->awake.data();
+  B->position = b->position.data(); B->rotation = b->rotation.data(); B->velocity = b->velocity.data();
+  B->angular = b->angular.data(); B->tumbled = b->tumbled.data(); B->ceiling = b->ceiling.data();
+  B->start = b->start.data(); B->start_q = b->startQ.data(); B->inv_i = b->invI.data();
+  B->inv_mass = b->invMass.data(); B->inertia = b->inertia.data(); B->inv_inertia = b->invInertia.data();
+  B->dims = b->dims.data(); B->damping = b->damping.data(); B->angular_damping = b->angularDamping.data();
+  B->gravity_scale = b->gravityScale.data(); B->type = b->type.data(); B->shape = b->shape.data();
+  B->frozen = b->frozen.data(); B->framed = b->framed.data(); B->lock = b->lock.data(); B->joint_head = b->jointHead.data();
+  R->count = b->row_off[n];
+  R->solved = 0;
+  for (int k = 0; k < BG_STARTS; k++) R->starts[k] = 0;
+  R->row = b->row.data(); R->a = b->a.data(); R->b = b->b.data(); R->points = b->points.data();
+  R->normal = b->normal.data(); R->t1 = b->t1.data(); R->t2 = b->t2.data(); R->friction = b->friction.data();
+  R->restitution = b->restitution.data(); R->tolerance = b->tolerance.data(); R->patch = b->patch.data();
+  R->separation = b->separation.data(); R->point = b->point.data(); R->shift = b->shift.data();
+  R->normal_impulse = b->normalImpulse.data(); R->tangent_impulse1 = b->tangentImpulse1.data();
+  R->tangent_impulse2 = b->tangentImpulse2.data(); R->roll_impulse1 = b->rollImpulse1.data();
+  R->roll_impulse2 = b->rollImpulse2.data(); R->spin_impulse = b->spinImpulse.data(); R->drift1 = b->drift1.data();
+  R->drift2 = b->drift2.data(); R->gap = b->gap.data(); R->max_normal_impulse = b->maxNormalImpulse.data();
+  R->relative_velocity = b->relativeVelocity.data(); R->sliding = b->sliding.data(); R->anchor_a = b->anchorA.data();
+  R->anchor_b = b->anchorB.data();
+  W->count = static_cast<int32_t>(n);
+  W->body_offset = b->body_off.data();
+  W->awake_offset = b->awake_off.data();
+  W->row_offset = b->row_off.data();
+  W->starts = b->starts.data();
+  W->gravity = nullptr;
+  bw_step_params(b->worlds[0], S);
+  S->dt = b->dt;
+  return BG_OK;
+}
+
+int32_t bw_batch_end_step(bw_batch* b, int32_t threads) {
+  if (b == nullptr || !b->begun) return BG_EINVAL;
+  b->begun = false;
+  const int n = static_cast<int>(b->worlds.size());
+  std::vector<int32_t> rcs(static_cast<size_t>(n), 0);
+  parallel(n, threads, [&](int i) {
+    bw_world* w = b->worlds[static_cast<size_t>(i)];
+    const size_t o = static_cast<size_t>(b->body_off[i]), r = static_cast<size_t>(b->row_off[i]),
+                 s = static_cast<size_t>(w->n), m = static_cast<size_t>(w->c.count);
+    take(b->position, 3 * o, w->position.data(), 3 * s); take(b->rotation, 4 * o, w->rotation.data(), 4 * s);
+    take(b->velocity, 3 * o, w->velocity.data(), 3 * s); take(b->angular, 3 * o, w->angular.data(), 3 * s);
+    take(b->tumbled, 3 * o, w->tumbled.data(), 3 * s); take(b->ceiling, o, w->ceiling.data(), s);
+    take(b->start, 3 * o, w->start.data(), 3 * s); take(b->startQ, 4 * o, w->startQ.data(), 4 * s);
+    take(b->invI, 6 * o, w->invI.data(), 6 * s);
+    Contacts& c = w->c;
+    take(b->normalImpulse, 4 * r, c.normalImpulse.data(), 4 * m);
+    take(b->tangentImpulse1, r, c.tangentImpulse1.data(), m); take(b->tangentImpulse2, r, c.tangentImpulse2.data(), m);
+    take(b->rollImpulse1, r, c.rollImpulse1.data(), m); take(b->rollImpulse2, r, c.rollImpulse2.data(), m);
+    take(b->spinImpulse, r, c.spinImpulse.data(), m); take(b->drift1, r, c.drift1.data(), m); take(b->drift2, r, c.drift2.data(), m);
+    take(b->gap, r, c.gap.data(), m); take(b->maxNormalImpulse, 4 * r, c.maxNormalImpulse.data(), 4 * m);
+    take(b->relativeVelocity, 4 * r, c.relativeVelocity.data(), 4 * m); take(b->sliding, r, c.sliding.data(), m);
+    take(b->anchorA, 3 * r, c.anchorA.data(), 3 * m); take(b->anchorB, 3 * r, c.anchorB.data(), 3 * m);
+    rcs[static_cast<size_t>(i)] = bw_end_step(w);
+  });
+  for (int32_t rc : rcs)
+    if (rc != BG_OK) return rc;
   return BG_OK;
 }
 

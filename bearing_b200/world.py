@@ -215,3 +215,62 @@ class World:
             self.destroy()
         except Exception:
             pass
+
+
+class Batch:
+    """Many independent worlds stepped together: each world's host side on CPU threads, then one
+    launch solves every world's stage on the GPU, one CTA a world (bg_batch_solve_step)."""
+
+    def __init__(self, worlds, device: int = 0, threads: int | None = None):
+        import os as _os
+        self.worlds = list(worlds)
+        self._lib = _ffi.host()
+        self._gpu = _ffi.gpu()
+        arr = (C.c_void_p * len(self.worlds))(*[w._w for w in self.worlds])
+        self._b = self._lib.bw_batch_create(arr, len(self.worlds))
+        if not self._b:
+            raise BearingError("Batch: no worlds")
+        self.ctx = self._gpu.bg_create(device, 0)
+        if not self.ctx:
+            raise BearingError(f"bg_create({device}) failed: no usable CUDA device")
+        self.threads = threads or max(1, (_os.cpu_count() or 1))
+
+    def begin_step(self, dt: float):
+        rc = self._lib.bw_batch_begin_step(self._b, float(dt), self.threads)
+        if rc != 0:
+            raise BearingError(f"batch step failed ({rc})")
+
+    def views(self):
+        B, R, W, S = _ffi.Bodies(), _ffi.Rows(), _ffi.Worlds(), _ffi.Step()
+        rc = self._lib.bw_batch_views(self._b, C.byref(B), C.byref(R), C.byref(W), C.byref(S))
+        if rc != 0:
+            raise BearingError("batch views: no step begun")
+        return B, R, W, S
+
+    def end_step(self):
+        rc = self._lib.bw_batch_end_step(self._b, self.threads)
+        if rc != 0:
+            raise BearingError(f"batch end step failed ({rc})")
+
+    def step(self, dt: float):
+        """One step of every world: host sides, one batched GPU launch, host sides again."""
+        self.begin_step(dt)
+        B, R, W, S = self.views()
+        rc = self._gpu.bg_batch_solve_step(self.ctx, C.byref(B), C.byref(R), C.byref(W), C.byref(S))
+        if rc != 0:
+            raise BearingError(f"batched solve failed ({rc}): {self._gpu.bg_last_error(self.ctx).decode()}")
+        self.end_step()
+
+    def destroy(self):
+        if self._b:
+            self._lib.bw_batch_destroy(self._b)
+            self._b = None
+        if self.ctx:
+            self._gpu.bg_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -220,6 +220,20 @@ def cpu_solve_times(copy, workers, sample):
     return times
 
 
+def measured_traffic(bodies, at):
+    """DRAM bytes per launch of the stage kernel from the committed ncu summary, if it was taken
+    on this workload (profiles/stage_grid_pile50k_dram.md), else None."""
+    if bodies != 50_000 or at != 300:
+        return None
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "stage_grid_pile50k_dram.md")):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -340,7 +354,7 @@ def main():
                 "e2e": {"value": e2e, "unit": "rows/s", "ms_per_step": ms_e2e, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                             "frac": achieved / hbm, "traffic": None, "kernel_ms": ms_stage,
+                             "frac": achieved / hbm, "traffic": measured_traffic(args.bodies, args.at), "kernel_ms": ms_stage,
                              "algorithmic_bytes": algo, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
                 "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches}
         print(json.dumps(line), flush=True)

@@ -92,6 +92,19 @@ int32_t bw_bodies_view(bw_world* world, bg_bodies* out);
 int32_t bw_rows_view(bw_world* world, bg_rows* out);
 int32_t bw_step_params(const bw_world* world, bg_step* out);
 
+/*
+ * Many worlds stepped together (no reference counterpart: a Bearing World steps alone).  The
+ * batch does each world's host side on `threads` CPU threads, then lays every world's solve-stage
+ * input end to end, as bg_batch_solve_step (bearing_gpu.h) takes it; bw_batch_end_step hands each
+ * world its part of the result back and finishes its step.  The worlds stay owned by the caller.
+ */
+typedef struct bw_batch bw_batch;
+bw_batch* bw_batch_create(bw_world* const* worlds, int32_t count);
+void bw_batch_destroy(bw_batch* batch);
+int32_t bw_batch_begin_step(bw_batch* batch, double dt, int32_t threads);
+int32_t bw_batch_views(bw_batch* batch, bg_bodies* bodies, bg_rows* rows, bg_worlds* worlds, bg_step* step);
+int32_t bw_batch_end_step(bw_batch* batch, int32_t threads);
+
 /* World.transforms: 7 floats per slot (position, rotation x y z w). */
 const float* bw_transforms(const bw_world* world);
 int32_t bw_stats_get(const bw_world* world, bw_stats* out);

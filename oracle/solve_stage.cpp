@@ -2,11 +2,11 @@
 // solve stage, used by tests/ and by bench.py's CPU-baseline leg as the checker and the timed
 // CPU baseline.  The product path (libbearing_gpu.so) never links or calls anything here.
 //
-// Parity status: the reference is JavaScript and no JS engine exists in this environment, so
+// Parity unpinned: the reference is JavaScript and no JS engine exists in this environment, so
 // no output of the reference itself can be produced here, and the reference's tests hold no
-// stored numeric vectors.  This restatement is pinned against the reference's behavioural
-// tests and published fingerprints (tests/test_oracle_*.py), and the CUDA path is pinned
-// against it bit for bit.
+// stored numeric vectors.  This restatement is checked against the reference's behavioural
+// tests and published measurements (tests/test_oracle_behaviour.py), and the CUDA path is
+// pinned against it bit for bit (tests/test_gpu_parity.py).
 //
 // Every function follows the reference's operation order exactly, in IEEE FP64, compiled
 // with -ffp-contract=off and no fast-math, so each + - * / sqrt rounds as JavaScript's does.
