@@ -203,34 +203,47 @@ struct GridTeam {
 // order, so the earliest waiting row always has every predecessor done or running: no cycle.
 // Every wait is bounded by the step's budget; past it the status word is set and all waits end.
 
-__device__ __forceinline__ unsigned int load_acquire(const unsigned int* p) {
+// Both bodies' counters are read together with relaxed loads and a single acq_rel fence follows
+// once both are far enough (the PTX memory model's fence-based acquire pattern); a row's writes are
+// published the same way, one fence and then relaxed stores (the release pattern).  Two ld.acquire
+// in a row would cost two trips to L2 on every row's critical path; this costs one.
+__device__ __forceinline__ unsigned int load_relaxed(const unsigned int* p) {
   unsigned int v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void store_release(unsigned int* p, unsigned int v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void store_relaxed(unsigned int* p, unsigned int v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// The count body x must reach before row m of `pass` may move it (0: no wait; a static body, or
+// the body's first row of the first pass).
+__device__ __forceinline__ unsigned int flow_target(const StageParams& p, int x, int rank, int pass) {
+  return rank < 0 ? 0u : static_cast<unsigned int>(pass) * static_cast<unsigned int>(ldi(p.B.deg + x)) +
+                             static_cast<unsigned int>(rank);
 }
 
-__device__ __forceinline__ bool wait_body(const StageParams& p, int x, int rank, int pass) {
-  if (rank < 0) return true;
-  const unsigned int target = static_cast<unsigned int>(pass) * static_cast<unsigned int>(ldi(p.B.deg + x)) +
-                              static_cast<unsigned int>(rank);
+__device__ __forceinline__ bool flow_wait(const StageParams& p, int a, unsigned int ta, int b, unsigned int tb) {
   long long it = 0;
-  while (load_acquire(p.B.done + x) < target) {
+  for (;;) {
+    const unsigned int va = ta == 0 ? 0u : load_relaxed(p.B.done + a);
+    const unsigned int vb = tb == 0 ? 0u : load_relaxed(p.B.done + b);
+    if (va >= ta && vb >= tb) break;
     if (++it > p.budget || ((it & 255) == 0 && *(volatile int32_t*)p.status != 0)) {
       atomicExch(p.status, 1);
       return false;
     }
   }
+  fence_acq_rel();
   return true;
 }
 
-__device__ __forceinline__ void signal_body(const StageParams& p, int x, int rank, int pass) {
-  if (rank < 0) return;
-  const unsigned int next = static_cast<unsigned int>(pass) * static_cast<unsigned int>(ldi(p.B.deg + x)) +
-                            static_cast<unsigned int>(rank) + 1u;
-  store_release(p.B.done + x, next);
+__device__ __forceinline__ void flow_signal(const StageParams& p, int a, int ra, unsigned int ta, int b, int rb,
+                                            unsigned int tb) {
+  fence_acq_rel();
+  if (ra >= 0) store_relaxed(p.B.done + a, ta + 1u);
+  if (rb >= 0) store_relaxed(p.B.done + b, tb + 1u);
 }
 
 template <class F>
@@ -244,12 +257,10 @@ __device__ __forceinline__ void flow_pass(const StageParams& p, int pass, F row)
       const int m = run.x + lane;
       const int a = ldi(p.R.a + m), b = ldi(p.R.b + m);
       const int ra = ldi(p.R.rank_a + m), rb = ldi(p.R.rank_b + m);
+      const unsigned int ta = flow_target(p, a, ra, pass), tb = flow_target(p, b, rb, pass);
       bool open = false;
-      row(m, [&]() { open = wait_body(p, a, ra, pass) && wait_body(p, b, rb, pass); return open; });
-      if (open) {
-        signal_body(p, a, ra, pass);
-        signal_body(p, b, rb, pass);
-      }
+      row(m, [&]() { open = flow_wait(p, a, ta, b, tb); return open; });
+      if (open) flow_signal(p, a, ra, ta, b, rb, tb);
     }
     __syncwarp();
   }
