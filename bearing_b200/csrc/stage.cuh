@@ -224,21 +224,6 @@ __device__ __forceinline__ unsigned int flow_target(const StageParams& p, int x,
                              static_cast<unsigned int>(rank);
 }
 
-__device__ __forceinline__ bool flow_wait(const StageParams& p, int a, unsigned int ta, int b, unsigned int tb) {
-  long long it = 0;
-  for (;;) {
-    const unsigned int va = ta == 0 ? 0u : load_relaxed(p.B.done + a);
-    const unsigned int vb = tb == 0 ? 0u : load_relaxed(p.B.done + b);
-    if (va >= ta && vb >= tb) break;
-    if (++it > p.budget || ((it & 255) == 0 && *(volatile int32_t*)p.status != 0)) {
-      atomicExch(p.status, 1);
-      return false;
-    }
-  }
-  fence_acq_rel();
-  return true;
-}
-
 __device__ __forceinline__ void flow_signal(const StageParams& p, int a, int ra, unsigned int ta, int b, int rb,
                                             unsigned int tb) {
   fence_acq_rel();
@@ -258,9 +243,27 @@ __device__ __forceinline__ void flow_pass(const StageParams& p, int pass, F row)
       const int a = ldi(p.R.a + m), b = ldi(p.R.b + m);
       const int ra = ldi(p.R.rank_a + m), rb = ldi(p.R.rank_b + m);
       const unsigned int ta = flow_target(p, a, ra, pass), tb = flow_target(p, b, rb, pass);
-      bool open = false;
-      row(m, [&]() { open = flow_wait(p, a, ta, b, tb); return open; });
-      if (open) flow_signal(p, a, ra, ta, b, rb, tb);
+      // The row's rest runs inside the wait, so each lane goes on the moment its own bodies are
+      // ready rather than when the whole run's are; a lane still waiting sleeps between polls,
+      // which lets the warp run the lanes that are ready.
+      row(m, [&](auto&& finish) {
+        long long it = 0;
+        for (;;) {
+          const unsigned int va = ta == 0 ? 0u : load_relaxed(p.B.done + a);
+          const unsigned int vb = tb == 0 ? 0u : load_relaxed(p.B.done + b);
+          if (va >= ta && vb >= tb) {
+            fence_acq_rel();
+            finish();
+            flow_signal(p, a, ra, ta, b, rb, tb);
+            return true;
+          }
+          if (++it > p.budget || ((it & 255) == 0 && *(volatile int32_t*)p.status != 0)) {
+            atomicExch(p.status, 1);
+            return false;
+          }
+          __nanosleep(200);
+        }
+      });
     }
     __syncwarp();
   }
@@ -653,8 +656,14 @@ __device__ __forceinline__ void write_back(const BodiesDev& B, double im, int s,
   stm(vw, vx); stm(vw + 1, vy); stm(vw + 2, vz); stm(vw + 3, wx); stm(vw + 4, wy); stm(vw + 5, wz);
 }
 
+// A row's gate: gate(finish) runs `finish` (the row once its bodies are ready) and says whether it
+// ran.  OpenGate runs it at once (a CTA's colour-by-colour passes); the grid's waits for its bodies.
 struct OpenGate {
-  __device__ __forceinline__ bool operator()() const { return true; }
+  template <class F>
+  __device__ __forceinline__ bool operator()(F&& finish) const {
+    finish();
+    return true;
+  }
 };
 
 // warmRows for row m: src/contact.js:1616-1663, for a row of N points.  Every array index below
@@ -690,44 +699,45 @@ __device__ __forceinline__ void warm_row_n(const StageParams& p, int m, Gate gat
   }
   const double l1 = ldm(R.ti1 + m), l2 = ldm(R.ti2 + m);
   const double r1 = ldm(R.ri1 + m), r2 = ldm(R.ri2 + m), sp = ldm(R.si + m);
-  if (!gate()) return;
-  BodyLoad A, Bb;
-  load_mass(B, a, A);
-  load_mass(B, b, Bb);
-  const double ima = A.im, imb = Bb.im;
-  const double* va = B.vw + 8 * a;
-  const double* vb = B.vw + 8 * b;
-  double vax = ldm(va), vay = ldm(va + 1), vaz = ldm(va + 2), wax = ldm(va + 3), way = ldm(va + 4), waz = ldm(va + 5);
-  double vbx = ldm(vb), vby = ldm(vb + 1), vbz = ldm(vb + 2), wbx = ldm(vb + 3), wby = ldm(vb + 4), wbz = ldm(vb + 5);
+  gate([&]() {
+    BodyLoad A, Bb;
+    load_mass(B, a, A);
+    load_mass(B, b, Bb);
+    const double ima = A.im, imb = Bb.im;
+    const double* va = B.vw + 8 * a;
+    const double* vb = B.vw + 8 * b;
+    double vax = ldm(va), vay = ldm(va + 1), vaz = ldm(va + 2), wax = ldm(va + 3), way = ldm(va + 4), waz = ldm(va + 5);
+    double vbx = ldm(vb), vby = ldm(vb + 1), vbz = ldm(vb + 2), wbx = ldm(vb + 3), wby = ldm(vb + 4), wbz = ldm(vb + 5);
 #pragma unroll
-  for (int k = 0; k < N; k++) {
-    const double l = ln[k];
-    const double px = nx * l, py = ny * l, pz = nz * l;
-    vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
-    vbx += imb * px; vby += imb * py; vbz += imb * pz;
-    wax -= ia[k][0] * l; way -= ia[k][1] * l; waz -= ia[k][2] * l;
-    wbx += ib[k][0] * l; wby += ib[k][1] * l; wbz += ib[k][2] * l;
-  }
-  {
-    const double px = t1x * l1 + t2x * l2, py = t1y * l1 + t2y * l2, pz = t1z * l1 + t2z * l2;
-    vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
-    vbx += imb * px; vby += imb * py; vbz += imb * pz;
-    wax -= fa[0] * l1 + fa[3] * l2; way -= fa[1] * l1 + fa[4] * l2; waz -= fa[2] * l1 + fa[5] * l2;
-    wbx += fb[0] * l1 + fb[3] * l2; wby += fb[1] * l1 + fb[4] * l2; wbz += fb[2] * l1 + fb[5] * l2;
-  }
-  {
-    const double* Ia = A.I;
-    const double* Ib = Bb.I;
-    const double lx = t1x * r1 + t2x * r2 + nx * sp, ly = t1y * r1 + t2y * r2 + ny * sp, lz = t1z * r1 + t2z * r2 + nz * sp;
-    wax -= Ia[0] * lx + Ia[1] * ly + Ia[2] * lz;
-    way -= Ia[1] * lx + Ia[3] * ly + Ia[4] * lz;
-    waz -= Ia[2] * lx + Ia[4] * ly + Ia[5] * lz;
-    wbx += Ib[0] * lx + Ib[1] * ly + Ib[2] * lz;
-    wby += Ib[1] * lx + Ib[3] * ly + Ib[4] * lz;
-    wbz += Ib[2] * lx + Ib[4] * ly + Ib[5] * lz;
-  }
-  write_back(B, ima, a, vax, vay, vaz, wax, way, waz);
-  write_back(B, imb, b, vbx, vby, vbz, wbx, wby, wbz);
+    for (int k = 0; k < N; k++) {
+      const double l = ln[k];
+      const double px = nx * l, py = ny * l, pz = nz * l;
+      vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
+      vbx += imb * px; vby += imb * py; vbz += imb * pz;
+      wax -= ia[k][0] * l; way -= ia[k][1] * l; waz -= ia[k][2] * l;
+      wbx += ib[k][0] * l; wby += ib[k][1] * l; wbz += ib[k][2] * l;
+    }
+    {
+      const double px = t1x * l1 + t2x * l2, py = t1y * l1 + t2y * l2, pz = t1z * l1 + t2z * l2;
+      vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
+      vbx += imb * px; vby += imb * py; vbz += imb * pz;
+      wax -= fa[0] * l1 + fa[3] * l2; way -= fa[1] * l1 + fa[4] * l2; waz -= fa[2] * l1 + fa[5] * l2;
+      wbx += fb[0] * l1 + fb[3] * l2; wby += fb[1] * l1 + fb[4] * l2; wbz += fb[2] * l1 + fb[5] * l2;
+    }
+    {
+      const double* Ia = A.I;
+      const double* Ib = Bb.I;
+      const double lx = t1x * r1 + t2x * r2 + nx * sp, ly = t1y * r1 + t2y * r2 + ny * sp, lz = t1z * r1 + t2z * r2 + nz * sp;
+      wax -= Ia[0] * lx + Ia[1] * ly + Ia[2] * lz;
+      way -= Ia[1] * lx + Ia[3] * ly + Ia[4] * lz;
+      waz -= Ia[2] * lx + Ia[4] * ly + Ia[5] * lz;
+      wbx += Ib[0] * lx + Ib[1] * ly + Ib[2] * lz;
+      wby += Ib[1] * lx + Ib[3] * ly + Ib[4] * lz;
+      wbz += Ib[2] * lx + Ib[4] * ly + Ib[5] * lz;
+    }
+    write_back(B, ima, a, vax, vay, vaz, wax, way, waz);
+    write_back(B, imb, b, vbx, vby, vbz, wbx, wby, wbz);
+  });
 }
 
 template <class Gate>
@@ -804,9 +814,10 @@ __device__ __forceinline__ void pushes_n(const double (&K)[N][N], int set, const
 }
 
 // solveRows for row m, one pass, a row of N points: src/contact.js:1805-2090.  The row's own
-// columns are read first, then `gate` (the grid's wait for the rows before it on its bodies; nothing
-// for a CTA), then its two bodies; every store is held to the end.  So once the gate opens, the
-// row costs one trip to memory (its bodies' records) and its arithmetic.
+// columns are read first; the rest (its two bodies, the arithmetic, every store at the end) is
+// handed to `gate`, which runs it once the rows before it on its bodies are done (the grid) or at
+// once (a CTA).  So once its bodies are ready, the row costs one trip to memory (their records)
+// and its arithmetic.
 template <int N, class Gate>
 __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bool known, Gate gate) {
   const RowsDev& R = p.R;
@@ -871,229 +882,230 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
   }
   const double s0 = ldm(R.si + m), smass = ldm(R.sm + m);
   // ---- the rows before this one on its bodies ----
-  if (!gate()) return;
-  // ---- its bodies ----
-  BodyLoad A, Bb;
-  load_mass(B, a, A);
-  load_mass(B, b, Bb);
-  const double* va = B.vw + 8 * a;
-  const double* vb = B.vw + 8 * b;
-  double vax = ldm(va), vay = ldm(va + 1), vaz = ldm(va + 2), wax = ldm(va + 3), way = ldm(va + 4), waz = ldm(va + 5);
-  double vbx = ldm(vb), vby = ldm(vb + 1), vbz = ldm(vb + 2), wbx = ldm(vb + 3), wby = ldm(vb + 4), wbz = ldm(vb + 5);
-  double dn = 0, nax = 0, nay = 0, naz = 0, nbx = 0, nby = 0, nbz = 0;
-  if (!known) {
-    const double* pqa = B.pq + 8 * a;
-    const double* pqb = B.pq + 8 * b;
-    const double* sta = B.st + 4 * a;
-    const double* stb = B.st + 4 * b;
-    const double dx = (ldm(pqb) - ldm(stb)) - (ldm(pqa) - ldm(sta));
-    const double dy = (ldm(pqb + 1) - ldm(stb + 1)) - (ldm(pqa + 1) - ldm(sta + 1));
-    const double dz = (ldm(pqb + 2) - ldm(stb + 2)) - (ldm(pqa + 2) - ldm(sta + 2));
-    dn = dx * nx + dy * ny + dz * nz;
-    double qa[4], qb[4], v3[3];
+  gate([&]() {
+    // ---- its bodies ----
+    BodyLoad A, Bb;
+    load_mass(B, a, A);
+    load_mass(B, b, Bb);
+    const double* va = B.vw + 8 * a;
+    const double* vb = B.vw + 8 * b;
+    double vax = ldm(va), vay = ldm(va + 1), vaz = ldm(va + 2), wax = ldm(va + 3), way = ldm(va + 4), waz = ldm(va + 5);
+    double vbx = ldm(vb), vby = ldm(vb + 1), vbz = ldm(vb + 2), wbx = ldm(vb + 3), wby = ldm(vb + 4), wbz = ldm(vb + 5);
+    double dn = 0, nax = 0, nay = 0, naz = 0, nbx = 0, nby = 0, nbz = 0;
+    if (!known) {
+      const double* pqa = B.pq + 8 * a;
+      const double* pqb = B.pq + 8 * b;
+      const double* sta = B.st + 4 * a;
+      const double* stb = B.st + 4 * b;
+      const double dx = (ldm(pqb) - ldm(stb)) - (ldm(pqa) - ldm(sta));
+      const double dy = (ldm(pqb + 1) - ldm(stb + 1)) - (ldm(pqa + 1) - ldm(sta + 1));
+      const double dz = (ldm(pqb + 2) - ldm(stb + 2)) - (ldm(pqa + 2) - ldm(sta + 2));
+      dn = dx * nx + dy * ny + dz * nz;
+      double qa[4], qb[4], v3[3];
 #pragma unroll
-    for (int k = 0; k < 4; k++) { qa[k] = ldm(pqa + 4 + k); qb[k] = ldm(pqb + 4 + k); }
-    rotate(qa, nx, ny, nz, true, v3);
-    nax = v3[0]; nay = v3[1]; naz = v3[2];
-    rotate(qb, nx, ny, nz, true, v3);
-    nbx = v3[0]; nby = v3[1]; nbz = v3[2];
-  }
-  // ---- the arithmetic, in the reference's order ----
-  double target[N], massScale[N], impulseScale[N], give[N], nowv[N];
-  double least = INFINITY;
-#pragma unroll
-  for (int k = 0; k < N; k++) {
-    double s;
-    if (known) {
-      s = sep[k];
-    } else {
-      s = dn + (lb[k][0] * nbx + lb[k][1] * nby + lb[k][2] * nbz) - (la[k][0] * nax + la[k][1] * nay + la[k][2] * naz)
-        + sep[k];
+      for (int k = 0; k < 4; k++) { qa[k] = ldm(pqa + 4 + k); qb[k] = ldm(pqb + 4 + k); }
+      rotate(qa, nx, ny, nz, true, v3);
+      nax = v3[0]; nay = v3[1]; naz = v3[2];
+      rotate(qb, nx, ny, nz, true, v3);
+      nbx = v3[0]; nby = v3[1]; nbz = v3[2];
     }
-    nowv[k] = s;
-    if (s < least) least = s;
-    if (s > 0) {
-      target[k] = s * inv; massScale[k] = 1; impulseScale[k] = 0; give[k] = COMPLIANCE;
-    } else if (bias) {
-      target[k] = js_max(soft.biasRate * s, -maxBias);
-      massScale[k] = soft.massScale; impulseScale[k] = soft.impulseScale; give[k] = springy;
-    } else {
-      target[k] = 0; massScale[k] = 1; impulseScale[k] = 0; give[k] = COMPLIANCE;
-    }
-  }
-  const double ima = A.im, imb = Bb.im;
-  double closingNow[N], solved[N];
-  if (N == 1 || !(Kb[0][0] > 0)) {
+    // ---- the arithmetic, in the reference's order ----
+    double target[N], massScale[N], impulseScale[N], give[N], nowv[N];
+    double least = INFINITY;
 #pragma unroll
     for (int k = 0; k < N; k++) {
-      const double* jac = jn[k];
-      const double vn = (vbx - vax) * nx + (vby - vay) * ny + (vbz - vaz) * nz
-        + wbx * jac[3] + wby * jac[4] + wbz * jac[5] - wax * jac[0] - way * jac[1] - waz * jac[2];
-      const double old = ni[k];
-      double next = old - nmass[k] * massScale[k] * (vn + target[k]) - impulseScale[k] * old;
-      if (next < 0) next = 0;
-      closingNow[k] = vn; solved[k] = next;
+      double s;
+      if (known) {
+        s = sep[k];
+      } else {
+        s = dn + (lb[k][0] * nbx + lb[k][1] * nby + lb[k][2] * nbz) - (la[k][0] * nax + la[k][1] * nay + la[k][2] * naz)
+          + sep[k];
+      }
+      nowv[k] = s;
+      if (s < least) least = s;
+      if (s > 0) {
+        target[k] = s * inv; massScale[k] = 1; impulseScale[k] = 0; give[k] = COMPLIANCE;
+      } else if (bias) {
+        target[k] = js_max(soft.biasRate * s, -maxBias);
+        massScale[k] = soft.massScale; impulseScale[k] = soft.impulseScale; give[k] = springy;
+      } else {
+        target[k] = 0; massScale[k] = 1; impulseScale[k] = 0; give[k] = COMPLIANCE;
+      }
     }
-  } else {
-#pragma unroll
-    for (int k = 0; k < N; k++) {
-      const double* jac = jn[k];
-      closingNow[k] = (vbx - vax) * nx + (vby - vay) * ny + (vbz - vaz) * nz
-        + wbx * jac[3] + wby * jac[4] + wbz * jac[5] - wax * jac[0] - way * jac[1] - waz * jac[2];
-    }
-    double wanted[N];
-    int set = 0;
-#pragma unroll
-    for (int k = 0; k < N; k++) {
-      double r = -closingNow[k] - target[k];
-#pragma unroll
-      for (int l = 0; l < N; l++) r += Kb[k][l] * ni[l];
-      wanted[k] = r;
-      if (r > 0) set |= 1 << k;
-    }
-    for (int round = 0;; round++) {
-      pushes_n<N>(Kb, set, give, wanted, solved);
-      int flip = -1;
+    const double ima = A.im, imb = Bb.im;
+    double closingNow[N], solved[N];
+    if (N == 1 || !(Kb[0][0] > 0)) {
 #pragma unroll
       for (int k = 0; k < N; k++) {
-        if (flip < 0) {
-          if (set >> k & 1) {
-            if (solved[k] < 0) flip = k;
-          } else {
-            double r = -wanted[k];
+        const double* jac = jn[k];
+        const double vn = (vbx - vax) * nx + (vby - vay) * ny + (vbz - vaz) * nz
+          + wbx * jac[3] + wby * jac[4] + wbz * jac[5] - wax * jac[0] - way * jac[1] - waz * jac[2];
+        const double old = ni[k];
+        double next = old - nmass[k] * massScale[k] * (vn + target[k]) - impulseScale[k] * old;
+        if (next < 0) next = 0;
+        closingNow[k] = vn; solved[k] = next;
+      }
+    } else {
 #pragma unroll
-            for (int l = 0; l < N; l++) r += Kb[k][l] * solved[l];
-            if (r < 0) flip = k;
+      for (int k = 0; k < N; k++) {
+        const double* jac = jn[k];
+        closingNow[k] = (vbx - vax) * nx + (vby - vay) * ny + (vbz - vaz) * nz
+          + wbx * jac[3] + wby * jac[4] + wbz * jac[5] - wax * jac[0] - way * jac[1] - waz * jac[2];
+      }
+      double wanted[N];
+      int set = 0;
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        double r = -closingNow[k] - target[k];
+#pragma unroll
+        for (int l = 0; l < N; l++) r += Kb[k][l] * ni[l];
+        wanted[k] = r;
+        if (r > 0) set |= 1 << k;
+      }
+      for (int round = 0;; round++) {
+        pushes_n<N>(Kb, set, give, wanted, solved);
+        int flip = -1;
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          if (flip < 0) {
+            if (set >> k & 1) {
+              if (solved[k] < 0) flip = k;
+            } else {
+              double r = -wanted[k];
+#pragma unroll
+              for (int l = 0; l < N; l++) r += Kb[k][l] * solved[l];
+              if (r < 0) flip = k;
+            }
           }
         }
+        if (flip < 0 || round == 1 << N) break;
+        set ^= 1 << flip;
       }
-      if (flip < 0 || round == 1 << N) break;
-      set ^= 1 << flip;
     }
-  }
-  double rv[N];
-  bool rvset[N];
+    double rv[N];
+    bool rvset[N];
 #pragma unroll
-  for (int k = 0; k < N; k++) {
-    const double old = ni[k], next = solved[k] > 0 ? solved[k] : 0;
-    const double d = next - old;
-    ni[k] = next;
-    rvset[k] = d > 0 && mx[k] == 0;
-    rv[k] = closingNow[k];
-    if (d > mx[k]) mx[k] = d;
-    const double px = nx * d, py = ny * d, pz = nz * d;
-    vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
-    vbx += imb * px; vby += imb * py; vbz += imb * pz;
-    wax -= jw[k][0] * d; way -= jw[k][1] * d; waz -= jw[k][2] * d;
-    wbx += jw[k][3] * d; wby += jw[k][4] * d; wbz += jw[k][5] * d;
-  }
-  double pressed = 0, twisted = 0;
+    for (int k = 0; k < N; k++) {
+      const double old = ni[k], next = solved[k] > 0 ? solved[k] : 0;
+      const double d = next - old;
+      ni[k] = next;
+      rvset[k] = d > 0 && mx[k] == 0;
+      rv[k] = closingNow[k];
+      if (d > mx[k]) mx[k] = d;
+      const double px = nx * d, py = ny * d, pz = nz * d;
+      vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
+      vbx += imb * px; vby += imb * py; vbz += imb * pz;
+      wax -= jw[k][0] * d; way -= jw[k][1] * d; waz -= jw[k][2] * d;
+      wbx += jw[k][3] * d; wby += jw[k][4] * d; wbz += jw[k][5] * d;
+    }
+    double pressed = 0, twisted = 0;
 #pragma unroll
-  for (int k = 0; k < N; k++) {
-    pressed += ni[k];
-    twisted += lev[k] * ni[k];
-  }
-  double n1f, n2f;
-  uint8_t sliding;
-  {
-    const double* g = fj + 12;
-    const double dvx = vbx - vax, dvy = vby - vay, dvz = vbz - vaz;
-    double v1 = dvx * t1x + dvy * t1y + dvz * t1z + wbx * fj[3] + wby * fj[4] + wbz * fj[5] - wax * fj[0] - way * fj[1] - waz * fj[2];
-    double v2 = dvx * t2x + dvy * t2y + dvz * t2z + wbx * g[3] + wby * g[4] + wbz * g[5] - wax * g[0] - way * g[1] - waz * g[2];
-    if (bias && (s1 != 0 || s2 != 0)) {
-      double b1 = soft.biasRate * s1, b2 = soft.biasRate * s2;
-      const double bb = b1 * b1 + b2 * b2;
-      if (bb > maxBias * maxBias) {
-        const double scale = maxBias / sqrt(bb);
-        b1 *= scale; b2 *= scale;
+    for (int k = 0; k < N; k++) {
+      pressed += ni[k];
+      twisted += lev[k] * ni[k];
+    }
+    double n1f, n2f;
+    uint8_t sliding;
+    {
+      const double* g = fj + 12;
+      const double dvx = vbx - vax, dvy = vby - vay, dvz = vbz - vaz;
+      double v1 = dvx * t1x + dvy * t1y + dvz * t1z + wbx * fj[3] + wby * fj[4] + wbz * fj[5] - wax * fj[0] - way * fj[1] - waz * fj[2];
+      double v2 = dvx * t2x + dvy * t2y + dvz * t2z + wbx * g[3] + wby * g[4] + wbz * g[5] - wax * g[0] - way * g[1] - waz * g[2];
+      if (bias && (s1 != 0 || s2 != 0)) {
+        double b1 = soft.biasRate * s1, b2 = soft.biasRate * s2;
+        const double bb = b1 * b1 + b2 * b2;
+        if (bb > maxBias * maxBias) {
+          const double scale = maxBias / sqrt(bb);
+          b1 *= scale; b2 *= scale;
+        }
+        v1 += b1; v2 += b2;
       }
-      v1 += b1; v2 += b2;
-    }
-    double n1 = o1 - (tm0 * v1 + tm1 * v2), n2 = o2 - (tm1 * v1 + tm2 * v2);
-    const double limit = mu * pressed, l2 = n1 * n1 + n2 * n2;
-    if (l2 > limit * limit) {
-      const double ma = tm0, mb = tm1, mc = tm2;
-      double al = 0, x = n1, y = n2, ll = l2;
-      while (limit > 0) {
-        const double ab = al * mb, d = (1 + al * ma) * (1 + al * mc) - ab * ab;
-        const double px = ma * x + mb * y, py = mb * x + mc * y;
-        const double wx = ((1 + al * mc) * px - ab * py) / d, wy = ((1 + al * ma) * py - ab * px) / d;
-        const double lw = x * wx + y * wy;
-        if (!(lw > 0)) break;
-        const double next = al + (sqrt(ll) / limit - 1) * ll / lw;
-        if (!(next > al)) break;
-        al = next;
-        const double ab2 = al * mb, d2 = (1 + al * ma) * (1 + al * mc) - ab2 * ab2;
-        x = ((1 + al * mc) * n1 - ab2 * n2) / d2; y = ((1 + al * ma) * n2 - ab2 * n1) / d2;
-        ll = x * x + y * y;
-        if (!(ll > limit * limit)) break;
+      double n1 = o1 - (tm0 * v1 + tm1 * v2), n2 = o2 - (tm1 * v1 + tm2 * v2);
+      const double limit = mu * pressed, l2 = n1 * n1 + n2 * n2;
+      if (l2 > limit * limit) {
+        const double ma = tm0, mb = tm1, mc = tm2;
+        double al = 0, x = n1, y = n2, ll = l2;
+        while (limit > 0) {
+          const double ab = al * mb, d = (1 + al * ma) * (1 + al * mc) - ab * ab;
+          const double px = ma * x + mb * y, py = mb * x + mc * y;
+          const double wx = ((1 + al * mc) * px - ab * py) / d, wy = ((1 + al * ma) * py - ab * px) / d;
+          const double lw = x * wx + y * wy;
+          if (!(lw > 0)) break;
+          const double next = al + (sqrt(ll) / limit - 1) * ll / lw;
+          if (!(next > al)) break;
+          al = next;
+          const double ab2 = al * mb, d2 = (1 + al * ma) * (1 + al * mc) - ab2 * ab2;
+          x = ((1 + al * mc) * n1 - ab2 * n2) / d2; y = ((1 + al * ma) * n2 - ab2 * n1) / d2;
+          ll = x * x + y * y;
+          if (!(ll > limit * limit)) break;
+        }
+        const double scale = limit / sqrt(ll);
+        n1 = x * scale; n2 = y * scale;
+        sliding = 1;
+      } else {
+        sliding = 0;
       }
-      const double scale = limit / sqrt(ll);
-      n1 = x * scale; n2 = y * scale;
-      sliding = 1;
-    } else {
-      sliding = 0;
+      n1f = n1; n2f = n2;
+      const double d1 = n1 - o1, d2 = n2 - o2;
+      const double px = t1x * d1 + t2x * d2, py = t1y * d1 + t2y * d2, pz = t1z * d1 + t2z * d2;
+      vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
+      vbx += imb * px; vby += imb * py; vbz += imb * pz;
+      wax -= fj[6] * d1 + g[6] * d2; way -= fj[7] * d1 + g[7] * d2; waz -= fj[8] * d1 + g[8] * d2;
+      wbx += fj[9] * d1 + g[9] * d2; wby += fj[10] * d1 + g[10] * d2; wbz += fj[11] * d1 + g[11] * d2;
     }
-    n1f = n1; n2f = n2;
-    const double d1 = n1 - o1, d2 = n2 - o2;
-    const double px = t1x * d1 + t2x * d2, py = t1y * d1 + t2y * d2, pz = t1z * d1 + t2z * d2;
-    vax -= ima * px; vay -= ima * py; vaz -= ima * pz;
-    vbx += imb * px; vby += imb * py; vbz += imb * pz;
-    wax -= fj[6] * d1 + g[6] * d2; way -= fj[7] * d1 + g[7] * d2; waz -= fj[8] * d1 + g[8] * d2;
-    wbx += fj[9] * d1 + g[9] * d2; wby += fj[10] * d1 + g[10] * d2; wbz += fj[11] * d1 + g[11] * d2;
-  }
-  const double* Ia = A.I;
-  const double* Ib = Bb.I;
-  double r1f = 0, r2f = 0;
-  if (N <= 2) {
-    const double most = patch * pressed;
-    const double ux = wbx - wax, uy = wby - way, uz = wbz - waz;
-    double n1 = r1 - rm1 * (ux * t1x + uy * t1y + uz * t1z);
-    double n2 = r2 - rm2 * (ux * t2x + uy * t2y + uz * t2z);
-    const double l2 = n1 * n1 + n2 * n2;
-    if (l2 > most * most) {
-      const double scale = most / sqrt(l2);
-      n1 *= scale; n2 *= scale;
+    const double* Ia = A.I;
+    const double* Ib = Bb.I;
+    double r1f = 0, r2f = 0;
+    if (N <= 2) {
+      const double most = patch * pressed;
+      const double ux = wbx - wax, uy = wby - way, uz = wbz - waz;
+      double n1 = r1 - rm1 * (ux * t1x + uy * t1y + uz * t1z);
+      double n2 = r2 - rm2 * (ux * t2x + uy * t2y + uz * t2z);
+      const double l2 = n1 * n1 + n2 * n2;
+      if (l2 > most * most) {
+        const double scale = most / sqrt(l2);
+        n1 *= scale; n2 *= scale;
+      }
+      r1f = n1; r2f = n2;
+      const double d1 = n1 - r1, d2 = n2 - r2;
+      const double lx = t1x * d1 + t2x * d2, ly = t1y * d1 + t2y * d2, lz = t1z * d1 + t2z * d2;
+      wax -= Ia[0] * lx + Ia[1] * ly + Ia[2] * lz;
+      way -= Ia[1] * lx + Ia[3] * ly + Ia[4] * lz;
+      waz -= Ia[2] * lx + Ia[4] * ly + Ia[5] * lz;
+      wbx += Ib[0] * lx + Ib[1] * ly + Ib[2] * lz;
+      wby += Ib[1] * lx + Ib[3] * ly + Ib[4] * lz;
+      wbz += Ib[2] * lx + Ib[4] * ly + Ib[5] * lz;
     }
-    r1f = n1; r2f = n2;
-    const double d1 = n1 - r1, d2 = n2 - r2;
-    const double lx = t1x * d1 + t2x * d2, ly = t1y * d1 + t2y * d2, lz = t1z * d1 + t2z * d2;
-    wax -= Ia[0] * lx + Ia[1] * ly + Ia[2] * lz;
-    way -= Ia[1] * lx + Ia[3] * ly + Ia[4] * lz;
-    waz -= Ia[2] * lx + Ia[4] * ly + Ia[5] * lz;
-    wbx += Ib[0] * lx + Ib[1] * ly + Ib[2] * lz;
-    wby += Ib[1] * lx + Ib[3] * ly + Ib[4] * lz;
-    wbz += Ib[2] * lx + Ib[4] * ly + Ib[5] * lz;
-  }
-  double s1f;
-  {
-    const double limit = N == 1 ? SPIN_DISC * mu * patch * pressed : mu * twisted;
-    double sv = s0 - smass * ((wbx - wax) * nx + (wby - way) * ny + (wbz - waz) * nz);
-    if (sv > limit) sv = limit; else if (sv < -limit) sv = -limit;
-    s1f = sv;
-    const double ds = sv - s0, lx = nx * ds, ly = ny * ds, lz = nz * ds;
-    wax -= Ia[0] * lx + Ia[1] * ly + Ia[2] * lz;
-    way -= Ia[1] * lx + Ia[3] * ly + Ia[4] * lz;
-    waz -= Ia[2] * lx + Ia[4] * ly + Ia[5] * lz;
-    wbx += Ib[0] * lx + Ib[1] * ly + Ib[2] * lz;
-    wby += Ib[1] * lx + Ib[3] * ly + Ib[4] * lz;
-    wbz += Ib[2] * lx + Ib[4] * ly + Ib[5] * lz;
-  }
-  // ---- every store, last: the bodies first, which the rows after this one wait for ----
-  write_back(B, ima, a, vax, vay, vaz, wax, way, waz);
-  write_back(B, imb, b, vbx, vby, vbz, wbx, wby, wbz);
+    double s1f;
+    {
+      const double limit = N == 1 ? SPIN_DISC * mu * patch * pressed : mu * twisted;
+      double sv = s0 - smass * ((wbx - wax) * nx + (wby - way) * ny + (wbz - waz) * nz);
+      if (sv > limit) sv = limit; else if (sv < -limit) sv = -limit;
+      s1f = sv;
+      const double ds = sv - s0, lx = nx * ds, ly = ny * ds, lz = nz * ds;
+      wax -= Ia[0] * lx + Ia[1] * ly + Ia[2] * lz;
+      way -= Ia[1] * lx + Ia[3] * ly + Ia[4] * lz;
+      waz -= Ia[2] * lx + Ia[4] * ly + Ia[5] * lz;
+      wbx += Ib[0] * lx + Ib[1] * ly + Ib[2] * lz;
+      wby += Ib[1] * lx + Ib[3] * ly + Ib[4] * lz;
+      wbz += Ib[2] * lx + Ib[4] * ly + Ib[5] * lz;
+    }
+    // ---- every store, last: the bodies first, which the rows after this one wait for ----
+    write_back(B, ima, a, vax, vay, vaz, wax, way, waz);
+    write_back(B, imb, b, vbx, vby, vbz, wbx, wby, wbz);
 #pragma unroll
-  for (int k = 0; k < N; k++) {
-    if (!known && !bias) stm(R.now + k * cap + m, nowv[k]);
-    stm(R.ni + k * cap + m, ni[k]);
-    if (rvset[k]) stm(R.relvel + k * cap + m, rv[k]);
-    stm(R.maxni + k * cap + m, mx[k]);
-  }
-  stm(R.gap + m, least);
-  stm(R.sliding + m, sliding);
-  stm(R.ti1 + m, n1f); stm(R.ti2 + m, n2f);
-  if (N <= 2) { stm(R.ri1 + m, r1f); stm(R.ri2 + m, r2f); }
-  stm(R.si + m, s1f);
+    for (int k = 0; k < N; k++) {
+      if (!known && !bias) stm(R.now + k * cap + m, nowv[k]);
+      stm(R.ni + k * cap + m, ni[k]);
+      if (rvset[k]) stm(R.relvel + k * cap + m, rv[k]);
+      stm(R.maxni + k * cap + m, mx[k]);
+    }
+    stm(R.gap + m, least);
+    stm(R.sliding + m, sliding);
+    stm(R.ti1 + m, n1f); stm(R.ti2 + m, n2f);
+    if (N <= 2) { stm(R.ri1 + m, r1f); stm(R.ri2 + m, r2f); }
+    stm(R.si + m, s1f);
+  });
 }
 
 template <class Gate>
