@@ -750,10 +750,11 @@ __device__ __forceinline__ void warm_row(const StageParams& p, int m, Gate gate)
   }
 }
 
-// pushes: src/contact.js:1672-1724.  One instance per point count N and point set SET, so
-// the points taken, and every index below, are compile-time constants: the reference's subset
-// Gaussian elimination, in its operation order, on registers.  (For N = 4 and SET = 15 this is
-// exactly the written-out path of src/contact.js:1673-1698, which does the same operations.)
+// pushes: src/contact.js:1672-1724.  The set of every point, which a resting manifold takes on
+// nearly every pass, has its own instance per point count with every index a compile-time constant
+// (the reference's own written-out set-15 path for four points is exactly these operations); any
+// other set takes the reference's loops, over index lists in local memory.  One unrolled instance
+// per point count rather than one per set keeps the row solver's code small.
 __host__ __device__ constexpr int set_size(int set, int n) {
   return n == 0 ? 0 : ((set & 1) + set_size(set >> 1, n - 1));
 }
@@ -798,19 +799,60 @@ __device__ __forceinline__ void solve_set(const double (&K)[N][N], const double 
   }
 }
 
+// Any subset, by the reference's own loops (src/contact.js:1700-1723): index lists and a small
+// matrix in local memory, the same operations in the same order.
+template <int N>
+__device__ __forceinline__ void pushes_any(const double (&K)[N][N], int set, const double (&give)[N],
+                                           const double (&wanted)[N], double (&solved)[N]) {
+  double Kl[N * N], gl[N], wl[N], sl[N];
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    gl[k] = give[k]; wl[k] = wanted[k]; sl[k] = 0;
+#pragma unroll
+    for (int l = 0; l < N; l++) Kl[k * N + l] = K[k][l];
+  }
+  int in[N];
+  int n = 0;
+#pragma unroll 1
+  for (int k = 0; k < N; k++)
+    if (set >> k & 1) in[n++] = k;
+  double AS[N * N], RS[N], XS[N];
+#pragma unroll 1
+  for (int r = 0; r < n; r++) {
+    const int kr = in[r];
+#pragma unroll 1
+    for (int s = 0; s < n; s++) AS[r * N + s] = Kl[kr * N + in[s]];
+    AS[r * N + r] *= 1 + gl[kr];
+    RS[r] = wl[kr];
+  }
+#pragma unroll 1
+  for (int col = 0; col < n; col++) {
+    const double pivot = AS[col * N + col];
+#pragma unroll 1
+    for (int r = col + 1; r < n; r++) {
+      const double f = AS[r * N + col] / pivot;
+#pragma unroll 1
+      for (int s = col + 1; s < n; s++) AS[r * N + s] -= f * AS[col * N + s];
+      RS[r] -= f * RS[col];
+    }
+  }
+#pragma unroll 1
+  for (int r = n - 1; r >= 0; r--) {
+    double x = RS[r];
+#pragma unroll 1
+    for (int s = r + 1; s < n; s++) x -= AS[r * N + s] * XS[s];
+    XS[r] = x / AS[r * N + r];
+    sl[in[r]] = XS[r];
+  }
+#pragma unroll
+  for (int k = 0; k < N; k++) solved[k] = sl[k];
+}
+
 template <int N>
 __device__ __forceinline__ void pushes_n(const double (&K)[N][N], int set, const double (&give)[N],
                                          const double (&wanted)[N], double (&solved)[N]) {
-#define BG_SET(S) \
-  case S:         \
-    if (S < (1 << N)) solve_set<N, (S < (1 << N) ? S : 0)>(K, give, wanted, solved); \
-    break;
-  switch (set) {
-    BG_SET(0) BG_SET(1) BG_SET(2) BG_SET(3) BG_SET(4) BG_SET(5) BG_SET(6) BG_SET(7)
-    BG_SET(8) BG_SET(9) BG_SET(10) BG_SET(11) BG_SET(12) BG_SET(13) BG_SET(14) BG_SET(15)
-    default: break;
-  }
-#undef BG_SET
+  if (set == (1 << N) - 1) solve_set<N, (1 << N) - 1>(K, give, wanted, solved);
+  else pushes_any<N>(K, set, give, wanted, solved);
 }
 
 // solveRows for row m, one pass, a row of N points: src/contact.js:1805-2090.  The row's own
@@ -1388,7 +1430,7 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
     t.each(0, w.nawake, [&](int i) { accelerate_body(p, ldi(p.B.awake_list + w.awake0 + i), h, w.gravity); });
     if (!t.sync(p)) return false;
     if (touching) {
-      if (Team::kGrid && p.nchunks > 0) {
+      if constexpr (Team::kGrid) {
         // warm and solve flow into each other: a solve row waits for its bodies' warm rows
         flow_pass(p, pass++, [&](int m, auto gate) { warm_row(p, m, gate); });
         flow_pass(p, pass++, [&](int m, auto gate) { solve_row(p, m, h, true, sub > 0, gate); });
@@ -1419,7 +1461,7 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
     t.each(0, w.nawake, [&](int i) { move_body(p, ldi(p.B.awake_list + w.awake0 + i), h); });
     if (!t.sync(p)) return false;
     if (touching) {
-      if (Team::kGrid && p.nchunks > 0) {
+      if constexpr (Team::kGrid) {
         flow_pass(p, pass++, [&](int m, auto gate) { solve_row(p, m, h, false, false, gate); });
         if (!t.sync(p)) return false;
       } else {
