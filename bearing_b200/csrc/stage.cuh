@@ -860,8 +860,13 @@ __device__ __forceinline__ void pushes_n(const double (&K)[N][N], int set, const
 // handed to `gate`, which runs it once the rows before it on its bodies are done (the grid) or at
 // once (a CTA).  So once its bodies are ready, the row costs one trip to memory (their records)
 // and its arithmetic.
-template <int N, class Gate>
-__device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bool known, Gate gate) {
+//
+// BIAS: the biased solve (the substep's first pass) or relax; KNOWN: the separations the last relax
+// pass left in `now` still hold (src/contact.js:1802-1803, 1852), or they are worked out from the
+// bodies' drift.  Each pass kind is its own instance, carrying only the values it uses.
+template <int N, bool BIAS, bool KNOWN, class Gate>
+__device__ void solve_row_n(const StageParams& p, int m, double h, Gate gate) {
+  constexpr bool bias = BIAS, known = KNOWN;
   const RowsDev& R = p.R;
   const BodiesDev& B = p.B;
   const int64_t cap = R.cap;
@@ -1150,18 +1155,22 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, bool bias, bo
   });
 }
 
-template <class Gate>
-__device__ __forceinline__ void solve_row(const StageParams& p, int m, double h, bool bias, bool known, Gate gate) {
+template <bool BIAS, bool KNOWN, class Gate>
+__device__ __forceinline__ void solve_row(const StageParams& p, int m, double h, Gate gate) {
   switch (ldi(p.R.points + m)) {
-    case 1: solve_row_n<1>(p, m, h, bias, known, gate); break;
-    case 2: solve_row_n<2>(p, m, h, bias, known, gate); break;
-    case 3: solve_row_n<3>(p, m, h, bias, known, gate); break;
-    default: solve_row_n<4>(p, m, h, bias, known, gate); break;
+    case 1: solve_row_n<1, BIAS, KNOWN>(p, m, h, gate); break;
+    case 2: solve_row_n<2, BIAS, KNOWN>(p, m, h, gate); break;
+    case 3: solve_row_n<3, BIAS, KNOWN>(p, m, h, gate); break;
+    default: solve_row_n<4, BIAS, KNOWN>(p, m, h, gate); break;
   }
 }
 
-__device__ __forceinline__ void solve_row(const StageParams& p, int m, double h, bool bias, bool known) {
-  solve_row(p, m, h, bias, known, OpenGate());
+// The substep's biased pass: the first substep works the separations out, later ones take the
+// relax pass's (src/contact.js:1802-1803).
+template <class Gate>
+__device__ __forceinline__ void solve_biased(const StageParams& p, int m, double h, int sub, Gate gate) {
+  if (sub > 0) solve_row<true, true>(p, m, h, gate);
+  else solve_row<true, false>(p, m, h, gate);
 }
 
 // Whether row m has a point restitution() works on: src/contact.js:2233-2241.  What it reads
@@ -1433,7 +1442,8 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
       if constexpr (Team::kGrid) {
         // warm and solve flow into each other: a solve row waits for its bodies' warm rows
         flow_pass(p, pass++, [&](int m, auto gate) { warm_row(p, m, gate); });
-        flow_pass(p, pass++, [&](int m, auto gate) { solve_row(p, m, h, true, sub > 0, gate); });
+        if (sub > 0) flow_pass(p, pass++, [&](int m, auto gate) { solve_row<true, true>(p, m, h, gate); });
+        else flow_pass(p, pass++, [&](int m, auto gate) { solve_row<true, false>(p, m, h, gate); });
         if (!t.sync(p)) return false;
       } else {
         for (int k = 0; k < NCOLOURS; k++) {
@@ -1448,12 +1458,12 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
         }
         for (int k = 0; k < NCOLOURS; k++) {
           if (starts[k + 1] <= starts[k]) continue;
-          t.each(starts[k], starts[k + 1], [&](int m) { solve_row(p, r0 + m, h, true, sub > 0); });
+          t.each(starts[k], starts[k + 1], [&](int m) { solve_biased(p, r0 + m, h, sub, OpenGate()); });
           if (!t.sync(p)) return false;
         }
         if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
           if (t.rank == 0)
-            for (int m = starts[OVERFLOW_RUN]; m < starts[OVERFLOW_RUN + 1]; m++) solve_row(p, r0 + m, h, true, sub > 0);
+            for (int m = starts[OVERFLOW_RUN]; m < starts[OVERFLOW_RUN + 1]; m++) solve_biased(p, r0 + m, h, sub, OpenGate());
           if (!t.sync(p)) return false;
         }
       }
@@ -1462,17 +1472,17 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
     if (!t.sync(p)) return false;
     if (touching) {
       if constexpr (Team::kGrid) {
-        flow_pass(p, pass++, [&](int m, auto gate) { solve_row(p, m, h, false, false, gate); });
+        flow_pass(p, pass++, [&](int m, auto gate) { solve_row<false, false>(p, m, h, gate); });
         if (!t.sync(p)) return false;
       } else {
         for (int k = 0; k < NCOLOURS; k++) {
           if (starts[k + 1] <= starts[k]) continue;
-          t.each(starts[k], starts[k + 1], [&](int m) { solve_row(p, r0 + m, h, false, false); });
+          t.each(starts[k], starts[k + 1], [&](int m) { solve_row<false, false>(p, r0 + m, h, OpenGate()); });
           if (!t.sync(p)) return false;
         }
         if (starts[OVERFLOW_RUN + 1] > starts[OVERFLOW_RUN]) {
           if (t.rank == 0)
-            for (int m = starts[OVERFLOW_RUN]; m < starts[OVERFLOW_RUN + 1]; m++) solve_row(p, r0 + m, h, false, false);
+            for (int m = starts[OVERFLOW_RUN]; m < starts[OVERFLOW_RUN + 1]; m++) solve_row<false, false>(p, r0 + m, h, OpenGate());
           if (!t.sync(p)) return false;
         }
       }
