@@ -9,11 +9,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
 #include <cstdarg>
-#include <mutex>
 #include <cstdio>
 #include <cstring>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/bearing_gpu.h"
@@ -218,6 +223,176 @@ struct DevBuf {
   size_t n = 0;
 };
 
+// ---- host threads for the copies between the caller's columns and pinned staging ----
+//
+// A fixed set of worker threads, started on a context's first transfer.  run(n, fn) calls fn(0..n-1)
+// on the workers and the calling thread and returns when all are done.  Tasks are claimed from a
+// cursor tagged with the call's generation, so a worker that wakes late for a finished call finds
+// the tag changed and claims nothing.
+class HostPool {
+ public:
+  explicit HostPool(int workers) {
+    for (int i = 0; i < workers; i++) threads_.emplace_back([this] { loop(); });
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> lock(mutex_);
+      stop_ = true;
+    }
+    wake_.notify_all();
+    for (std::thread& t : threads_) t.join();
+  }
+  int size() const { return static_cast<int>(threads_.size()) + 1; }
+  void run(int n, const std::function<void(int)>& fn) {
+    if (n <= 0) return;
+    if (threads_.empty() || n == 1) {
+      for (int i = 0; i < n; i++) fn(i);
+      return;
+    }
+    uint32_t gen;
+    {
+      std::lock_guard<std::mutex> lock(mutex_);
+      gen = ++gen_;
+      fn_ = &fn;
+      n_ = n;
+      pending_.store(n);
+      cursor_.store(static_cast<uint64_t>(gen) << 32);
+    }
+    wake_.notify_all();
+    work(gen, &fn, n);
+    std::unique_lock<std::mutex> lock(mutex_);
+    done_.wait(lock, [this] { return pending_.load() == 0; });
+  }
+
+ private:
+  void work(uint32_t gen, const std::function<void(int)>* fn, int n) {
+    for (;;) {
+      uint64_t cur = cursor_.load();
+      if (static_cast<uint32_t>(cur >> 32) != gen) return;
+      const int i = static_cast<int>(cur & 0xffffffffu);
+      if (i >= n) return;
+      if (!cursor_.compare_exchange_weak(cur, cur + 1)) continue;
+      (*fn)(i);
+      if (pending_.fetch_sub(1) == 1) {
+        std::lock_guard<std::mutex> lock(mutex_);
+        done_.notify_all();
+      }
+    }
+  }
+  void loop() {
+    uint32_t seen = 0;
+    for (;;) {
+      uint32_t gen;
+      const std::function<void(int)>* fn;
+      int n;
+      {
+        std::unique_lock<std::mutex> lock(mutex_);
+        wake_.wait(lock, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen = gen_;
+        fn = fn_;
+        n = n_;
+      }
+      work(gen, fn, n);
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex mutex_;
+  std::condition_variable wake_, done_;
+  bool stop_ = false;
+  uint32_t gen_ = 0;
+  const std::function<void(int)>* fn_ = nullptr;
+  int n_ = 0;
+  std::atomic<uint64_t> cursor_{0};
+  std::atomic<int> pending_{0};
+};
+
+// ---- staging: every column of one direction in one block, laid out per call ----
+//
+// The caller's columns are gathered into one pinned host block and moved with a few large
+// copies (and the results the other way), instead of one pageable copy per column, which the
+// driver would stage through a small bounce buffer of its own.  Each column starts on a 256-byte
+// boundary; the device block has the same layout, so the unpack and pack kernels read and write
+// it in place.
+struct Piece {
+  const void* from;   // upload: the caller's column
+  void* to;           // download: the caller's column (NULL: not wanted)
+  size_t off, bytes;
+  const char* name;
+};
+
+struct Plan {
+  unsigned char* base = nullptr;   // the device block the kernels see
+  size_t end = 0;
+  std::vector<Piece> pieces;
+  template <class T>
+  T* in(const T* from, size_t n, const char* name) {
+    pieces.push_back(Piece{from, nullptr, end, n * sizeof(T), name});
+    return place<T>(n);
+  }
+  template <class T>
+  T* out(T* to, size_t n, const char* name) {
+    pieces.push_back(Piece{nullptr, to, end, n * sizeof(T), name});
+    return place<T>(n);
+  }
+
+ private:
+  template <class T>
+  T* place(size_t n) {
+    T* at = reinterpret_cast<T*>(base + end);
+    end = (end + n * sizeof(T) + 255) & ~static_cast<size_t>(255);
+    return at;
+  }
+};
+
+// Splits a plan's pieces into at most `groups` runs of neighbouring pieces of similar size (the
+// last run takes whatever is left, empty pieces included).
+std::vector<std::pair<size_t, size_t>> piece_groups(const Plan& plan, int groups) {
+  std::vector<std::pair<size_t, size_t>> out;   // [first piece, last piece + 1)
+  const size_t total = plan.end, n = plan.pieces.size();
+  size_t first = 0;
+  for (size_t i = 0; i < n; i++) {
+    const size_t upto = plan.pieces[i].off + plan.pieces[i].bytes;
+    const size_t want = total * (out.size() + 1) / static_cast<size_t>(groups);
+    if ((upto >= want && out.size() + 1 < static_cast<size_t>(groups)) || i + 1 == n) {
+      out.emplace_back(first, i + 1);
+      first = i + 1;
+    }
+  }
+  return out;
+}
+
+// Whether host memory is page-locked (cudaHostAlloc'd or registered): the device can copy it
+// directly, with no gather through the library's own pinned block.
+bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Host copies of up to 4 MiB each for pieces [first, last), run on the pool.
+struct Slice {
+  const unsigned char* from;
+  unsigned char* to;
+  size_t bytes;
+};
+
+void copy_slices(HostPool* pool, const std::vector<Slice>& slices) {
+  pool->run(static_cast<int>(slices.size()), [&](int i) {
+    const Slice& sl = slices[static_cast<size_t>(i)];
+    std::memcpy(sl.to, sl.from, sl.bytes);
+  });
+}
+
+void add_slices(std::vector<Slice>& slices, const unsigned char* from, unsigned char* to, size_t bytes) {
+  constexpr size_t kSlice = 4u << 20;
+  for (size_t at = 0; at < bytes; at += kSlice)
+    slices.push_back(Slice{from + at, to + at, std::min(kSlice, bytes - at)});
+}
+
 }  // namespace
 
 struct bg_ctx {
@@ -269,6 +444,18 @@ struct bg_ctx {
   unsigned int* bar = nullptr;   // [0] count, [1] generation
   int32_t* status = nullptr;
   int32_t* block_counts = nullptr;
+  // staging blocks, one per direction (see Plan), and the threads that fill and empty them
+  unsigned char* d_in = nullptr;
+  unsigned char* d_out = nullptr;
+  unsigned char* h_in = nullptr;    // pinned
+  unsigned char* h_out = nullptr;   // pinned
+  unsigned char* h_meta = nullptr;  // pinned: order_rows()'s tables on their way to the device
+  std::vector<void*> host_allocs;
+  cudaEvent_t in_free = nullptr;    // the last upload's copies have read h_in
+  bool in_pending = false;
+  static constexpr int kGroups = 4; // copies a direction is split into, to overlap host and DMA
+  cudaEvent_t out_ready[kGroups] = {};
+  std::unique_ptr<HostPool> pool;
   // what was uploaded
   int nbodies = 0, nrows = 0, nawake = 0, nworlds = 0;
   bool uploaded = false;
@@ -302,15 +489,132 @@ bool dev_alloc(bg_ctx* c, T** p, size_t n) {
   return true;
 }
 
+bool host_alloc(bg_ctx* c, unsigned char** p, size_t n) {
+  void* q = nullptr;
+  if (n == 0) n = 1;
+  if (!cuda_ok(c, cudaHostAlloc(&q, n, cudaHostAllocDefault), "cudaHostAlloc")) return false;
+  c->host_allocs.push_back(q);
+  *p = static_cast<unsigned char*>(q);
+  return true;
+}
+
 void free_all(bg_ctx* c) {
   for (void* p : c->allocs) cudaFree(p);
   c->allocs.clear();
+  for (void* p : c->host_allocs) cudaFreeHost(p);
+  c->host_allocs.clear();
+  c->in_pending = false;
+}
+
+// The upload's layout for b slots, r rows and na awake entries: sets the staging pointers the
+// unpack kernels read (into `base`) and lists the caller's columns (NULL when only sizing).
+Plan plan_in(bg_ctx* c, const bg_bodies* B, const bg_rows* R, size_t b, size_t r, size_t na, unsigned char* base) {
+  Plan P;
+  P.base = base;
+  BodyStage& s = c->bin;
+  s.position = P.in<double>(B ? B->position : nullptr, 3 * b, "position");
+  s.rotation = P.in<double>(B ? B->rotation : nullptr, 4 * b, "rotation");
+  s.velocity = P.in<double>(B ? B->velocity : nullptr, 3 * b, "velocity");
+  s.angular = P.in<double>(B ? B->angular : nullptr, 3 * b, "angular");
+  s.tumbled = P.in<double>(B ? B->tumbled : nullptr, 3 * b, "tumbled");
+  s.ceiling = P.in<double>(B ? B->ceiling : nullptr, b, "ceiling");
+  s.start = P.in<double>(B ? B->start : nullptr, 3 * b, "start");
+  s.inv_mass = P.in<double>(B ? B->inv_mass : nullptr, b, "inv_mass");
+  s.inertia = P.in<double>(B ? B->inertia : nullptr, 3 * b, "inertia");
+  s.inv_inertia = P.in<double>(B ? B->inv_inertia : nullptr, 3 * b, "inv_inertia");
+  s.dims = P.in<double>(B ? B->dims : nullptr, 3 * b, "dims");
+  s.damping = P.in<double>(B ? B->damping : nullptr, b, "damping");
+  s.angular_damping = P.in<double>(B ? B->angular_damping : nullptr, b, "angular_damping");
+  s.gravity_scale = P.in<double>(B ? B->gravity_scale : nullptr, b, "gravity_scale");
+  s.type = P.in<uint8_t>(B ? B->type : nullptr, b, "type");
+  s.shape = P.in<uint8_t>(B ? B->shape : nullptr, b, "shape");
+  s.frozen = P.in<uint8_t>(B ? B->frozen : nullptr, b, "frozen");
+  s.framed = P.in<uint8_t>(B ? B->framed : nullptr, b, "framed");
+  s.lock = P.in<uint8_t>(B ? B->lock : nullptr, b, "lock");
+  s.joint_head = P.in<int32_t>(B ? B->joint_head : nullptr, b, "joint_head");
+  s.awake = P.in<uint8_t>(B ? B->awake : nullptr, b, "awake");
+  c->awake_in = P.in<int32_t>(B ? B->awake_list : nullptr, na, "awake_list");
+  s.inv_i = P.in<double>(B ? B->inv_i : nullptr, 6 * b, "inv_i");
+  RowStage& q = c->rin;
+  q.row = P.in<int32_t>(R ? R->row : nullptr, r, "row");
+  q.a = P.in<int32_t>(R ? R->a : nullptr, r, "a");
+  q.b = P.in<int32_t>(R ? R->b : nullptr, r, "b");
+  q.points = P.in<uint8_t>(R ? R->points : nullptr, r, "points");
+  q.normal = P.in<double>(R ? R->normal : nullptr, 3 * r, "normal");
+  q.t1 = P.in<double>(R ? R->t1 : nullptr, 3 * r, "t1");
+  q.t2 = P.in<double>(R ? R->t2 : nullptr, 3 * r, "t2");
+  q.friction = P.in<double>(R ? R->friction : nullptr, r, "friction");
+  q.restitution = P.in<double>(R ? R->restitution : nullptr, r, "restitution");
+  q.tolerance = P.in<double>(R ? R->tolerance : nullptr, r, "tolerance");
+  q.patch = P.in<double>(R ? R->patch : nullptr, r, "patch");
+  q.separation = P.in<double>(R ? R->separation : nullptr, 4 * r, "separation");
+  q.point = P.in<double>(R ? R->point : nullptr, 12 * r, "point");
+  q.shift = P.in<double>(R ? R->shift : nullptr, 12 * r, "shift");
+  q.normal_impulse = P.in<double>(R ? R->normal_impulse : nullptr, 4 * r, "normal_impulse");
+  q.ti1 = P.in<double>(R ? R->tangent_impulse1 : nullptr, r, "tangent_impulse1");
+  q.ti2 = P.in<double>(R ? R->tangent_impulse2 : nullptr, r, "tangent_impulse2");
+  q.ri1 = P.in<double>(R ? R->roll_impulse1 : nullptr, r, "roll_impulse1");
+  q.ri2 = P.in<double>(R ? R->roll_impulse2 : nullptr, r, "roll_impulse2");
+  q.si = P.in<double>(R ? R->spin_impulse : nullptr, r, "spin_impulse");
+  q.drift1 = P.in<double>(R ? R->drift1 : nullptr, r, "drift1");
+  q.drift2 = P.in<double>(R ? R->drift2 : nullptr, r, "drift2");
+  c->maxni_in = P.in<double>(R ? R->max_normal_impulse : nullptr, 4 * r, "max_normal_impulse");
+  c->relvel_in = P.in<double>(R ? R->relative_velocity : nullptr, 4 * r, "relative_velocity");
+  c->gap_in = P.in<double>(R ? R->gap : nullptr, r, "gap");
+  return P;
+}
+
+// The download's layout: sets the staging pointers the pack kernels write (into `base`) and lists
+// the caller's columns (NULL when only sizing, or when the caller does not want a column).
+Plan plan_out(bg_ctx* c, const bg_bodies* B, const bg_rows* R, size_t b, size_t r, unsigned char* base) {
+  Plan P;
+  P.base = base;
+  BodyOut& o = c->bout;
+  o.position = P.out<double>(B ? B->position : nullptr, 3 * b, "position");
+  o.rotation = P.out<double>(B ? B->rotation : nullptr, 4 * b, "rotation");
+  o.velocity = P.out<double>(B ? B->velocity : nullptr, 3 * b, "velocity");
+  o.angular = P.out<double>(B ? B->angular : nullptr, 3 * b, "angular");
+  o.tumbled = P.out<double>(B ? B->tumbled : nullptr, 3 * b, "tumbled");
+  o.ceiling = P.out<double>(B ? B->ceiling : nullptr, b, "ceiling");
+  o.start = P.out<double>(B ? B->start : nullptr, 3 * b, "start");
+  o.start_q = P.out<double>(B ? B->start_q : nullptr, 4 * b, "start_q");
+  o.inv_i = P.out<double>(B ? B->inv_i : nullptr, 6 * b, "inv_i");
+  RowOut& q = c->rout;
+  q.normal_impulse = P.out<double>(R ? R->normal_impulse : nullptr, 4 * r, "normal_impulse");
+  q.ti1 = P.out<double>(R ? R->tangent_impulse1 : nullptr, r, "tangent_impulse1");
+  q.ti2 = P.out<double>(R ? R->tangent_impulse2 : nullptr, r, "tangent_impulse2");
+  q.ri1 = P.out<double>(R ? R->roll_impulse1 : nullptr, r, "roll_impulse1");
+  q.ri2 = P.out<double>(R ? R->roll_impulse2 : nullptr, r, "roll_impulse2");
+  q.si = P.out<double>(R ? R->spin_impulse : nullptr, r, "spin_impulse");
+  q.drift1 = P.out<double>(R ? R->drift1 : nullptr, r, "drift1");
+  q.drift2 = P.out<double>(R ? R->drift2 : nullptr, r, "drift2");
+  q.gap = P.out<double>(R ? R->gap : nullptr, r, "gap");
+  q.maxni = P.out<double>(R ? R->max_normal_impulse : nullptr, 4 * r, "max_normal_impulse");
+  q.relvel = P.out<double>(R ? R->relative_velocity : nullptr, 4 * r, "relative_velocity");
+  q.sliding = P.out<uint8_t>(R ? R->sliding : nullptr, r, "sliding");
+  q.anchor_a = P.out<double>(R ? R->anchor_a : nullptr, 3 * r, "anchor_a");
+  q.anchor_b = P.out<double>(R ? R->anchor_b : nullptr, 3 * r, "anchor_b");
+  return P;
+}
+
+HostPool* pool_of(bg_ctx* c) {
+  if (!c->pool) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int workers = static_cast<int>(std::min(15u, hw > 1 ? hw - 1 : 0u));
+    c->pool = std::make_unique<HostPool>(workers);
+  }
+  return c->pool.get();
 }
 
 size_t grown(size_t have, size_t want) {
   size_t c = have > 0 ? have : 64;
   while (c < want) c *= 2;
   return c;
+}
+
+// Bytes of the pinned block order_rows()'s tables pass through (see send_order).
+size_t meta_bytes(size_t nb, size_t nr) {
+  return 4 * nr * sizeof(int32_t) + nb * sizeof(int32_t) + (nr + 64) * sizeof(int2) + 5 * 256;
 }
 
 // (Re)allocates every buffer for at least the given sizes.  Everything is reallocated together,
@@ -332,27 +636,6 @@ bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
        dev_alloc(c, &B.st, 4 * nb) && dev_alloc(c, &B.sq, 4 * nb) && dev_alloc(c, &B.tc, 4 * nb) &&
        dev_alloc(c, &B.pr, 12 * nb) && dev_alloc(c, &B.fl, nb) && dev_alloc(c, &B.awake_list, na) &&
        dev_alloc(c, &B.head, nb);
-  BodyStage& bi = c->bin;
-  double *position, *rotation, *velocity, *angular, *tumbled, *ceiling, *start, *inv_mass, *inertia, *inv_inertia,
-      *dims, *damping, *angular_damping, *gravity_scale, *inv_i;
-  uint8_t *type, *shape, *frozen, *framed, *lock, *awake;
-  int32_t* joint_head;
-  ok = ok && dev_alloc(c, &position, 3 * nb) && dev_alloc(c, &rotation, 4 * nb) && dev_alloc(c, &velocity, 3 * nb) &&
-       dev_alloc(c, &angular, 3 * nb) && dev_alloc(c, &tumbled, 3 * nb) && dev_alloc(c, &ceiling, nb) &&
-       dev_alloc(c, &start, 3 * nb) && dev_alloc(c, &inv_mass, nb) && dev_alloc(c, &inertia, 3 * nb) &&
-       dev_alloc(c, &inv_inertia, 3 * nb) && dev_alloc(c, &dims, 3 * nb) && dev_alloc(c, &damping, nb) &&
-       dev_alloc(c, &angular_damping, nb) && dev_alloc(c, &gravity_scale, nb) && dev_alloc(c, &type, nb) &&
-       dev_alloc(c, &shape, nb) && dev_alloc(c, &frozen, nb) && dev_alloc(c, &framed, nb) && dev_alloc(c, &lock, nb) &&
-       dev_alloc(c, &joint_head, nb) && dev_alloc(c, &awake, nb) && dev_alloc(c, &c->awake_in, na) &&
-       dev_alloc(c, &inv_i, 6 * nb);
-  if (!ok) return false;
-  bi = BodyStage{position, rotation, velocity, angular, tumbled, ceiling, start, inv_mass, inertia, inv_inertia, dims,
-                 damping, angular_damping, gravity_scale, type, shape, frozen, framed, lock, joint_head, awake, inv_i};
-  BodyOut& bo = c->bout;
-  ok = ok && dev_alloc(c, &bo.position, 3 * nb) && dev_alloc(c, &bo.rotation, 4 * nb) &&
-       dev_alloc(c, &bo.velocity, 3 * nb) && dev_alloc(c, &bo.angular, 3 * nb) && dev_alloc(c, &bo.tumbled, 3 * nb) &&
-       dev_alloc(c, &bo.ceiling, nb) && dev_alloc(c, &bo.start, 3 * nb) && dev_alloc(c, &bo.start_q, 4 * nb) &&
-       dev_alloc(c, &bo.inv_i, 6 * nb);
   // rows
   bg::RowsDev& R = c->R;
   R.cap = static_cast<int64_t>(nr);
@@ -370,30 +653,16 @@ bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
        dev_alloc(c, &R.K, 16 * nr) && dev_alloc(c, &R.fjac, 24 * nr) && dev_alloc(c, &R.tm, 3 * nr) &&
        dev_alloc(c, &R.rm1, nr) && dev_alloc(c, &R.rm2, nr) && dev_alloc(c, &R.sm, nr) &&
        dev_alloc(c, &R.active, nr) && dev_alloc(c, &R.pending, nr);
-  RowStage& ri = c->rin;
-  int32_t *row, *a, *b;
-  uint8_t* points;
-  double *normal, *t1, *t2, *friction, *restitution, *tolerance, *patch, *separation, *point, *shift, *ni, *ti1, *ti2,
-      *ri1, *ri2, *si, *drift1, *drift2;
-  ok = ok && dev_alloc(c, &row, nr) && dev_alloc(c, &a, nr) && dev_alloc(c, &b, nr) && dev_alloc(c, &points, nr) &&
-       dev_alloc(c, &normal, 3 * nr) && dev_alloc(c, &t1, 3 * nr) && dev_alloc(c, &t2, 3 * nr) &&
-       dev_alloc(c, &friction, nr) && dev_alloc(c, &restitution, nr) && dev_alloc(c, &tolerance, nr) &&
-       dev_alloc(c, &patch, nr) && dev_alloc(c, &separation, 4 * nr) && dev_alloc(c, &point, 12 * nr) &&
-       dev_alloc(c, &shift, 12 * nr) && dev_alloc(c, &ni, 4 * nr) && dev_alloc(c, &ti1, nr) && dev_alloc(c, &ti2, nr) &&
-       dev_alloc(c, &ri1, nr) && dev_alloc(c, &ri2, nr) && dev_alloc(c, &si, nr) && dev_alloc(c, &drift1, nr) &&
-       dev_alloc(c, &drift2, nr) && dev_alloc(c, &c->maxni_in, 4 * nr) && dev_alloc(c, &c->relvel_in, 4 * nr) &&
-       dev_alloc(c, &c->gap_in, nr) && dev_alloc(c, &c->perm_dev, nr) && dev_alloc(c, &c->iperm_dev, nr) &&
-       dev_alloc(c, &c->rank_dev, 2 * nr) && dev_alloc(c, &c->deg_dev, nb) && dev_alloc(c, &c->done_dev, nb) &&
-       dev_alloc(c, &c->chunks_dev, nr + 64);
-  if (!ok) return false;
-  ri = RowStage{row, a, b, points, normal, t1, t2, friction, restitution, tolerance, patch, separation, point, shift,
-                ni, ti1, ti2, ri1, ri2, si, drift1, drift2};
-  RowOut& ro = c->rout;
-  ok = ok && dev_alloc(c, &ro.normal_impulse, 4 * nr) && dev_alloc(c, &ro.ti1, nr) && dev_alloc(c, &ro.ti2, nr) &&
-       dev_alloc(c, &ro.ri1, nr) && dev_alloc(c, &ro.ri2, nr) && dev_alloc(c, &ro.si, nr) && dev_alloc(c, &ro.drift1, nr) &&
-       dev_alloc(c, &ro.drift2, nr) && dev_alloc(c, &ro.gap, nr) && dev_alloc(c, &ro.maxni, 4 * nr) &&
-       dev_alloc(c, &ro.relvel, 4 * nr) && dev_alloc(c, &ro.sliding, nr) && dev_alloc(c, &ro.anchor_a, 3 * nr) &&
-       dev_alloc(c, &ro.anchor_b, 3 * nr);
+  ok = ok && dev_alloc(c, &c->perm_dev, nr) && dev_alloc(c, &c->iperm_dev, nr) && dev_alloc(c, &c->rank_dev, 2 * nr) &&
+       dev_alloc(c, &c->deg_dev, nb) && dev_alloc(c, &c->done_dev, nb) && dev_alloc(c, &c->chunks_dev, nr + 64);
+  // staging blocks, sized for the capacities (a call's own layout is never larger)
+  {
+    const size_t in_bytes = plan_in(c, nullptr, nullptr, nb, nr, na, nullptr).end;
+    const size_t out_bytes = plan_out(c, nullptr, nullptr, nb, nr, nullptr).end;
+    ok = ok && dev_alloc(c, &c->d_in, in_bytes) && dev_alloc(c, &c->d_out, out_bytes) &&
+         host_alloc(c, &c->h_in, in_bytes) && host_alloc(c, &c->h_out, out_bytes) &&
+         host_alloc(c, &c->h_meta, meta_bytes(nb, nr));
+  }
   // worlds
   ok = ok && dev_alloc(c, &c->worlds_dev, nw) && dev_alloc(c, &c->body_offset_dev, nw + 1) &&
        dev_alloc(c, &c->awake_offset_dev, nw + 1) && dev_alloc(c, &c->row_offset_dev, nw + 1);
@@ -416,12 +685,6 @@ bool put(bg_ctx* c, T* dst, const T* src, size_t n, const char* what) {
     return false;
   }
   return cuda_ok(c, cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, c->stream), what);
-}
-
-template <class T>
-bool get(bg_ctx* c, T* dst, const T* src, size_t n, const char* what) {
-  if (n == 0 || dst == nullptr) return true;
-  return cuda_ok(c, cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, c->stream), what);
 }
 
 int validate(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
@@ -454,56 +717,49 @@ int validate_world(bg_ctx* c, int nbodies, int nrows, const int32_t* starts, int
   return BG_OK;
 }
 
-// Copies the caller's columns for `nb` slots / `nr` rows / `na` awake entries into staging.
+// Copies the caller's columns for `nb` slots / `nr` rows / `na` awake entries to the device.  A
+// page-locked column is copied straight from the caller's memory; the others are gathered by the
+// pool into the library's pinned block a group at a time, each group's copy to the device starting
+// as soon as it is gathered, while the next group is.  Returns with the copies in flight.
 int upload_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R, int nb, int nr, int na) {
-  const size_t b = static_cast<size_t>(nb), r = static_cast<size_t>(nr);
-  BodyStage& s = c->bin;
-  bool ok = put(c, const_cast<double*>(s.position), B->position, 3 * b, "position") &&
-            put(c, const_cast<double*>(s.rotation), B->rotation, 4 * b, "rotation") &&
-            put(c, const_cast<double*>(s.velocity), B->velocity, 3 * b, "velocity") &&
-            put(c, const_cast<double*>(s.angular), B->angular, 3 * b, "angular") &&
-            put(c, const_cast<double*>(s.tumbled), B->tumbled, 3 * b, "tumbled") &&
-            put(c, const_cast<double*>(s.ceiling), B->ceiling, b, "ceiling") &&
-            put(c, const_cast<double*>(s.start), B->start, 3 * b, "start") &&
-            put(c, const_cast<double*>(s.inv_mass), B->inv_mass, b, "inv_mass") &&
-            put(c, const_cast<double*>(s.inertia), B->inertia, 3 * b, "inertia") &&
-            put(c, const_cast<double*>(s.inv_inertia), B->inv_inertia, 3 * b, "inv_inertia") &&
-            put(c, const_cast<double*>(s.dims), B->dims, 3 * b, "dims") &&
-            put(c, const_cast<double*>(s.damping), B->damping, b, "damping") &&
-            put(c, const_cast<double*>(s.angular_damping), B->angular_damping, b, "angular_damping") &&
-            put(c, const_cast<double*>(s.gravity_scale), B->gravity_scale, b, "gravity_scale") &&
-            put(c, const_cast<uint8_t*>(s.type), B->type, b, "type") &&
-            put(c, const_cast<uint8_t*>(s.shape), B->shape, b, "shape") &&
-            put(c, const_cast<uint8_t*>(s.frozen), B->frozen, b, "frozen") &&
-            put(c, const_cast<uint8_t*>(s.framed), B->framed, b, "framed") &&
-            put(c, const_cast<uint8_t*>(s.lock), B->lock, b, "lock") &&
-            put(c, const_cast<int32_t*>(s.joint_head), B->joint_head, b, "joint_head") &&
-            put(c, const_cast<uint8_t*>(s.awake), B->awake, b, "awake") &&
-            put(c, c->awake_in, B->awake_list, static_cast<size_t>(na), "awake_list") &&
-            put(c, const_cast<double*>(s.inv_i), B->inv_i, 6 * b, "inv_i");
-  RowStage& q = c->rin;
-  ok = ok && put(c, const_cast<int32_t*>(q.row), R->row, r, "row") && put(c, const_cast<int32_t*>(q.a), R->a, r, "a") &&
-       put(c, const_cast<int32_t*>(q.b), R->b, r, "b") && put(c, const_cast<uint8_t*>(q.points), R->points, r, "points") &&
-       put(c, const_cast<double*>(q.normal), R->normal, 3 * r, "normal") &&
-       put(c, const_cast<double*>(q.t1), R->t1, 3 * r, "t1") && put(c, const_cast<double*>(q.t2), R->t2, 3 * r, "t2") &&
-       put(c, const_cast<double*>(q.friction), R->friction, r, "friction") &&
-       put(c, const_cast<double*>(q.restitution), R->restitution, r, "restitution") &&
-       put(c, const_cast<double*>(q.tolerance), R->tolerance, r, "tolerance") &&
-       put(c, const_cast<double*>(q.patch), R->patch, r, "patch") &&
-       put(c, const_cast<double*>(q.separation), R->separation, 4 * r, "separation") &&
-       put(c, const_cast<double*>(q.point), R->point, 12 * r, "point") &&
-       put(c, const_cast<double*>(q.shift), R->shift, 12 * r, "shift") &&
-       put(c, const_cast<double*>(q.normal_impulse), R->normal_impulse, 4 * r, "normal_impulse") &&
-       put(c, const_cast<double*>(q.ti1), R->tangent_impulse1, r, "tangent_impulse1") &&
-       put(c, const_cast<double*>(q.ti2), R->tangent_impulse2, r, "tangent_impulse2") &&
-       put(c, const_cast<double*>(q.ri1), R->roll_impulse1, r, "roll_impulse1") &&
-       put(c, const_cast<double*>(q.ri2), R->roll_impulse2, r, "roll_impulse2") &&
-       put(c, const_cast<double*>(q.si), R->spin_impulse, r, "spin_impulse") &&
-       put(c, const_cast<double*>(q.drift1), R->drift1, r, "drift1") &&
-       put(c, const_cast<double*>(q.drift2), R->drift2, r, "drift2") &&
-       put(c, c->maxni_in, R->max_normal_impulse, 4 * r, "max_normal_impulse") &&
-       put(c, c->relvel_in, R->relative_velocity, 4 * r, "relative_velocity") && put(c, c->gap_in, R->gap, r, "gap");
-  return ok ? BG_OK : BG_ECUDA;
+  Plan plan = plan_in(c, B, R, static_cast<size_t>(nb), static_cast<size_t>(nr), static_cast<size_t>(na), c->d_in);
+  for (const Piece& pc : plan.pieces)
+    if (pc.bytes > 0 && pc.from == nullptr) {
+      set_error(c, "upload: column %s is NULL", pc.name);
+      return BG_EINVAL;
+    }
+  Plan staged;   // the pageable columns, at their places in the device block
+  staged.end = plan.end;
+  for (const Piece& pc : plan.pieces) {
+    if (pc.bytes == 0) continue;
+    if (host_pinned(pc.from)) {
+      if (!cuda_ok(c, cudaMemcpyAsync(c->d_in + pc.off, pc.from, pc.bytes, cudaMemcpyHostToDevice, c->stream), "upload"))
+        return BG_ECUDA;
+    } else {
+      staged.pieces.push_back(pc);
+    }
+  }
+  if (staged.pieces.empty()) return BG_OK;
+  // The last upload's copies must be done reading the pinned block before it is refilled.
+  if (c->in_pending && !cuda_ok(c, cudaEventSynchronize(c->in_free), "upload")) return BG_ECUDA;
+  c->in_pending = false;
+  HostPool* pool = pool_of(c);
+  for (const auto& g : piece_groups(staged, bg_ctx::kGroups)) {
+    std::vector<Slice> slices;
+    for (size_t k = g.first; k < g.second; k++) {
+      const Piece& pc = staged.pieces[k];
+      add_slices(slices, static_cast<const unsigned char*>(pc.from), c->h_in + pc.off, pc.bytes);
+    }
+    copy_slices(pool, slices);
+    const size_t lo = staged.pieces[g.first].off;
+    const size_t hi = staged.pieces[g.second - 1].off + staged.pieces[g.second - 1].bytes;
+    if (hi > lo &&
+        !cuda_ok(c, cudaMemcpyAsync(c->d_in + lo, c->h_in + lo, hi - lo, cudaMemcpyHostToDevice, c->stream), "upload"))
+      return BG_ECUDA;
+  }
+  if (!cuda_ok(c, cudaEventRecord(c->in_free, c->stream), "upload")) return BG_ECUDA;
+  c->in_pending = true;
+  return BG_OK;
 }
 
 // The order rows are solved in on the device: within each colour, rows by point count (a
@@ -552,12 +808,45 @@ int order_rows(bg_ctx* c, const uint8_t* points, const int32_t* a, const int32_t
         c->chunks.push_back(make_int2(m, std::min(32, w.starts[k + 1] - m)));
     for (int m = w.starts[bg::OVERFLOW_RUN]; m < w.starts[bg::OVERFLOW_RUN + 1]; m++) c->chunks.push_back(make_int2(m, 1));
   }
-  bool ok = put(c, c->perm_dev, c->perm.data(), static_cast<size_t>(n), "perm") &&
-            put(c, c->iperm_dev, c->iperm.data(), static_cast<size_t>(n), "iperm") &&
-            put(c, c->rank_dev, c->rank.data(), 2 * static_cast<size_t>(n), "rank") &&
-            put(c, c->deg_dev, c->deg.data(), static_cast<size_t>(c->nbodies), "deg") &&
-            put(c, c->chunks_dev, c->chunks.data(), c->chunks.size(), "chunks");
+  return BG_OK;
+}
+
+// order_rows()'s tables to the device, through the pinned block (a copy from pageable memory would
+// first wait for everything queued on the stream, the columns' copies included).
+int send_order(bg_ctx* c) {
+  const size_t n = static_cast<size_t>(c->nrows);
+  unsigned char* h = c->h_meta;
+  size_t off = 0;
+  auto send = [&](void* dev, const void* host, size_t bytes) {
+    if (bytes == 0) return true;
+    std::memcpy(h + off, host, bytes);
+    const bool ok = cuda_ok(c, cudaMemcpyAsync(dev, h + off, bytes, cudaMemcpyHostToDevice, c->stream), "order");
+    off = (off + bytes + 255) & ~static_cast<size_t>(255);
+    return ok;
+  };
+  const bool ok = send(c->perm_dev, c->perm.data(), n * sizeof(int32_t)) &&
+                  send(c->iperm_dev, c->iperm.data(), n * sizeof(int32_t)) &&
+                  send(c->rank_dev, c->rank.data(), 2 * n * sizeof(int32_t)) &&
+                  send(c->deg_dev, c->deg.data(), static_cast<size_t>(c->nbodies) * sizeof(int32_t)) &&
+                  send(c->chunks_dev, c->chunks.data(), c->chunks.size() * sizeof(int2));
   return ok ? BG_OK : BG_ECUDA;
+}
+
+// The caller's columns and the solve order, together: order_rows() works on its own thread while
+// the pool gathers the columns and their copies start.
+int upload_and_order(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
+  if ((c->nrows > 0 && (R->points == nullptr || R->a == nullptr || R->b == nullptr)) ||
+      (c->nbodies > 0 && B->inv_mass == nullptr)) {
+    set_error(c, "upload: rows.points, rows.a, rows.b and bodies.inv_mass must be given");
+    return BG_EINVAL;
+  }
+  int order_rc = BG_OK;
+  std::thread orderer([&] { order_rc = order_rows(c, R->points, R->a, R->b, B->inv_mass); });
+  const int rc = upload_columns(c, B, R, c->nbodies, c->nrows, c->nawake);
+  orderer.join();
+  if (rc != BG_OK) return rc;
+  if (order_rc != BG_OK) return order_rc;
+  return send_order(c);
 }
 
 int unpack(bg_ctx* c) {
@@ -640,6 +929,7 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
 
 int finish(bg_ctx* c) {
   const int nb = c->nbodies, nr = c->nrows;
+  plan_out(c, nullptr, nullptr, static_cast<size_t>(nb), static_cast<size_t>(nr), c->d_out);
   const int blocks = std::max(1, std::min(4 * c->sms, (std::max(nb, nr) + kUnpackThreads - 1) / kUnpackThreads));
   pack_bodies<<<blocks, kUnpackThreads, 0, c->stream>>>(c->B, c->bout, nb);
   pack_rows<<<blocks, kUnpackThreads, 0, c->stream>>>(c->R, c->rout, nr, c->perm_dev);
@@ -647,23 +937,43 @@ int finish(bg_ctx* c) {
   return cuda_ok(c, cudaGetLastError(), "pack") ? BG_OK : BG_ECUDA;
 }
 
+// The results back to the caller's columns.  A page-locked column is copied straight into the
+// caller's memory; for the others, each group of the pinned block is copied from the device and,
+// once it has landed, scattered to the caller's columns by the pool while the next group is still
+// on its way.
 int download_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
-  const size_t b = static_cast<size_t>(c->nbodies), r = static_cast<size_t>(c->nrows);
-  BodyOut& o = c->bout;
-  RowOut& q = c->rout;
-  bool ok = get(c, B->position, o.position, 3 * b, "position") && get(c, B->rotation, o.rotation, 4 * b, "rotation") &&
-            get(c, B->velocity, o.velocity, 3 * b, "velocity") && get(c, B->angular, o.angular, 3 * b, "angular") &&
-            get(c, B->tumbled, o.tumbled, 3 * b, "tumbled") && get(c, B->ceiling, o.ceiling, b, "ceiling") &&
-            get(c, B->start, o.start, 3 * b, "start") && get(c, B->start_q, o.start_q, 4 * b, "start_q") &&
-            get(c, B->inv_i, o.inv_i, 6 * b, "inv_i");
-  ok = ok && get(c, R->normal_impulse, q.normal_impulse, 4 * r, "normal_impulse") &&
-       get(c, R->tangent_impulse1, q.ti1, r, "tangent_impulse1") && get(c, R->tangent_impulse2, q.ti2, r, "tangent_impulse2") &&
-       get(c, R->roll_impulse1, q.ri1, r, "roll_impulse1") && get(c, R->roll_impulse2, q.ri2, r, "roll_impulse2") &&
-       get(c, R->spin_impulse, q.si, r, "spin_impulse") && get(c, R->drift1, q.drift1, r, "drift1") &&
-       get(c, R->drift2, q.drift2, r, "drift2") && get(c, R->gap, q.gap, r, "gap") &&
-       get(c, R->max_normal_impulse, q.maxni, 4 * r, "max_normal_impulse") &&
-       get(c, R->relative_velocity, q.relvel, 4 * r, "relative_velocity") && get(c, R->sliding, q.sliding, r, "sliding") &&
-       get(c, R->anchor_a, q.anchor_a, 3 * r, "anchor_a") && get(c, R->anchor_b, q.anchor_b, 3 * r, "anchor_b");
+  const Plan all = plan_out(c, B, R, static_cast<size_t>(c->nbodies), static_cast<size_t>(c->nrows), c->d_out);
+  Plan plan;   // the columns going through the pinned block
+  plan.end = all.end;
+  bool ok = true;
+  for (const Piece& pc : all.pieces) {
+    if (pc.bytes == 0 || pc.to == nullptr) continue;
+    if (host_pinned(pc.to))
+      ok = ok && cuda_ok(c, cudaMemcpyAsync(pc.to, c->d_out + pc.off, pc.bytes, cudaMemcpyDeviceToHost, c->stream),
+                         "download");
+    else
+      plan.pieces.push_back(pc);
+  }
+  const auto groups = plan.pieces.empty() ? std::vector<std::pair<size_t, size_t>>() : piece_groups(plan, bg_ctx::kGroups);
+  for (size_t gi = 0; gi < groups.size() && ok; gi++) {
+    const auto& g = groups[gi];
+    const size_t lo = plan.pieces[g.first].off;
+    const size_t hi = plan.pieces[g.second - 1].off + plan.pieces[g.second - 1].bytes;
+    if (hi > lo)
+      ok = cuda_ok(c, cudaMemcpyAsync(c->h_out + lo, c->d_out + lo, hi - lo, cudaMemcpyDeviceToHost, c->stream), "download");
+    ok = ok && cuda_ok(c, cudaEventRecord(c->out_ready[gi], c->stream), "download");
+  }
+  HostPool* pool = pool_of(c);
+  for (size_t gi = 0; gi < groups.size() && ok; gi++) {
+    ok = cuda_ok(c, cudaEventSynchronize(c->out_ready[gi]), "download");
+    if (!ok) break;
+    std::vector<Slice> slices;
+    for (size_t k = groups[gi].first; k < groups[gi].second; k++) {
+      const Piece& pc = plan.pieces[k];
+      if (pc.to != nullptr) add_slices(slices, c->h_out + pc.off, static_cast<unsigned char*>(pc.to), pc.bytes);
+    }
+    copy_slices(pool, slices);
+  }
   int32_t status = 0;
   ok = ok && cuda_ok(c, cudaMemcpyAsync(&status, c->status, sizeof status, cudaMemcpyDeviceToHost, c->stream), "status") &&
        cuda_ok(c, cudaStreamSynchronize(c->stream), "synchronize");
@@ -695,6 +1005,8 @@ bg_ctx* bg_create(int32_t device, uint32_t flags) {
   cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
   cudaEventCreate(&c->stage_begin);
   cudaEventCreate(&c->stage_end);
+  cudaEventCreateWithFlags(&c->in_free, cudaEventDisableTiming);
+  for (cudaEvent_t& e : c->out_ready) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_grid, kGridThreads, 0);
   if (per_sm < 1) per_sm = 1;
@@ -711,6 +1023,10 @@ void bg_destroy(bg_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_all(c);
+  c->pool.reset();
+  if (c->in_free) cudaEventDestroy(c->in_free);
+  for (cudaEvent_t e : c->out_ready)
+    if (e) cudaEventDestroy(e);
   if (c->stage_begin) cudaEventDestroy(c->stage_begin);
   if (c->stage_end) cudaEventDestroy(c->stage_end);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -758,9 +1074,7 @@ int32_t bg_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
   for (int k = 0; k < bg::NSTARTS; k++) w.starts[k] = R->starts[k];
   w.gravity[0] = 0; w.gravity[1] = 0; w.gravity[2] = 0;
   c->worlds.assign(1, w);
-  rc = upload_columns(c, B, R, c->nbodies, c->nrows, c->nawake);
-  if (rc != BG_OK) return rc;
-  rc = order_rows(c, R->points, R->a, R->b, B->inv_mass);
+  rc = upload_and_order(c, B, R);
   if (rc != BG_OK) return rc;
   std::vector<int32_t> bo = {0, c->nbodies}, ao = {0, c->nawake}, ro = {0, c->nrows};
   rc = upload_worlds(c, bo, ao, ro);
@@ -850,9 +1164,7 @@ int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const b
   c->nworlds = nw;
   c->batch = true;
   c->worlds = worlds;
-  rc = upload_columns(c, B, R, c->nbodies, c->nrows, c->nawake);
-  if (rc != BG_OK) return rc;
-  rc = order_rows(c, R->points, R->a, R->b, B->inv_mass);
+  rc = upload_and_order(c, B, R);
   if (rc != BG_OK) return rc;
   std::vector<int32_t> bo(W->body_offset, W->body_offset + nw + 1), ao(W->awake_offset, W->awake_offset + nw + 1),
       ro(W->row_offset, W->row_offset + nw + 1);

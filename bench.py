@@ -8,8 +8,8 @@ row visits) / solve-stage seconds.
 
   value     the solve stage with its input resident in HBM: bg_restore (untimed), an L2 flush
             (untimed), then CUDA events around bg_solve on the library's stream
-  e2e       the same solve stage through bg_solve_step with host arrays: upload, solve and
-            download inside the timed region, events on the same stream
+  e2e       the same solve stage through bg_solve_step with host arrays in page-locked memory:
+            upload, solve and download inside the timed region, events on the same stream
   roofline  algorithmic bytes of one solve-stage kernel (counted from the rows' point counts by
             the rule in algorithmic_bytes()) / that kernel's event-timed duration, against the
             measured HBM copy bandwidth
@@ -178,11 +178,14 @@ def time_resident(lib, ctx, copy, steps, warmup, torch):
 
 
 def time_e2e(lib, ctx, copy, steps, warmup, torch):
-    """bg_solve_step with host arrays: uploads, solve and downloads inside the timed region."""
+    """bg_solve_step with host arrays in page-locked memory (as a World that keeps its columns
+    pinned passes them): uploads, solve and downloads inside the timed region.  The arrays are
+    refilled with the step's input, untimed, before every call."""
     stream = torch.cuda.ExternalStream(lib.bg_stream(ctx))
+    work = copy.pinned()
     times = []
     for i in range(warmup + steps):
-        work = copy.copy()
+        work.fill(copy)
         B, R, S = work.views()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -352,7 +355,7 @@ def main():
                                colours=int(sum(1 for k in range(32) if copy.starts[k + 1] > copy.starts[k])),
                                overflow=int(copy.starts[33] - copy.starts[32]), awake=copy.awake_count),
                 "e2e": {"value": e2e, "unit": "rows/s", "ms_per_step": ms_e2e, "h2d_bytes_per_step": h2d,
-                        "d2h_bytes_per_step": d2h},
+                        "d2h_bytes_per_step": d2h, "host_memory": "page-locked"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": measured_traffic(args.bodies, args.at), "kernel_ms": ms_stage,
                              "algorithmic_bytes": algo, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},

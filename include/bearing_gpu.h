@@ -58,7 +58,10 @@ extern "C" {
 
 /* bg_create flags */
 #define BG_FLAG_NONE 0u
-/* Register the caller's host arrays as pinned on first use (cudaHostRegister) and keep them so. */
+/* Reserved (accepted, no effect).  Every transfer already takes the fastest route by itself: a
+ * column in page-locked host memory (cudaHostAlloc'd or registered by the caller) is copied to and
+ * from directly; any other column goes through the library's own pinned staging, gathered and
+ * scattered by a pool of host threads. */
 #define BG_FLAG_PIN_HOST 1u
 /* Run every single world on the persistent grid (the path large worlds take), whatever its size. */
 #define BG_FLAG_GRID 2u

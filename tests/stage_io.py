@@ -82,6 +82,36 @@ class StageCopy:
             starts=self.starts.copy(), rows={k: v.copy() for k, v in self.rows.items()}, dt=self.dt,
             substeps=self.substeps, gravity=self.gravity))
 
+    def pinned(self):
+        """The same arrays in page-locked host memory (torch's pinned allocator), which the CUDA
+        library copies to and from directly."""
+        import torch
+
+        keep = []
+
+        def pin(arr):
+            t = torch.empty(max(arr.size, 1), dtype=getattr(torch, arr.dtype.name)).pin_memory()
+            keep.append(t)
+            out = t.numpy()[: arr.size]
+            out[:] = arr
+            return out
+
+        c = StageCopy(arrays=dict(
+            capacity=self.capacity, awake_count=self.awake_count, awake_list=pin(self.awake_list),
+            body={k: pin(v) for k, v in self.body.items()}, count=self.count, solved=self.solved,
+            starts=self.starts.copy(), rows={k: pin(v) for k, v in self.rows.items()}, dt=self.dt,
+            substeps=self.substeps, gravity=self.gravity))
+        c._pinned = keep
+        return c
+
+    def fill(self, other):
+        """Copies other's values into these arrays (same sizes)."""
+        np.copyto(self.awake_list, other.awake_list)
+        for k, v in other.body.items():
+            np.copyto(self.body[k], v)
+        for k, v in other.rows.items():
+            np.copyto(self.rows[k], v)
+
     def views(self):
         B = _ffi.Bodies()
         B.capacity = self.capacity
