@@ -153,6 +153,37 @@ def test_locked_and_frozen_bodies():
     assert first_difference(a, b) is None
 
 
+@pytest.mark.parametrize("path", ["grid", "block"])
+def test_awake_bodies_without_mass_and_moved_bodies_not_awake(path):
+    # Two inputs the grid's body passes treat apart, on both paths: awake bodies with inverse mass
+    # 0 (frozen here; kinematic alike), whose moves no counter orders, so the move pass keeps its
+    # grid barriers; and dynamic bodies the rows move that are not on the awake list, which are
+    # neither accelerated nor moved but still take their turns.
+    w = oracle_world()
+    scenes.pyramid(w)
+    for _ in range(4):
+        w.step(DT)
+    w.begin_step(DT)
+    base = StageCopy(w)
+    slots = base.awake_list.copy()
+    frozen = slots[5::9]
+    base.body["frozen"][frozen] = 1
+    base.body["inv_mass"][frozen] = 0.0
+    a = oracle_io.solve(base.copy())
+    b = gpu_io.solve(base.copy(), path)
+    assert first_difference(a, b) is None, "frozen awake bodies"
+    base = StageCopy(w)
+    dropped = set(int(x) for x in slots[3::7])
+    kept = np.array([x for x in slots if int(x) not in dropped], dtype=np.int32)
+    base.awake_list = kept
+    base.awake_count = len(kept)
+    for x in dropped:
+        base.body["awake"][x] = 0
+    a = oracle_io.solve(base.copy())
+    b = gpu_io.solve(base.copy(), path)
+    assert first_difference(a, b) is None, "moved bodies off the awake list"
+
+
 def test_no_contacts_free_fall():
     w = oracle_world()
     w.addBody({"position": (0.0, 10.0, 0.0), "angularVelocity": (1.0, 2.0, 3.0), "size": (1.0, 2.0, 3.0)})
