@@ -223,18 +223,24 @@ def cpu_solve_times(copy, workers, sample):
     return times
 
 
-def measured_traffic(bodies, at):
-    """DRAM bytes per launch of the stage kernel from the committed ncu summary, if it was taken
-    on this workload (profiles/stage_grid_pile50k_dram.md), else None."""
-    if bodies != 50_000 or at != 300:
+def measured_traffic(bodies, algorithmic):
+    """DRAM bytes per launch of the stage kernel, from the committed ncu capture of the same pile
+    (profiles/stage_grid_pile50k_dram.md), scaled from the captured launch to this one by their
+    algorithmic bytes (the traffic grows with the rows and points a launch works through); None
+    for another workload."""
+    if bodies != 50_000:
         return None
+    got = {}
     try:
         for line in open(os.path.join(ROOT, "profiles", "stage_grid_pile50k_dram.md")):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return int(line.split(":")[1])
-    except OSError:
-        pass
-    return None
+            key, _, value = line.partition(":")
+            if key in ("traffic_bytes_per_launch", "algorithmic_bytes_per_launch"):
+                got[key] = int(value)
+    except (OSError, ValueError):
+        return None
+    if len(got) != 2:
+        return None
+    return int(round(got["traffic_bytes_per_launch"] * algorithmic / got["algorithmic_bytes_per_launch"]))
 
 
 def host_threads():
@@ -357,7 +363,8 @@ def main():
                 "e2e": {"value": e2e, "unit": "rows/s", "ms_per_step": ms_e2e, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "host_memory": "page-locked"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                             "frac": achieved / hbm, "traffic": measured_traffic(args.bodies, args.at), "kernel_ms": ms_stage,
+                             "frac": achieved / hbm, "traffic": measured_traffic(args.bodies, algo),
+                             "traffic_source": "ncu capture at step 101, scaled by algorithmic bytes", "kernel_ms": ms_stage,
                              "algorithmic_bytes": algo, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
                 "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches}
         print(json.dumps(line), flush=True)
