@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=2, help="solve stages the CPU baseline times")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--resident-only", action="store_true", help="time the resident solve only (for profiling)")
+    p.add_argument("--batch-worlds", type=int, default=4096, help="worlds in the batched-worlds measurement")
+    p.add_argument("--batch-at", type=int, default=60, help="steps the batch takes before its timed solve stage")
+    p.add_argument("--no-batch", action="store_true", help="skip the batched-worlds measurement")
     return p.parse_args()
 
 
@@ -243,6 +246,91 @@ def measured_traffic(bodies, algorithmic):
     return int(round(got["traffic_bytes_per_launch"] * algorithmic / got["algorithmic_bytes_per_launch"]))
 
 
+def measure_batch(args, lib, torch, device, log):
+    """Config 4: many small independent worlds solved in one launch (bg_batch_*, one CTA a world)
+    against the plain path called world by world (bg_solve_step).  The worlds (a pyramid, a box
+    stack or a sphere pile of 8..512 bodies each, friction U(0.3, 0.8), restitution U(0, 0.4)) are
+    stepped together to step `batch_at`; then that step's solve stage is timed: batched with its
+    input resident, batched through bg_batch_solve_step with host arrays, and as a loop of
+    bg_solve_step over the worlds (host arrays too).  The loop's results must equal the batch's
+    bit for bit."""
+    import numpy as np
+    from bearing_b200 import scenes
+    from bearing_b200.world import Batch, World
+    from stage_io import BatchCopy, first_difference
+    rng = np.random.default_rng(4096)
+    t0 = time.time()
+    worlds = []
+    for _ in range(args.batch_worlds):
+        w = World({}, solver=(0, 0))   # stepped by the batch, never by a solver of its own
+        scenes.batch_world(w, rng)
+        worlds.append(w)
+    batch = Batch(worlds, device=device, threads=host_threads())
+    for _ in range(args.batch_at):
+        batch.step(DT)
+    batch.begin_step(DT)
+    base = BatchCopy(*batch.views())
+    if log:
+        log(f"batch of {args.batch_worlds} worlds built and stepped to {args.batch_at} in {time.time() - t0:.0f} s: "
+            f"{base.stage.capacity} slots, {base.stage.count} rows")
+    ctx = lib.bg_create(device, 0)
+    stream = torch.cuda.ExternalStream(lib.bg_stream(ctx))
+    # resident
+    B, R, W, S = base.views()
+    assert lib.bg_batch_upload(ctx, C.byref(B), C.byref(R), C.byref(W)) == 0, lib.bg_last_error(ctx)
+    resident = []
+    for i in range(args.warmup + args.steps):
+        assert lib.bg_restore(ctx) == 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        assert lib.bg_batch_solve(ctx, C.byref(S)) == 0, lib.bg_last_error(ctx)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= args.warmup:
+            resident.append(e0.elapsed_time(e1))
+    # batched, host arrays
+    work = base.copy()
+    batched = []
+    for i in range(args.warmup + args.steps):
+        work.fill(base)
+        B, R, W, S = work.views()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        assert lib.bg_batch_solve_step(ctx, C.byref(B), C.byref(R), C.byref(W), C.byref(S)) == 0, lib.bg_last_error(ctx)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= args.warmup:
+            batched.append(e0.elapsed_time(e1))
+    # the plain path, world by world
+    parts = [base.world(i) for i in range(base.worlds)]
+    one = lib.bg_create(device, 0)
+    loop = []
+    for i in range(2):
+        outs = [p.copy() for p in parts]
+        views = [o.views() for o in outs]
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for Bw, Rw, Sw in views:
+            assert lib.bg_solve_step(one, C.byref(Bw), C.byref(Rw), C.byref(Sw)) == 0, lib.bg_last_error(one)
+        torch.cuda.synchronize()
+        loop.append((time.perf_counter() - t) * 1000)
+    same = all(first_difference(work.world(i), outs[i]) is None for i in range(base.worlds))
+    lib.bg_destroy(one)
+    lib.bg_destroy(ctx)
+    batch.destroy()
+    n = base.worlds
+    ms_res, ms_bat, ms_loop = statistics.mean(resident), statistics.mean(batched), min(loop)
+    return {"workload": f"{n} independent worlds (pyramid, box stack or sphere pile of 8..512 bodies), "
+                        f"solve stage at step {args.batch_at + 1}",
+            "worlds": n, "slots": int(base.stage.capacity), "rows": int(base.stage.count),
+            "solved_rows": int(sum(int(base.starts[_k * 35 + 33]) for _k in range(n))),
+            "unit": "world-steps/s",
+            "batched_resident": {"value": n / (ms_res / 1000), "ms_per_step": ms_res},
+            "batched_e2e": {"value": n / (ms_bat / 1000), "ms_per_step": ms_bat},
+            "per_world_loop_e2e": {"value": n / (ms_loop / 1000), "ms_per_step": ms_loop},
+            "speedup_e2e": ms_loop / ms_bat, "bit_identical": same}
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -353,6 +441,9 @@ def main():
         if threads > 1:
             tn = cpu_solve_times(copy, threads - 1, args.cpu_sample)
             cpu["all_threads"] = {"value": rows_per_stage / statistics.mean(tn), "cores": threads}
+    batch = None
+    if rank == 0 and world_size == 1 and not args.no_batch and not args.resident_only:
+        batch = measure_batch(args, lib, torch, local, log)
     if rank == 0:
         line = {"metric": "contact rows/s", "value": value, "unit": "rows/s", "n_gpus": world_size,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -366,7 +457,7 @@ def main():
                              "frac": achieved / hbm, "traffic": measured_traffic(args.bodies, algo),
                              "traffic_source": "ncu capture at step 101, scaled by algorithmic bytes", "kernel_ms": ms_stage,
                              "algorithmic_bytes": algo, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
-                "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches}
+                "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches, "batch": batch}
         print(json.dumps(line), flush=True)
     lib.bg_destroy(ctx)
     solver.close()

@@ -58,11 +58,11 @@ def _read(ptr, n, dtype):
 class StageCopy:
     """A solve stage's input, in arrays of its own."""
 
-    def __init__(self, world=None, *, arrays=None):
+    def __init__(self, world=None, *, arrays=None, views=None):
         if arrays is not None:
             self.__dict__.update(arrays)
             return
-        B, R, S = world.views()
+        B, R, S = views if views is not None else world.views()
         self.capacity = B.capacity
         self.awake_count = B.awake_count
         self.awake_list = _read(B.awake_list, B.awake_count, np.int32)
@@ -162,3 +162,58 @@ def max_relative_difference(a: StageCopy, b: StageCopy) -> float:
         if d.size:
             worst = max(worst, float(np.nanmax(d)))
     return worst
+
+
+class BatchCopy:
+    """A batch's solve-stage input (bw_batch_views: every world's arrays end to end, and the table
+    of where each world's part starts) in arrays of its own."""
+
+    def __init__(self, B, R, W, S):
+        self.stage = StageCopy(views=(B, R, S))
+        n = W.count
+        self.worlds = n
+        self.body_offset = _read(W.body_offset, n + 1, np.int32)
+        self.awake_offset = _read(W.awake_offset, n + 1, np.int32)
+        self.row_offset = _read(W.row_offset, n + 1, np.int32)
+        self.starts = _read(W.starts, _ffi.BG_STARTS * n, np.int32)
+
+    def copy(self):
+        c = BatchCopy.__new__(BatchCopy)
+        c.stage = self.stage.copy()
+        c.worlds = self.worlds
+        for k in ("body_offset", "awake_offset", "row_offset", "starts"):
+            setattr(c, k, getattr(self, k).copy())
+        return c
+
+    def fill(self, other):
+        self.stage.fill(other.stage)
+
+    def views(self):
+        B, R, S = self.stage.views()
+        W = _ffi.Worlds(self.worlds, _ptr(self.body_offset, np.int32), _ptr(self.awake_offset, np.int32),
+                        _ptr(self.row_offset, np.int32), _ptr(self.starts, np.int32), None)
+        self._keep = (B, R, W, S)
+        return B, R, W, S
+
+    def world(self, i):
+        """World i's part as a StageCopy of its own (the batch keeps slots and rows world-local)."""
+        b0, b1 = int(self.body_offset[i]), int(self.body_offset[i + 1])
+        a0, a1 = int(self.awake_offset[i]), int(self.awake_offset[i + 1])
+        r0, r1 = int(self.row_offset[i]), int(self.row_offset[i + 1])
+        st = self.stage
+        starts = self.starts[_ffi.BG_STARTS * i: _ffi.BG_STARTS * (i + 1)].copy()
+        return StageCopy(arrays=dict(
+            capacity=b1 - b0, awake_count=a1 - a0, awake_list=st.awake_list[a0:a1].copy(),
+            body={f: st.body[f][per * b0: per * b1].copy() for f, _, per in BODY_COLUMNS},
+            count=r1 - r0, solved=int(starts[33]), starts=starts,
+            rows={f: st.rows[f][per * r0: per * r1].copy() for f, _, per in ROW_COLUMNS},
+            dt=st.dt, substeps=st.substeps, gravity=st.gravity))
+
+    def part(self, i, out):
+        """Writes StageCopy `out` (world i's part, solved alone) back over this batch's arrays."""
+        b0, b1 = int(self.body_offset[i]), int(self.body_offset[i + 1])
+        r0, r1 = int(self.row_offset[i]), int(self.row_offset[i + 1])
+        for f, _, per in BODY_COLUMNS:
+            self.stage.body[f][per * b0: per * b1] = out.body[f]
+        for f, _, per in ROW_COLUMNS:
+            self.stage.rows[f][per * r0: per * r1] = out.rows[f]
