@@ -120,6 +120,18 @@ def pile(world, count=50_000, seed=50_000, spacing=1.5, jitter=0.2, extent=100.0
     return slots
 
 
+def batch_rng(seed, i):
+    """World i's own generator in a batch: worlds draw independently, so any subset of a batch
+    (one rank's shard) builds exactly as it would in the whole batch."""
+    return np.random.default_rng([seed, i])
+
+
+def batch_world_bodies(rng_seed, i):
+    """The body count batch_world draws first for world i (its weight when sharding)."""
+    rng = batch_rng(rng_seed, i)
+    return int(round(math.exp(rng.uniform(math.log(8), math.log(512)))))
+
+
 def batch_world(world, rng):
     """One world of the batch: a pyramid, a box stack or a sphere pile of 8..512 bodies."""
     n = int(round(math.exp(rng.uniform(math.log(8), math.log(512)))))

@@ -246,24 +246,27 @@ def measured_traffic(bodies, algorithmic):
     return int(round(got["traffic_bytes_per_launch"] * algorithmic / got["algorithmic_bytes_per_launch"]))
 
 
-def measure_batch(args, lib, torch, device, log):
+def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None):
     """Config 4: many small independent worlds solved in one launch (bg_batch_*, one CTA a world)
     against the plain path called world by world (bg_solve_step).  The worlds (a pyramid, a box
     stack or a sphere pile of 8..512 bodies each, friction U(0.3, 0.8), restitution U(0, 0.4)) are
     stepped together to step `batch_at`; then that step's solve stage is timed: batched with its
     input resident, batched through bg_batch_solve_step with host arrays, and as a loop of
     bg_solve_step over the worlds (host arrays too).  The loop's results must equal the batch's
-    bit for bit."""
-    import numpy as np
-    from bearing_b200 import scenes
+    bit for bit.  Under torchrun the worlds are sharded over the ranks by their body counts
+    (bearing_b200.shard), each rank building and solving only its own; times are the max over
+    ranks, and no data crosses between ranks."""
+    from bearing_b200 import scenes, shard
     from bearing_b200.world import Batch, World
     from stage_io import BatchCopy, first_difference
-    rng = np.random.default_rng(4096)
+    seed = 4096
+    weights = [scenes.batch_world_bodies(seed, i) for i in range(args.batch_worlds)]
+    mine = shard.shard_of(weights, rank, world_size)
     t0 = time.time()
     worlds = []
-    for _ in range(args.batch_worlds):
+    for i in mine:
         w = World({}, solver=(0, 0))   # stepped by the batch, never by a solver of its own
-        scenes.batch_world(w, rng)
+        scenes.batch_world(w, scenes.batch_rng(seed, i))
         worlds.append(w)
     batch = Batch(worlds, device=device, threads=host_threads())
     for _ in range(args.batch_at):
@@ -318,12 +321,21 @@ def measure_batch(args, lib, torch, device, log):
     lib.bg_destroy(one)
     lib.bg_destroy(ctx)
     batch.destroy()
-    n = base.worlds
     ms_res, ms_bat, ms_loop = statistics.mean(resident), statistics.mean(batched), min(loop)
+    slots, rows = int(base.stage.capacity), int(base.stage.count)
+    solved = int(sum(int(base.starts[k * 35 + 33]) for k in range(base.worlds)))
+    if dist:
+        t = torch.tensor([ms_res, ms_bat, ms_loop], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_res, ms_bat, ms_loop = (float(x) for x in t.tolist())
+        t = torch.tensor([slots, rows, solved, 0 if same else 1], device="cuda", dtype=torch.int64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        slots, rows, solved, unequal = (int(x) for x in t.tolist())
+        same = unequal == 0
+    n = args.batch_worlds
     return {"workload": f"{n} independent worlds (pyramid, box stack or sphere pile of 8..512 bodies), "
                         f"solve stage at step {args.batch_at + 1}",
-            "worlds": n, "slots": int(base.stage.capacity), "rows": int(base.stage.count),
-            "solved_rows": int(sum(int(base.starts[_k * 35 + 33]) for _k in range(n))),
+            "worlds": n, "ranks": world_size, "slots": slots, "rows": rows, "solved_rows": solved,
             "unit": "world-steps/s",
             "batched_resident": {"value": n / (ms_res / 1000), "ms_per_step": ms_res},
             "batched_e2e": {"value": n / (ms_bat / 1000), "ms_per_step": ms_bat},
@@ -442,8 +454,8 @@ def main():
             tn = cpu_solve_times(copy, threads - 1, args.cpu_sample)
             cpu["all_threads"] = {"value": rows_per_stage / statistics.mean(tn), "cores": threads}
     batch = None
-    if rank == 0 and world_size == 1 and not args.no_batch and not args.resident_only:
-        batch = measure_batch(args, lib, torch, local, log)
+    if not args.no_batch and not args.resident_only:   # every rank, or none: it holds collectives
+        batch = measure_batch(args, lib, torch, local, log, rank, world_size, dist)
     if rank == 0:
         line = {"metric": "contact rows/s", "value": value, "unit": "rows/s", "n_gpus": world_size,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
