@@ -241,6 +241,10 @@ def gpu() -> C.CDLL:
         lib.bg_set_wait_budget.argtypes = [C.c_void_p, C.c_int64]
         lib.bg_last_stage_ms.argtypes = [C.c_void_p]
         lib.bg_last_stage_ms.restype = C.c_double
+        lib.bg_set_block_threads.argtypes = [C.c_void_p, C.c_int32]
+        lib.bg_set_block_threads.restype = C.c_int32
+        lib.bg_block_threads.argtypes = [C.c_void_p]
+        lib.bg_block_threads.restype = C.c_int32
         lib.bg_solve_step_static.argtypes = [C.POINTER(Bodies), C.POINTER(Rows), C.POINTER(Step), C.c_void_p]
         lib.bg_solve_step_static.restype = C.c_int32
         for f in ("bg_solve_step", "bg_upload", "bg_restore", "bg_solve", "bg_download",
@@ -255,7 +259,8 @@ def gpu() -> C.CDLL:
 GPU_SYMBOLS = [
     "bg_create", "bg_destroy", "bg_last_error", "bg_version", "bg_solve_step", "bg_upload", "bg_restore",
     "bg_solve", "bg_download", "bg_batch_solve_step", "bg_batch_upload", "bg_batch_solve",
-    "bg_batch_download", "bg_stream", "bg_last_launches", "bg_last_stage_ms", "bg_set_wait_budget", "bg_solve_step_static",
+    "bg_batch_download", "bg_stream", "bg_last_launches", "bg_last_stage_ms", "bg_set_wait_budget", "bg_set_block_threads",
+    "bg_block_threads", "bg_solve_step_static",
 ]
 HOST_SYMBOLS = [
     "bw_create", "bw_destroy", "bw_last_error", "bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step",

@@ -207,7 +207,8 @@ __global__ void __launch_bounds__(kGridThreads) stage_grid(bg::StageParams p) {
 
 __global__ void __launch_bounds__(kBlockThreads) stage_block(bg::StageParams p) {
   bg::BlockTeam t;
-  for (int wi = blockIdx.x; wi < p.nworlds; wi += gridDim.x) {
+  for (int k = blockIdx.x; k < p.nworlds; k += gridDim.x) {
+    const int wi = p.world_order != nullptr ? p.world_order[k] : k;
     const bg::WorldDesc w = p.worlds[wi];
     if (!bg::solve_stage(p, w, t)) return;
     __syncthreads();
@@ -430,6 +431,11 @@ struct bg_ctx {
   unsigned int* done_dev = nullptr;
   int2* chunks_dev = nullptr;
   std::vector<int32_t> rank, deg;
+  // batches: the order CTAs take the worlds in, and the threads a world's CTA has (0: tune on the
+  // next batched solve, see tune_block_threads)
+  int32_t* order_dev = nullptr;
+  std::vector<int32_t> world_order;
+  int block_threads = 0;
   std::vector<int2> chunks;
   // staging out
   BodyOut bout = {};
@@ -664,7 +670,7 @@ bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
          host_alloc(c, &c->h_meta, meta_bytes(nb, nr));
   }
   // worlds
-  ok = ok && dev_alloc(c, &c->worlds_dev, nw) && dev_alloc(c, &c->body_offset_dev, nw + 1) &&
+  ok = ok && dev_alloc(c, &c->worlds_dev, nw) && dev_alloc(c, &c->order_dev, nw) && dev_alloc(c, &c->body_offset_dev, nw + 1) &&
        dev_alloc(c, &c->awake_offset_dev, nw + 1) && dev_alloc(c, &c->row_offset_dev, nw + 1);
   ok = ok && dev_alloc(c, &c->bar, 2) && dev_alloc(c, &c->status, 1) &&
        dev_alloc(c, &c->block_counts, static_cast<size_t>(c->grid_blocks > 0 ? c->grid_blocks : 1024));
@@ -863,7 +869,16 @@ int unpack(bg_ctx* c) {
 int upload_worlds(bg_ctx* c, const std::vector<int32_t>& body_off, const std::vector<int32_t>& awake_off,
                   const std::vector<int32_t>& row_off) {
   const size_t nw = c->worlds.size();
+  // CTAs take a batch's worlds largest first (solved rows, then slots), so the longest worlds
+  // start in the first wave rather than the last; worlds are independent, so no result changes.
+  c->world_order.resize(nw);
+  for (size_t i = 0; i < nw; i++) c->world_order[i] = static_cast<int32_t>(i);
+  std::stable_sort(c->world_order.begin(), c->world_order.end(), [&](int32_t x, int32_t y) {
+    const bg::WorldDesc &a = c->worlds[static_cast<size_t>(x)], &b = c->worlds[static_cast<size_t>(y)];
+    return a.solved != b.solved ? a.solved > b.solved : a.nbodies > b.nbodies;
+  });
   bool ok = put(c, c->worlds_dev, c->worlds.data(), nw, "worlds") &&
+            put(c, c->order_dev, c->world_order.data(), nw, "world order") &&
             put(c, c->body_offset_dev, body_off.data(), nw + 1, "body_offset") &&
             put(c, c->awake_offset_dev, awake_off.data(), nw + 1, "awake_offset") &&
             put(c, c->row_offset_dev, row_off.data(), nw + 1, "row_offset");
@@ -904,6 +919,7 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
   p.R.rank_b = c->rank_dev + c->nrows;
   p.chunks = c->chunks_dev;
   p.nchunks = static_cast<int32_t>(c->chunks.size());
+  p.world_order = c->batch ? c->order_dev : nullptr;
   if (!cuda_ok(c, cudaMemsetAsync(c->done_dev, 0, sizeof(unsigned int) * static_cast<size_t>(c->nbodies > 0 ? c->nbodies : 1),
                                   c->stream), "done")) return BG_ECUDA;
   if (!cuda_ok(c, cudaMemsetAsync(c->status, 0, sizeof(int32_t), c->stream), "status")) return BG_ECUDA;
@@ -918,8 +934,9 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
                                                       dim3(kGridThreads), args, 0, c->stream);
     if (!cuda_ok(c, e, "stage_grid launch")) return BG_ECUDA;
   } else {
+    const int threads = c->batch && c->block_threads > 0 ? c->block_threads : kBlockThreads;
     const int blocks = std::min(c->nworlds, 64 * c->sms);
-    stage_block<<<blocks, kBlockThreads, 0, c->stream>>>(p);
+    stage_block<<<blocks, threads, 0, c->stream>>>(p);
     if (!cuda_ok(c, cudaGetLastError(), "stage_block launch")) return BG_ECUDA;
   }
   cudaEventRecord(c->stage_end, c->stream);
@@ -1038,6 +1055,18 @@ const char* bg_last_error(const bg_ctx* c) { return c == nullptr ? "no context" 
 void* bg_stream(bg_ctx* c) { return c == nullptr ? nullptr : static_cast<void*>(c->stream); }
 
 int32_t bg_last_launches(const bg_ctx* c) { return c == nullptr ? 0 : c->last_launches; }
+
+int32_t bg_set_block_threads(bg_ctx* c, int32_t threads) {
+  if (c == nullptr) return BG_EINVAL;
+  if (threads != 0 && threads != 32 && threads != 64 && threads != 128 && threads != 256) {
+    set_error(c, "block threads must be 0 (tune), 32, 64, 128 or 256");
+    return BG_EINVAL;
+  }
+  c->block_threads = threads;
+  return BG_OK;
+}
+
+int32_t bg_block_threads(const bg_ctx* c) { return c == nullptr ? BG_EINVAL : c->block_threads; }
 
 double bg_last_stage_ms(bg_ctx* c) {
   if (c == nullptr || !c->stage_timed) return -1.0;
@@ -1174,6 +1203,42 @@ int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const b
   return unpack(c);
 }
 
+// The batch's CTA size, by measurement: a world's CTA holds 255 registers a thread, so an SM runs
+// 8, 4, 2 or 1 worlds at once with 32, 64, 128 or 256 threads each; small worlds leave most of a
+// large CTA idle, large ones want the threads.  Each candidate solves the uploaded batch once
+// (timed with events), the input is restored from staging after each, and the fastest is kept.
+// Results do not depend on the choice.
+static int tune_block_threads(bg_ctx* c, const bg_step* step) {
+  static const int kCandidates[] = {32, 64, 128, 256};
+  float best = 0;
+  int chosen = kBlockThreads;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (!cuda_ok(c, cudaEventCreate(&e0), "tune") || !cuda_ok(c, cudaEventCreate(&e1), "tune")) return BG_ECUDA;
+  int rc = BG_OK;
+  for (int threads : kCandidates) {
+    c->block_threads = threads;
+    cudaEventRecord(e0, c->stream);
+    rc = launch_stage(c, step);
+    if (rc != BG_OK) break;
+    cudaEventRecord(e1, c->stream);
+    float ms = 0;
+    if (!cuda_ok(c, cudaEventSynchronize(e1), "tune") || !cuda_ok(c, cudaEventElapsedTime(&ms, e0, e1), "tune")) {
+      rc = BG_ECUDA;
+      break;
+    }
+    if (best == 0 || ms < best) {
+      best = ms;
+      chosen = threads;
+    }
+    rc = unpack(c);   // back to the uploaded input
+    if (rc != BG_OK) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->block_threads = chosen;
+  return rc;
+}
+
 int32_t bg_batch_solve(bg_ctx* c, const bg_step* step) {
   if (c == nullptr || !c->uploaded || !c->batch) {
     if (c) set_error(c, "batch solve: no batch uploaded");
@@ -1190,6 +1255,10 @@ int32_t bg_batch_solve(bg_ctx* c, const bg_step* step) {
   if (changed) {
     if (!put(c, c->worlds_dev, c->worlds.data(), c->worlds.size(), "worlds")) return BG_ECUDA;
     if (!cuda_ok(c, cudaStreamSynchronize(c->stream), "worlds")) return BG_ECUDA;
+  }
+  if (c->block_threads == 0) {
+    const int trc = tune_block_threads(c, step);
+    if (trc != BG_OK) return trc;
   }
   int rc = launch_stage(c, step);
   if (rc != BG_OK) return rc;

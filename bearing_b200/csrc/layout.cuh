@@ -140,6 +140,8 @@ struct StageParams {
   // one colour (or one row of the overflow); warp w takes runs w, w + warps, ... in order.
   const int2* chunks;
   int32_t nchunks;
+  // The order CTAs take the worlds of a batch in (largest first), or NULL for 0, 1, 2, ...
+  const int32_t* world_order;
 };
 
 }  // namespace bg

@@ -291,6 +291,7 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
         e1.synchronize()
         if i >= args.warmup:
             resident.append(e0.elapsed_time(e1))
+    cta_threads = lib.bg_block_threads(ctx)   # chosen by the library's tuner on the first solve
     # batched, host arrays
     work = base.copy()
     batched = []
@@ -340,7 +341,7 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
             "batched_resident": {"value": n / (ms_res / 1000), "ms_per_step": ms_res},
             "batched_e2e": {"value": n / (ms_bat / 1000), "ms_per_step": ms_bat},
             "per_world_loop_e2e": {"value": n / (ms_loop / 1000), "ms_per_step": ms_loop},
-            "speedup_e2e": ms_loop / ms_bat, "bit_identical": same}
+            "speedup_e2e": ms_loop / ms_bat, "bit_identical": same, "cta_threads": cta_threads}
 
 
 def host_threads():

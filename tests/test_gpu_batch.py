@@ -35,3 +35,42 @@ def test_batched_worlds_match_the_oracle_world_by_world():
             assert sa[k].tobytes() == sb[k].tobytes(), f"world {i}: {k}"
     assert sum(w.stats()["rows"] for w in gpu_worlds) > 1000
     batch.destroy()
+
+
+def test_batched_results_do_not_depend_on_the_cta_size():
+    # 32, 64 and 256 threads a world, and the tuner's own choice: the same bits, the oracle's.
+    import ctypes as C
+    from stage_io import BatchCopy, first_difference
+    from bearing_b200 import _ffi
+    worlds = make(40, 23, oracle_io.solver(0))
+    for w in worlds:
+        for _ in range(25):
+            w.step(DT)
+    host = _ffi.host()
+    handles = (C.c_void_p * len(worlds))(*[w._w for w in worlds])
+    b = host.bw_batch_create(handles, len(worlds))
+    try:
+        assert host.bw_batch_begin_step(b, DT, 4) == 0
+        B, R, W, S = _ffi.Bodies(), _ffi.Rows(), _ffi.Worlds(), _ffi.Step()
+        assert host.bw_batch_views(b, C.byref(B), C.byref(R), C.byref(W), C.byref(S)) == 0
+        base = BatchCopy(B, R, W, S)
+    finally:
+        host.bw_batch_destroy(b)
+    g = _ffi.gpu()
+    want = [oracle_io.solve(base.world(i).copy()) for i in range(base.worlds)]
+    for threads in (32, 64, 256, 0):
+        ctx = g.bg_create(0, 0)
+        try:
+            assert g.bg_set_block_threads(ctx, threads) == 0
+            work = base.copy()
+            Bw, Rw, Ww, Sw = work.views()
+            rc = g.bg_batch_solve_step(ctx, C.byref(Bw), C.byref(Rw), C.byref(Ww), C.byref(Sw))
+            assert rc == 0, g.bg_last_error(ctx).decode()
+            used = g.bg_block_threads(ctx)
+            assert used == threads if threads else used in (32, 64, 128, 256)
+            for i in range(base.worlds):
+                d = first_difference(want[i], work.world(i))
+                assert d is None, f"{threads} threads, world {i}: {d}"
+        finally:
+            g.bg_destroy(ctx)
+    assert g.bg_set_block_threads(None, 32) == _ffi.BG_EINVAL
