@@ -699,10 +699,10 @@ __device__ __forceinline__ void warm_row_n(const StageParams& p, int m, Gate gat
   }
   const double l1 = ldm(R.ti1 + m), l2 = ldm(R.ti2 + m);
   const double r1 = ldm(R.ri1 + m), r2 = ldm(R.ri2 + m), sp = ldm(R.si + m);
+  BodyLoad A, Bb;   // the bodies' masses: fixed for the whole stage
+  load_mass(B, a, A);
+  load_mass(B, b, Bb);
   gate([&]() {
-    BodyLoad A, Bb;
-    load_mass(B, a, A);
-    load_mass(B, b, Bb);
     const double ima = A.im, imb = Bb.im;
     const double* va = B.vw + 8 * a;
     const double* vb = B.vw + 8 * b;
@@ -856,10 +856,12 @@ __device__ __forceinline__ void pushes_n(const double (&K)[N][N], int set, const
 }
 
 // solveRows for row m, one pass, a row of N points: src/contact.js:1805-2090.  The row's own
-// columns are read first; the rest (its two bodies, the arithmetic, every store at the end) is
-// handed to `gate`, which runs it once the rows before it on its bodies are done (the grid) or at
-// once (a CTA).  So once its bodies are ready, the row costs one trip to memory (their records)
-// and its arithmetic.
+// columns are read first, then what no row of the pass can change: its bodies' masses (fixed for
+// the stage) and, where the separations are worked out, their poses (moves happen between passes),
+// with the separations and soft targets they give.  The rest (its bodies' velocities, the
+// arithmetic, every store at the end) is handed to `gate`, which runs it once the rows before it
+// on its bodies are done (the grid) or at once (a CTA).  So once its bodies are ready, the row
+// costs one trip to memory (their two velocity records) and its velocity arithmetic.
 //
 // BIAS: the biased solve (the substep's first pass) or relax; KNOWN: the separations the last relax
 // pass left in `now` still hold (src/contact.js:1802-1803, 1852), or they are worked out from the
@@ -928,57 +930,59 @@ __device__ void solve_row_n(const StageParams& p, int m, double h, Gate gate) {
     rm1 = ldm(R.rm1 + m); rm2 = ldm(R.rm2 + m);
   }
   const double s0 = ldm(R.si + m), smass = ldm(R.sm + m);
+  // ---- what the pass cannot change: the bodies' masses (fixed for the stage) and, where the
+  // separations are worked out, their poses (moves happen between passes) ----
+  BodyLoad A, Bb;
+  load_mass(B, a, A);
+  load_mass(B, b, Bb);
+  double dn = 0, nax = 0, nay = 0, naz = 0, nbx = 0, nby = 0, nbz = 0;
+  if (!known) {
+    const double* pqa = B.pq + 8 * a;
+    const double* pqb = B.pq + 8 * b;
+    const double* sta = B.st + 4 * a;
+    const double* stb = B.st + 4 * b;
+    const double dx = (ldm(pqb) - ldm(stb)) - (ldm(pqa) - ldm(sta));
+    const double dy = (ldm(pqb + 1) - ldm(stb + 1)) - (ldm(pqa + 1) - ldm(sta + 1));
+    const double dz = (ldm(pqb + 2) - ldm(stb + 2)) - (ldm(pqa + 2) - ldm(sta + 2));
+    dn = dx * nx + dy * ny + dz * nz;
+    double qa[4], qb[4], v3[3];
+#pragma unroll
+    for (int k = 0; k < 4; k++) { qa[k] = ldm(pqa + 4 + k); qb[k] = ldm(pqb + 4 + k); }
+    rotate(qa, nx, ny, nz, true, v3);
+    nax = v3[0]; nay = v3[1]; naz = v3[2];
+    rotate(qb, nx, ny, nz, true, v3);
+    nbx = v3[0]; nby = v3[1]; nbz = v3[2];
+  }
+  // ---- the arithmetic, in the reference's order ----
+  double target[N], massScale[N], impulseScale[N], give[N], nowv[N];
+  double least = INFINITY;
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    double s;
+    if (known) {
+      s = sep[k];
+    } else {
+      s = dn + (lb[k][0] * nbx + lb[k][1] * nby + lb[k][2] * nbz) - (la[k][0] * nax + la[k][1] * nay + la[k][2] * naz)
+        + sep[k];
+    }
+    nowv[k] = s;
+    if (s < least) least = s;
+    if (s > 0) {
+      target[k] = s * inv; massScale[k] = 1; impulseScale[k] = 0; give[k] = COMPLIANCE;
+    } else if (bias) {
+      target[k] = js_max(soft.biasRate * s, -maxBias);
+      massScale[k] = soft.massScale; impulseScale[k] = soft.impulseScale; give[k] = springy;
+    } else {
+      target[k] = 0; massScale[k] = 1; impulseScale[k] = 0; give[k] = COMPLIANCE;
+    }
+  }
   // ---- the rows before this one on its bodies ----
   gate([&]() {
-    // ---- its bodies ----
-    BodyLoad A, Bb;
-    load_mass(B, a, A);
-    load_mass(B, b, Bb);
+    // ---- its bodies' velocities, the only thing the rows before it change ----
     const double* va = B.vw + 8 * a;
     const double* vb = B.vw + 8 * b;
     double vax = ldm(va), vay = ldm(va + 1), vaz = ldm(va + 2), wax = ldm(va + 3), way = ldm(va + 4), waz = ldm(va + 5);
     double vbx = ldm(vb), vby = ldm(vb + 1), vbz = ldm(vb + 2), wbx = ldm(vb + 3), wby = ldm(vb + 4), wbz = ldm(vb + 5);
-    double dn = 0, nax = 0, nay = 0, naz = 0, nbx = 0, nby = 0, nbz = 0;
-    if (!known) {
-      const double* pqa = B.pq + 8 * a;
-      const double* pqb = B.pq + 8 * b;
-      const double* sta = B.st + 4 * a;
-      const double* stb = B.st + 4 * b;
-      const double dx = (ldm(pqb) - ldm(stb)) - (ldm(pqa) - ldm(sta));
-      const double dy = (ldm(pqb + 1) - ldm(stb + 1)) - (ldm(pqa + 1) - ldm(sta + 1));
-      const double dz = (ldm(pqb + 2) - ldm(stb + 2)) - (ldm(pqa + 2) - ldm(sta + 2));
-      dn = dx * nx + dy * ny + dz * nz;
-      double qa[4], qb[4], v3[3];
-#pragma unroll
-      for (int k = 0; k < 4; k++) { qa[k] = ldm(pqa + 4 + k); qb[k] = ldm(pqb + 4 + k); }
-      rotate(qa, nx, ny, nz, true, v3);
-      nax = v3[0]; nay = v3[1]; naz = v3[2];
-      rotate(qb, nx, ny, nz, true, v3);
-      nbx = v3[0]; nby = v3[1]; nbz = v3[2];
-    }
-    // ---- the arithmetic, in the reference's order ----
-    double target[N], massScale[N], impulseScale[N], give[N], nowv[N];
-    double least = INFINITY;
-#pragma unroll
-    for (int k = 0; k < N; k++) {
-      double s;
-      if (known) {
-        s = sep[k];
-      } else {
-        s = dn + (lb[k][0] * nbx + lb[k][1] * nby + lb[k][2] * nbz) - (la[k][0] * nax + la[k][1] * nay + la[k][2] * naz)
-          + sep[k];
-      }
-      nowv[k] = s;
-      if (s < least) least = s;
-      if (s > 0) {
-        target[k] = s * inv; massScale[k] = 1; impulseScale[k] = 0; give[k] = COMPLIANCE;
-      } else if (bias) {
-        target[k] = js_max(soft.biasRate * s, -maxBias);
-        massScale[k] = soft.massScale; impulseScale[k] = soft.impulseScale; give[k] = springy;
-      } else {
-        target[k] = 0; massScale[k] = 1; impulseScale[k] = 0; give[k] = COMPLIANCE;
-      }
-    }
     const double ima = A.im, imb = Bb.im;
     double closingNow[N], solved[N];
     if (N == 1 || !(Kb[0][0] > 0)) {
