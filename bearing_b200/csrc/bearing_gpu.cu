@@ -784,12 +784,19 @@ int order_rows(bg_ctx* c, const uint8_t* points, const int32_t* a, const int32_t
         for (int m = from; m < to; m++) c->perm[static_cast<size_t>(w.row0 + m)] = w.row0 + m;
         continue;
       }
-      int at = from;
-      for (int count = 1; count <= bg::P; count++)
-        for (int m = from; m < to; m++) {
-          const int pc = points[w.row0 + m] < 1 ? 1 : points[w.row0 + m] > bg::P ? bg::P : points[w.row0 + m];
-          if (pc == count) c->perm[static_cast<size_t>(w.row0 + at++)] = w.row0 + m;
-        }
+      // a stable counting sort on the point count (1..P): one pass to count, one to place
+      auto count_of = [&](int m) {
+        const int pc = points[w.row0 + m];
+        return pc < 1 ? 1 : pc > bg::P ? bg::P : pc;
+      };
+      int at[bg::P + 1] = {0};
+      for (int m = from; m < to; m++) at[count_of(m)]++;
+      for (int k2 = 1, next = from; k2 <= bg::P; k2++) {
+        const int here = at[k2];
+        at[k2] = next;
+        next += here;
+      }
+      for (int m = from; m < to; m++) c->perm[static_cast<size_t>(w.row0 + at[count_of(m)]++)] = w.row0 + m;
     }
   }
   for (int d = 0; d < n; d++) c->iperm[static_cast<size_t>(c->perm[static_cast<size_t>(d)])] = d;
