@@ -930,6 +930,10 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
   if (!cuda_ok(c, cudaMemsetAsync(c->done_dev, 0, sizeof(unsigned int) * static_cast<size_t>(c->nbodies > 0 ? c->nbodies : 1),
                                   c->stream), "done")) return BG_ECUDA;
   if (!cuda_ok(c, cudaMemsetAsync(c->status, 0, sizeof(int32_t), c->stream), "status")) return BG_ECUDA;
+  // The grid barrier's arrival count starts at zero: a launch that lost its step (a wait past its
+  // budget) can leave it part-way through a count, which would release the next launch's first
+  // barrier early.  (Its generation word only ever needs to change, so it keeps its value.)
+  if (!cuda_ok(c, cudaMemsetAsync(c->bar, 0, sizeof(unsigned int), c->stream), "barrier")) return BG_ECUDA;
   c->last_launches += 1;
   cudaEventRecord(c->stage_begin, c->stream);
   bool big = !c->batch && c->nworlds == 1 && c->worlds[0].solved >= kGridRows;
