@@ -227,15 +227,31 @@ def test_pyramid_on_the_grid_path():
         finish_with(w, a)
 
 
-def test_gpu_world_matches_oracle_world_over_300_steps():
-    # The whole loop: a World on the GPU against a World on the oracle, 2,000 spheres raining.
+@pytest.mark.parametrize("config", ["pyramid", "rain"])
+def test_gpu_world_matches_oracle_world_over_600_steps(config):
+    # The whole loop at the survey's configs 1 and 2: the 20-row pyramid (210 boxes) and 2,000
+    # spheres raining into a walled container, 600 steps each, a World on the GPU against the
+    # same World on the oracle, state and transforms identical after every step while the
+    # oracle's world stays finite.  The rain goes non-finite in the reference's own arithmetic
+    # at step 172 (a contact's normal impulse decays to 3.3e-163, the friction limit's square
+    # underflows to 0 and the cone's Newton step overflows); from there the two differ only in
+    # where the NaN spreads (restitution's push writes static bodies in the reference, not here).
     wa, wb = oracle_world(), gpu_world()
-    scenes.rain(wa, count=400, seed=3)
-    scenes.rain(wb, count=400, seed=3)
-    for i in range(300):
+    for w in (wa, wb):
+        if config == "pyramid":
+            scenes.pyramid(w)
+        else:
+            scenes.rain(w, count=2000, seed=2000)
+    finite_steps = 0
+    for i in range(600):
         wa.step(DT)
         wb.step(DT)
-    sa, sb = wa.state(), wb.state()
-    for k in sa:
-        assert sa[k].tobytes() == sb[k].tobytes(), k
-    assert wa.transforms.tobytes() == wb.transforms.tobytes()
+        sa, sb = wa.state(), wb.state()
+        if not all(np.all(np.isfinite(sa[k])) for k in sa):
+            break
+        for k in sa:
+            assert sa[k].tobytes() == sb[k].tobytes(), f"step {i + 1}: {k}"
+        assert wa.transforms.tobytes() == wb.transforms.tobytes(), f"step {i + 1}: transforms"
+        finite_steps += 1
+    assert finite_steps == (600 if config == "pyramid" else 171), finite_steps
+    assert wa.stats()["rows"] > 100 or config == "rain"
