@@ -447,7 +447,7 @@ struct bg_ctx {
   int32_t* row_offset_dev = nullptr;
   std::vector<bg::WorldDesc> worlds;
   // barrier and status
-  unsigned int* bar = nullptr;   // [0] count, [1] generation
+  unsigned int* bar = nullptr;   // the grid barrier's arrival count
   int32_t* status = nullptr;
   int32_t* block_counts = nullptr;
   // staging blocks, one per direction (see Plan), and the threads that fill and empty them
@@ -916,7 +916,6 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
   p.substeps = step->substeps;
   p.soft = make_soft(step->dt / step->substeps);
   p.bar_count = c->bar;
-  p.bar_gen = c->bar + 1;
   p.status = c->status;
   p.block_counts = c->block_counts;
   p.budget = c->budget;
@@ -930,9 +929,8 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
   if (!cuda_ok(c, cudaMemsetAsync(c->done_dev, 0, sizeof(unsigned int) * static_cast<size_t>(c->nbodies > 0 ? c->nbodies : 1),
                                   c->stream), "done")) return BG_ECUDA;
   if (!cuda_ok(c, cudaMemsetAsync(c->status, 0, sizeof(int32_t), c->stream), "status")) return BG_ECUDA;
-  // The grid barrier's arrival count starts at zero: a launch that lost its step (a wait past its
-  // budget) can leave it part-way through a count, which would release the next launch's first
-  // barrier early.  (Its generation word only ever needs to change, so it keeps its value.)
+  // The grid barrier's arrival count starts at zero for every launch (it only grows within one,
+  // and a launch that lost its step can leave it anywhere).
   if (!cuda_ok(c, cudaMemsetAsync(c->bar, 0, sizeof(unsigned int), c->stream), "barrier")) return BG_ECUDA;
   c->last_launches += 1;
   cudaEventRecord(c->stage_begin, c->stream);

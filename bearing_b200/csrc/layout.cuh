@@ -132,7 +132,6 @@ struct StageParams {
   Soft soft;
   // grid barrier state and the step's status word (0 ok; 1 a wait ran past its budget)
   unsigned int* bar_count;
-  unsigned int* bar_gen;
   int32_t* status;
   int32_t* block_counts;  // per-block counts for restitution's compaction
   long long budget;

@@ -141,27 +141,27 @@ __device__ __forceinline__ double ref_atan2(double y, double x) {
 // ---- barriers ----
 
 // A grid-wide barrier whose wait is bounded: past `budget` polls it records status 1 and every
-// block leaves the stage at its next barrier, so the kernel always ends.
+// block leaves the stage at its next barrier, so the kernel always ends.  The arrival count only
+// grows (the host zeroes it before each launch): a block arriving as the k-th of all arrivals is in
+// barrier k / blocks and waits for the count to reach the end of that barrier, so no block has to
+// reset anything for the next one.
 __device__ __forceinline__ bool grid_barrier(const StageParams& p) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    volatile unsigned int* gen = p.bar_gen;
-    const unsigned int g = *gen;
+    const unsigned int G = gridDim.x;
     __threadfence();
-    const unsigned int arrived = atomicAdd(p.bar_count, 1u) + 1u;
-    if (arrived == gridDim.x) {
-      atomicExch(p.bar_count, 0u);
-      __threadfence();
-      atomicAdd(p.bar_gen, 1u);
-    } else {
-      long long it = 0;
-      while (*gen == g) {
-        if (++it > p.budget) {
-          atomicExch(p.status, 1);
-          break;
-        }
+    const unsigned int old = atomicAdd(p.bar_count, 1u);
+    const unsigned int target = (old / G + 1u) * G;
+    long long it = 0;
+    for (;;) {
+      unsigned int seen;
+      asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(p.bar_count) : "memory");
+      if (seen >= target) break;
+      if (++it > p.budget) {
+        atomicExch(p.status, 1);
+        break;
       }
     }
     __threadfence();
