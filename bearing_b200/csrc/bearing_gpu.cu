@@ -1,11 +1,14 @@
 // libbearing_gpu.so: the C ABI of include/bearing_gpu.h over the device solve stage in
 // stage.cuh.  Per context: one CUDA stream, device buffers grown by doubling (the rule
-// src/contact.js:250-255 uses for its columns), a staging copy of each input column in the
-// caller's layout (so bg_restore can run the same input again), and the packed device layout.
+// src/contact.js:250-255 uses for its columns), a staging block holding every input column in the
+// caller's layout (so bg_restore can run the same input again), the packed device layout, pinned
+// host staging and a small pool of host threads.
 //
-// A step is: copy the caller's columns in (one cudaMemcpyAsync per column), unpack them into
-// the device layout, run the solve stage (a persistent cooperative grid for a large world, one
-// CTA per world otherwise), pack the written columns and copy them out.
+// A step is: copy the caller's columns in (straight from page-locked caller memory, or gathered
+// into the pinned staging a group at a time, the copies overlapping the gathering) while another
+// host thread works out the solve order; unpack them into the device layout; run the solve stage
+// (a persistent cooperative grid for a large world, one CTA per world otherwise); pack the written
+// columns and copy them out the same way.
 #include <cuda_runtime.h>
 
 #include <algorithm>

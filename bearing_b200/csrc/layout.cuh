@@ -130,7 +130,8 @@ struct StageParams {
   double dt;
   int32_t substeps;
   Soft soft;
-  // grid barrier state and the step's status word (0 ok; 1 a wait ran past its budget)
+  // the grid barrier's arrival count and the step's status word (0 ok; 1 a wait ran past its
+  // budget)
   unsigned int* bar_count;
   int32_t* status;
   int32_t* block_counts;  // per-block counts for restitution's compaction
