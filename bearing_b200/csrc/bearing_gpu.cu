@@ -815,13 +815,22 @@ int order_rows(bg_ctx* c, const uint8_t* points, const int32_t* a, const int32_t
       if (inv_mass[y] != 0) c->rank[static_cast<size_t>(n) + d] = c->deg[static_cast<size_t>(y)]++;
     }
   }
-  // The grid's runs: each colour's rows in runs of 32, then the overflow's one row a run.
+  // The grid's runs: each colour's rows in runs of up to 32 that also end where the point count
+  // changes, so every warp runs one row solver (a warp whose lanes take two point counts runs the
+  // two one after the other), then the overflow's one row a run.
   c->chunks.clear();
   if (c->nworlds == 1) {
     const bg::WorldDesc& w = c->worlds[0];
-    for (int k = 0; k < bg::NCOLOURS; k++)
-      for (int m = w.starts[k]; m < w.starts[k + 1]; m += 32)
-        c->chunks.push_back(make_int2(m, std::min(32, w.starts[k + 1] - m)));
+    for (int k = 0; k < bg::NCOLOURS; k++) {
+      int m = w.starts[k];
+      while (m < w.starts[k + 1]) {
+        const int pc = points[c->perm[static_cast<size_t>(m)]];
+        int e = m + 1;
+        while (e < w.starts[k + 1] && e - m < 32 && points[c->perm[static_cast<size_t>(e)]] == pc) e++;
+        c->chunks.push_back(make_int2(m, e - m));
+        m = e;
+      }
+    }
     for (int m = w.starts[bg::OVERFLOW_RUN]; m < w.starts[bg::OVERFLOW_RUN + 1]; m++) c->chunks.push_back(make_int2(m, 1));
   }
   return BG_OK;
