@@ -1,8 +1,8 @@
 // The solve stage on the device: every phase of src/world.js:962-1032 as device functions over
 // the layout in layout.cuh, written once for a "team" of threads.  GridTeam is every thread of
-// a persistent cooperative grid working on one large world: grid-wide barriers between phases,
+// a persistent cooperative grid working on one world: grid-wide barriers between phases,
 // and within each row pass a dataflow over per-body counters instead of a barrier per colour (see
-// flow_pass).  BlockTeam is one CTA working on one small world, colour by colour with block
+// flow_pass).  BlockTeam is one CTA working on one world of a batch, colour by colour with block
 // barriers.  Within a colour no two rows share a body the solve moves (src/graph.js:1-33), so a
 // colour's rows run in any order with the same bits; across colours only each body's own order
 // of rows matters, which is what the counters keep.

@@ -63,9 +63,9 @@ extern "C" {
  * from directly; any other column goes through the library's own pinned staging, gathered and
  * scattered by a pool of host threads. */
 #define BG_FLAG_PIN_HOST 1u
-/* Run every single world on the persistent grid (the path large worlds take), whatever its size. */
+/* Run single worlds on the persistent grid (the default for a single world). */
 #define BG_FLAG_GRID 2u
-/* Run every single world on one CTA (the path small and batched worlds take), whatever its size. */
+/* Run single worlds on one CTA (the path batched worlds take) instead of the grid. */
 #define BG_FLAG_BLOCK 4u
 
 /* World body type codes: src/world.js TYPES (dynamic 0, static 1, kinematic 2, character 3). */
