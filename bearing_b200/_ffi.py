@@ -27,6 +27,7 @@ BG_EUNSUPPORTED = -5
 BG_EFAULT = -6
 
 BG_FLAG_PIN_HOST, BG_FLAG_GRID, BG_FLAG_BLOCK = 1, 2, 4
+BG_BATCH_ON_GRID = 1
 BG_STATIC_MAX_BODIES, BG_STATIC_MAX_ROWS = 512, 2048
 
 BG_DYNAMIC, BG_STATIC, BG_KINEMATIC = 0, 1, 2

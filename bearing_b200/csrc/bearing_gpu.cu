@@ -210,6 +210,8 @@ __global__ void __launch_bounds__(kGridThreads) stage_grid(bg::StageParams p) {
   bg::solve_stage(p, w, t);
 }
 
+__global__ void __launch_bounds__(kGridThreads) stage_grid_batch(bg::StageParams p) { bg::batch_stage(p); }
+
 __global__ void __launch_bounds__(kBlockThreads) stage_block(bg::StageParams p) {
   bg::BlockTeam t;
   for (int k = blockIdx.x; k < p.nworlds; k += gridDim.x) {
@@ -435,7 +437,11 @@ struct bg_ctx {
   int32_t* deg_dev = nullptr;
   unsigned int* done_dev = nullptr;
   int2* chunks_dev = nullptr;
-  std::vector<int32_t> rank, deg;
+  int32_t* body_world_dev = nullptr;   // each body's world (a batch on the grid)
+  int32_t* brun_rows_dev = nullptr;    // a batch's runs across worlds (see StageParams::bruns)
+  int2* bruns_dev = nullptr;
+  std::vector<int32_t> rank, deg, body_world, brun_rows;
+  std::vector<int2> bruns;
   // batches: the order CTAs take the worlds in, and the threads a world's CTA has (0: tune on the
   // next batched solve, see tune_block_threads)
   int32_t* order_dev = nullptr;
@@ -625,7 +631,7 @@ size_t grown(size_t have, size_t want) {
 
 // Bytes of the pinned block order_rows()'s tables pass through (see send_order).
 size_t meta_bytes(size_t nb, size_t nr) {
-  return 4 * nr * sizeof(int32_t) + nb * sizeof(int32_t) + (nr + 64) * sizeof(int2) + 5 * 256;
+  return 5 * nr * sizeof(int32_t) + 2 * nb * sizeof(int32_t) + 2 * (nr + 64) * sizeof(int2) + 8 * 256;
 }
 
 // (Re)allocates every buffer for at least the given sizes.  Everything is reallocated together,
@@ -665,7 +671,8 @@ bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
        dev_alloc(c, &R.rm1, nr) && dev_alloc(c, &R.rm2, nr) && dev_alloc(c, &R.sm, nr) &&
        dev_alloc(c, &R.active, nr) && dev_alloc(c, &R.pending, nr);
   ok = ok && dev_alloc(c, &c->perm_dev, nr) && dev_alloc(c, &c->iperm_dev, nr) && dev_alloc(c, &c->rank_dev, 2 * nr) &&
-       dev_alloc(c, &c->deg_dev, nb) && dev_alloc(c, &c->done_dev, nb) && dev_alloc(c, &c->chunks_dev, nr + 64);
+       dev_alloc(c, &c->deg_dev, nb) && dev_alloc(c, &c->done_dev, nb) && dev_alloc(c, &c->chunks_dev, nr + 64) &&
+       dev_alloc(c, &c->body_world_dev, nb) && dev_alloc(c, &c->brun_rows_dev, nr) && dev_alloc(c, &c->bruns_dev, nr + 64);
   // staging blocks, sized for the capacities (a call's own layout is never larger)
   {
     const size_t in_bytes = plan_in(c, nullptr, nullptr, nb, nr, na, nullptr).end;
@@ -821,19 +828,47 @@ int order_rows(bg_ctx* c, const uint8_t* points, const int32_t* a, const int32_t
   // changes, so every warp runs one row solver (a warp whose lanes take two point counts runs the
   // two one after the other), then the overflow's one row a run.
   c->chunks.clear();
-  if (c->nworlds == 1) {
-    const bg::WorldDesc& w = c->worlds[0];
+  for (const bg::WorldDesc& w : c->worlds) {
     for (int k = 0; k < bg::NCOLOURS; k++) {
-      int m = w.starts[k];
-      while (m < w.starts[k + 1]) {
+      int m = w.row0 + w.starts[k];
+      while (m < w.row0 + w.starts[k + 1]) {
         const int pc = points[c->perm[static_cast<size_t>(m)]];
         int e = m + 1;
-        while (e < w.starts[k + 1] && e - m < 32 && points[c->perm[static_cast<size_t>(e)]] == pc) e++;
+        while (e < w.row0 + w.starts[k + 1] && e - m < 32 && points[c->perm[static_cast<size_t>(e)]] == pc) e++;
         c->chunks.push_back(make_int2(m, e - m));
         m = e;
       }
     }
-    for (int m = w.starts[bg::OVERFLOW_RUN]; m < w.starts[bg::OVERFLOW_RUN + 1]; m++) c->chunks.push_back(make_int2(m, 1));
+    for (int m = w.starts[bg::OVERFLOW_RUN]; m < w.starts[bg::OVERFLOW_RUN + 1]; m++) c->chunks.push_back(make_int2(w.row0 + m, 1));
+  }
+  // A batch's runs for the grid: every world's rows of one colour and one point count together
+  // (rows of different worlds share no body), 32 a run, colour after colour; then each world's
+  // overflow rows, one a run, in their order.  Each run's rows wait only on rows of earlier runs.
+  c->brun_rows.clear();
+  c->bruns.clear();
+  if (c->nworlds > 1) {
+    for (int k = 0; k < bg::NCOLOURS; k++)
+      for (int pc = 1; pc <= bg::P; pc++) {
+        const size_t first = c->brun_rows.size();
+        for (const bg::WorldDesc& w : c->worlds)
+          for (int d = w.row0 + w.starts[k]; d < w.row0 + w.starts[k + 1]; d++) {
+            const int q = points[c->perm[static_cast<size_t>(d)]];
+            if ((q < 1 ? 1 : q > bg::P ? bg::P : q) == pc) c->brun_rows.push_back(d);
+          }
+        for (size_t r = first; r < c->brun_rows.size(); r += 32)
+          c->bruns.push_back(make_int2(static_cast<int>(r), static_cast<int>(std::min<size_t>(32, c->brun_rows.size() - r))));
+      }
+    for (const bg::WorldDesc& w : c->worlds)
+      for (int m = w.starts[bg::OVERFLOW_RUN]; m < w.starts[bg::OVERFLOW_RUN + 1]; m++) {
+        c->bruns.push_back(make_int2(static_cast<int>(c->brun_rows.size()), 1));
+        c->brun_rows.push_back(w.row0 + m);
+      }
+  }
+  // each body's world, for the body passes of a batch on the grid
+  c->body_world.assign(static_cast<size_t>(c->nbodies), 0);
+  for (size_t wi = 0; wi < c->worlds.size(); wi++) {
+    const bg::WorldDesc& w = c->worlds[wi];
+    for (int x = w.body0; x < w.body0 + w.nbodies; x++) c->body_world[static_cast<size_t>(x)] = static_cast<int32_t>(wi);
   }
   return BG_OK;
 }
@@ -855,7 +890,10 @@ int send_order(bg_ctx* c) {
                   send(c->iperm_dev, c->iperm.data(), n * sizeof(int32_t)) &&
                   send(c->rank_dev, c->rank.data(), 2 * n * sizeof(int32_t)) &&
                   send(c->deg_dev, c->deg.data(), static_cast<size_t>(c->nbodies) * sizeof(int32_t)) &&
-                  send(c->chunks_dev, c->chunks.data(), c->chunks.size() * sizeof(int2));
+                  send(c->chunks_dev, c->chunks.data(), c->chunks.size() * sizeof(int2)) &&
+                  send(c->body_world_dev, c->body_world.data(), c->body_world.size() * sizeof(int32_t)) &&
+                  send(c->brun_rows_dev, c->brun_rows.data(), c->brun_rows.size() * sizeof(int32_t)) &&
+                  send(c->bruns_dev, c->bruns.data(), c->bruns.size() * sizeof(int2));
   return ok ? BG_OK : BG_ECUDA;
 }
 
@@ -940,6 +978,11 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
   p.chunks = c->chunks_dev;
   p.nchunks = static_cast<int32_t>(c->chunks.size());
   p.world_order = c->batch ? c->order_dev : nullptr;
+  p.body_world = c->body_world_dev;
+  p.nawake_total = c->nawake;
+  p.brun_rows = c->brun_rows_dev;
+  p.bruns = c->bruns_dev;
+  p.nbruns = static_cast<int32_t>(c->bruns.size());
   if (!cuda_ok(c, cudaMemsetAsync(c->done_dev, 0, sizeof(unsigned int) * static_cast<size_t>(c->nbodies > 0 ? c->nbodies : 1),
                                   c->stream), "done")) return BG_ECUDA;
   if (!cuda_ok(c, cudaMemsetAsync(c->status, 0, sizeof(int32_t), c->stream), "status")) return BG_ECUDA;
@@ -948,6 +991,15 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
   if (!cuda_ok(c, cudaMemsetAsync(c->bar, 0, sizeof(unsigned int), c->stream), "barrier")) return BG_ECUDA;
   c->last_launches += 1;
   cudaEventRecord(c->stage_begin, c->stream);
+  if (c->batch && c->block_threads == BG_BATCH_ON_GRID) {
+    void* args[] = {&p};
+    const cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(stage_grid_batch), dim3(c->grid_blocks),
+                                                      dim3(kGridThreads), args, 0, c->stream);
+    if (!cuda_ok(c, e, "stage_grid_batch launch")) return BG_ECUDA;
+    cudaEventRecord(c->stage_end, c->stream);
+    c->stage_timed = true;
+    return BG_OK;
+  }
   bool big = !c->batch && c->nworlds == 1;
   if (!c->batch && (c->flags & BG_FLAG_GRID)) big = true;
   if (!c->batch && (c->flags & BG_FLAG_BLOCK)) big = false;
@@ -1081,8 +1133,8 @@ int32_t bg_last_launches(const bg_ctx* c) { return c == nullptr ? 0 : c->last_la
 
 int32_t bg_set_block_threads(bg_ctx* c, int32_t threads) {
   if (c == nullptr) return BG_EINVAL;
-  if (threads != 0 && threads != 32 && threads != 64 && threads != 128 && threads != 256) {
-    set_error(c, "block threads must be 0 (tune), 32, 64, 128 or 256");
+  if (threads != 0 && threads != BG_BATCH_ON_GRID && threads != 32 && threads != 64 && threads != 128 && threads != 256) {
+    set_error(c, "block threads must be 0 (tune), BG_BATCH_ON_GRID, 32, 64, 128 or 256");
     return BG_EINVAL;
   }
   c->block_threads = threads;
@@ -1232,7 +1284,7 @@ int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const b
 // (timed with events), the input is restored from staging after each, and the fastest is kept.
 // Results do not depend on the choice.
 static int tune_block_threads(bg_ctx* c, const bg_step* step) {
-  static const int kCandidates[] = {32, 64, 128, 256};
+  static const int kCandidates[] = {32, 64, 128, 256, BG_BATCH_ON_GRID};
   float best = 0;
   int chosen = kBlockThreads;
   cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -142,6 +142,14 @@ struct StageParams {
   int32_t nchunks;
   // The order CTAs take the worlds of a batch in (largest first), or NULL for 0, 1, 2, ...
   const int32_t* world_order;
+  // A batch on the grid: each body's world, and the awake entries of every world together.
+  const int32_t* body_world;
+  int32_t nawake_total;
+  // ... and its runs, drawn across worlds: run c is rows brun_rows[bruns[c].x ...][bruns[c].y]
+  // (one colour and one point count; each world's overflow rows last, one a run).
+  const int32_t* brun_rows;
+  const int2* bruns;
+  int32_t nbruns;
 };
 
 }  // namespace bg

@@ -1503,4 +1503,97 @@ __device__ bool solve_stage(const StageParams& p, const WorldDesc& w, const Team
   return true;
 }
 
+// Every world of a batch on the persistent grid, as one stage: the body passes over all worlds'
+// awake bodies at once (each with its own world's gravity), the row passes as one flow over all
+// worlds' runs (worlds share no body, so their rows never wait on each other), and restitution
+// and the drift update world by world, one block a world, since both keep each world's found
+// order.  The same operations as solve_stage on each world, in each body's same order.
+// A flow pass over a batch's runs (each row's turn exactly as in flow_pass).
+template <class F>
+__device__ __forceinline__ void batch_flow_pass(const StageParams& p, int pass, F row) {
+  const int lane = static_cast<int>(threadIdx.x) & 31;
+  const int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int warps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+  for (int c = warp; c < p.nbruns; c += warps) {
+    const int2 run = p.bruns[c];
+    if (lane < run.y) {
+      const int m = ldi(p.brun_rows + run.x + lane);
+      const int a = ldi(p.R.a + m), b = ldi(p.R.b + m);
+      const int ra = ldi(p.R.rank_a + m), rb = ldi(p.R.rank_b + m);
+      const unsigned int ta = flow_target(p, a, ra, pass), tb = flow_target(p, b, rb, pass);
+      row(m, [&](auto&& finish) {
+        long long it = 0;
+        for (;;) {
+          const unsigned int va = ta == 0 ? 0u : load_relaxed(p.B.done + a);
+          const unsigned int vb = tb == 0 ? 0u : load_relaxed(p.B.done + b);
+          if (va >= ta && vb >= tb) {
+            fence_acq_rel();
+            finish();
+            flow_signal(p, a, ra, ta, b, rb, tb);
+            return true;
+          }
+          if (++it > p.budget || ((it & 255) == 0 && *(volatile int32_t*)p.status != 0)) {
+            atomicExch(p.status, 1);
+            return false;
+          }
+          __nanosleep(200);
+        }
+      });
+    }
+    __syncwarp();
+  }
+}
+
+__device__ bool batch_stage(const StageParams& p) {
+  GridTeam t;
+  const int substeps = p.substeps;
+  const double h = p.dt / substeps;
+  const int lane = static_cast<int>(threadIdx.x) & 31;
+  const int warp = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int warps = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+  // every solved row once: the runs list holds exactly the solved rows of every world
+  auto each_row = [&](auto f) {
+    for (int c = warp; c < p.nbruns; c += warps) {
+      const int2 run = p.bruns[c];
+      if (lane < run.y) f(ldi(p.brun_rows + run.x + lane));
+    }
+  };
+  auto world_of_body = [&](int x) -> const WorldDesc& { return p.worlds[ldi(p.body_world + x)]; };
+  t.each(0, p.nawake_total, [&](int i) {
+    const int x = ldi(p.B.awake_list + i);
+    body_begin(p, x, world_of_body(x).nrows > 0);
+  });
+  if (!t.sync(p)) return false;
+  each_row([&](int m) { prepare_row(p, m); });
+  if (!t.sync(p)) return false;
+  int pass = 0;
+  for (int sub = 0; sub < substeps; sub++) {
+    t.each(0, p.nawake_total, [&](int i) {
+      const int x = ldi(p.B.awake_list + i);
+      accelerate_body(p, x, h, world_of_body(x).gravity);
+    });
+    if (!t.sync(p)) return false;
+    batch_flow_pass(p, pass++, [&](int m, auto gate) { warm_row(p, m, gate); });
+    if (sub > 0) batch_flow_pass(p, pass++, [&](int m, auto gate) { solve_row<true, true>(p, m, h, gate); });
+    else batch_flow_pass(p, pass++, [&](int m, auto gate) { solve_row<true, false>(p, m, h, gate); });
+    if (!t.sync(p)) return false;
+    t.each(0, p.nawake_total, [&](int i) { move_body(p, ldi(p.B.awake_list + i), h); });
+    if (!t.sync(p)) return false;
+    batch_flow_pass(p, pass++, [&](int m, auto gate) { solve_row<false, false>(p, m, h, gate); });
+    if (!t.sync(p)) return false;
+  }
+  BlockTeam bt;
+  for (int wi = blockIdx.x; wi < p.nworlds; wi += gridDim.x) {
+    const WorldDesc w = p.worlds[wi];
+    if (w.nrows > 0) {
+      const double* g = w.gravity;
+      const double gravity = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+      if (!restitution_stage(p, w, bt, gravity)) return false;
+      bt.each(0, w.solved, [&](int m) { slipped_row(p, w.row0 + m); });
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
 }  // namespace bg

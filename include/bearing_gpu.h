@@ -217,12 +217,14 @@ double bg_last_stage_ms(bg_ctx* ctx);
 /* Grid barriers each colour pass waits at, and the spin budget (iterations) of each wait.
  * 0 restores the default.  A wait past its budget makes the step return BG_ETIMEOUT. */
 int32_t bg_set_wait_budget(bg_ctx* ctx, int64_t iterations);
-/* Threads of each world's CTA in batched solves (no counterpart in the reference: a Bearing World
- * steps alone).  0 (the default) tunes it on the next bg_batch_solve / bg_batch_solve_step: each of
- * 32, 64, 128 and 256 solves the uploaded batch once, timed, from the same input, and the fastest
- * is kept for the context's later batched solves.  Results never depend on it. */
+/* How batched solves run (no counterpart in the reference: a Bearing World steps alone): one CTA of
+ * 32, 64, 128 or 256 threads a world, or BG_BATCH_ON_GRID, every world on the persistent grid as
+ * one flow.  0 (the default) tunes it on the next bg_batch_solve / bg_batch_solve_step: each
+ * candidate solves the uploaded batch once, timed, from the same input, and the fastest is kept
+ * for the context's later batched solves.  Results never depend on it. */
+#define BG_BATCH_ON_GRID 1
 int32_t bg_set_block_threads(bg_ctx* ctx, int32_t threads);
-/* The threads batched solves use now (0 until tuned). */
+/* What batched solves use now (0 until tuned). */
 int32_t bg_block_threads(const bg_ctx* ctx);
 
 /*

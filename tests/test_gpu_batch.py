@@ -38,7 +38,8 @@ def test_batched_worlds_match_the_oracle_world_by_world():
 
 
 def test_batched_results_do_not_depend_on_the_cta_size():
-    # 32, 64 and 256 threads a world, and the tuner's own choice: the same bits, the oracle's.
+    # 32, 64 and 256 threads a world, every world on the grid as one flow, and the tuner's own
+    # choice: the same bits, the oracle's.
     import ctypes as C
     from stage_io import BatchCopy, first_difference
     from bearing_b200 import _ffi
@@ -58,7 +59,7 @@ def test_batched_results_do_not_depend_on_the_cta_size():
         host.bw_batch_destroy(b)
     g = _ffi.gpu()
     want = [oracle_io.solve(base.world(i).copy()) for i in range(base.worlds)]
-    for threads in (32, 64, 256, 0):
+    for threads in (32, 64, 256, _ffi.BG_BATCH_ON_GRID, 0):
         ctx = g.bg_create(0, 0)
         try:
             assert g.bg_set_block_threads(ctx, threads) == 0
@@ -67,7 +68,7 @@ def test_batched_results_do_not_depend_on_the_cta_size():
             rc = g.bg_batch_solve_step(ctx, C.byref(Bw), C.byref(Rw), C.byref(Ww), C.byref(Sw))
             assert rc == 0, g.bg_last_error(ctx).decode()
             used = g.bg_block_threads(ctx)
-            assert used == threads if threads else used in (32, 64, 128, 256)
+            assert used == threads if threads else used in (32, 64, 128, 256, _ffi.BG_BATCH_ON_GRID)
             for i in range(base.worlds):
                 d = first_difference(want[i], work.world(i))
                 assert d is None, f"{threads} threads, world {i}: {d}"
