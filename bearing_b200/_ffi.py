@@ -28,6 +28,7 @@ BG_EFAULT = -6
 
 BG_FLAG_PIN_HOST, BG_FLAG_GRID, BG_FLAG_BLOCK = 1, 2, 4
 BG_BATCH_ON_GRID = 1
+BG_MAX_BATCH_GROUPS = 8
 BG_STATIC_MAX_BODIES, BG_STATIC_MAX_ROWS = 512, 2048
 
 BG_DYNAMIC, BG_STATIC, BG_KINEMATIC = 0, 1, 2
@@ -246,6 +247,8 @@ def gpu() -> C.CDLL:
         lib.bg_set_block_threads.restype = C.c_int32
         lib.bg_block_threads.argtypes = [C.c_void_p]
         lib.bg_block_threads.restype = C.c_int32
+        lib.bg_set_batch_groups.argtypes = [C.c_void_p, C.c_int32]
+        lib.bg_set_batch_groups.restype = C.c_int32
         lib.bg_solve_step_static.argtypes = [C.POINTER(Bodies), C.POINTER(Rows), C.POINTER(Step), C.c_void_p]
         lib.bg_solve_step_static.restype = C.c_int32
         for f in ("bg_solve_step", "bg_upload", "bg_restore", "bg_solve", "bg_download",
@@ -261,7 +264,7 @@ GPU_SYMBOLS = [
     "bg_create", "bg_destroy", "bg_last_error", "bg_version", "bg_solve_step", "bg_upload", "bg_restore",
     "bg_solve", "bg_download", "bg_batch_solve_step", "bg_batch_upload", "bg_batch_solve",
     "bg_batch_download", "bg_stream", "bg_last_launches", "bg_last_stage_ms", "bg_set_wait_budget", "bg_set_block_threads",
-    "bg_block_threads", "bg_solve_step_static",
+    "bg_block_threads", "bg_set_batch_groups", "bg_solve_step_static",
 ]
 HOST_SYMBOLS = [
     "bw_create", "bw_destroy", "bw_last_error", "bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step",

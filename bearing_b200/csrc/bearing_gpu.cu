@@ -32,6 +32,8 @@ namespace {
 
 constexpr int kGridThreads = 256;
 constexpr int kBlockThreads = 256;
+// bg_batch_solve_step's rows per group of worlds (twice as many for pageable columns; see groups_for).
+constexpr int kRowsPerGroup = 131072;
 constexpr int kUnpackThreads = 256;
 // A single world runs on the whole grid whatever its size: measured against one CTA on B200 it was
 // faster at every size tried, from a 10-row stack (0.37 against 0.47 ms a step) and the 590-row
@@ -448,6 +450,10 @@ struct bg_ctx {
   std::vector<int32_t> world_order;
   int block_threads = 0;
   std::vector<int2> chunks;
+  // bg_batch_solve_step's groups of worlds (see batch_in_groups): how many (0 by the batch's rows),
+  // and a context of its own for each
+  int batch_groups = 0;
+  std::vector<bg_ctx*> kids;
   // staging out
   BodyOut bout = {};
   RowOut rout = {};
@@ -844,9 +850,10 @@ int order_rows(bg_ctx* c, const uint8_t* points, const int32_t* a, const int32_t
   // A batch's runs for the grid: every world's rows of one colour and one point count together
   // (rows of different worlds share no body), 32 a run, colour after colour; then each world's
   // overflow rows, one a run, in their order.  Each run's rows wait only on rows of earlier runs.
+  // (A batch of one world needs them too: it may run on the grid as a batch.)
   c->brun_rows.clear();
   c->bruns.clear();
-  if (c->nworlds > 1) {
+  if (c->batch) {
     for (int k = 0; k < bg::NCOLOURS; k++)
       for (int pc = 1; pc <= bg::P; pc++) {
         const size_t first = c->brun_rows.size();
@@ -1114,6 +1121,8 @@ void bg_destroy(bg_ctx* c) {
   if (c == nullptr) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (bg_ctx* k : c->kids) bg_destroy(k);
+  c->kids.clear();
   free_all(c);
   c->pool.reset();
   if (c->in_free) cudaEventDestroy(c->in_free);
@@ -1225,9 +1234,12 @@ int32_t bg_solve_step(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_
   return bg_download(c, B, R);
 }
 
-int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_worlds* W) {
-  if (c == nullptr) return BG_EINVAL;
-  cudaSetDevice(c->device);
+}  // extern "C"
+
+namespace {
+
+// A batch's table of worlds from the caller's offsets, every world checked.
+int batch_worlds(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_worlds* W, std::vector<bg::WorldDesc>& worlds) {
   int rc = validate(c, B, R);
   if (rc != BG_OK) return rc;
   if (W == nullptr || W->count < 1 || W->body_offset == nullptr || W->awake_offset == nullptr ||
@@ -1241,7 +1253,7 @@ int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const b
     set_error(c, "batch: offsets must start at 0 and end at the arrays' lengths");
     return BG_EINVAL;
   }
-  std::vector<bg::WorldDesc> worlds(static_cast<size_t>(nw));
+  worlds.assign(static_cast<size_t>(nw), bg::WorldDesc{});
   for (int i = 0; i < nw; i++) {
     bg::WorldDesc& w = worlds[static_cast<size_t>(i)];
     w.body0 = W->body_offset[i];
@@ -1260,6 +1272,20 @@ int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const b
     if (rc != BG_OK) return rc;
     for (int k = 0; k < 3; k++) w.gravity[k] = W->gravity != nullptr ? W->gravity[3 * i + k] : NAN;
   }
+  return BG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_worlds* W) {
+  if (c == nullptr) return BG_EINVAL;
+  cudaSetDevice(c->device);
+  std::vector<bg::WorldDesc> worlds;
+  int rc = batch_worlds(c, B, R, W, worlds);
+  if (rc != BG_OK) return rc;
+  const int nw = W->count;
   c->last_launches = 0;
   if (!ensure(c, B->capacity, R->count, B->awake_count, nw)) return BG_ENOMEM;
   c->nbodies = B->capacity;
@@ -1342,7 +1368,194 @@ int32_t bg_batch_solve(bg_ctx* c, const bg_step* step) {
 
 int32_t bg_batch_download(bg_ctx* c, const bg_bodies* B, const bg_rows* R) { return bg_download(c, B, R); }
 
+int32_t bg_set_batch_groups(bg_ctx* c, int32_t groups) {
+  if (c == nullptr) return BG_EINVAL;
+  if (groups < 0 || groups > BG_MAX_BATCH_GROUPS) {
+    set_error(c, "batch groups must be 0 (by the batch's rows) to %d", BG_MAX_BATCH_GROUPS);
+    return BG_EINVAL;
+  }
+  c->batch_groups = groups;
+  return BG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+template <class T>
+T* advanced(T* p, size_t k) { return p == nullptr ? nullptr : p + k; }
+
+// Worlds [w0, w1) of a batch: the caller's columns advanced to the group's first slot, awake entry
+// and row (slots, awake entries and rows are local to their world, so no value changes), and the
+// group's own table of offsets.
+struct Group {
+  bg_bodies B;
+  bg_rows R;
+  bg_worlds W;
+  std::vector<int32_t> body_offset, awake_offset, row_offset;
+};
+
+void make_group(Group& g, const bg_bodies* B, const bg_rows* R, const bg_worlds* W, int w0, int w1) {
+  const size_t s = static_cast<size_t>(W->body_offset[w0]), a = static_cast<size_t>(W->awake_offset[w0]),
+               r = static_cast<size_t>(W->row_offset[w0]);
+  for (int i = w0; i <= w1; i++) {
+    g.body_offset.push_back(W->body_offset[i] - static_cast<int32_t>(s));
+    g.awake_offset.push_back(W->awake_offset[i] - static_cast<int32_t>(a));
+    g.row_offset.push_back(W->row_offset[i] - static_cast<int32_t>(r));
+  }
+  g.B = *B;
+  g.B.capacity = g.body_offset.back();
+  g.B.awake_count = g.awake_offset.back();
+  g.B.awake_list = advanced(B->awake_list, a);
+  g.B.awake = advanced(B->awake, s);
+  g.B.position = advanced(B->position, 3 * s);
+  g.B.rotation = advanced(B->rotation, 4 * s);
+  g.B.velocity = advanced(B->velocity, 3 * s);
+  g.B.angular = advanced(B->angular, 3 * s);
+  g.B.tumbled = advanced(B->tumbled, 3 * s);
+  g.B.ceiling = advanced(B->ceiling, s);
+  g.B.start = advanced(B->start, 3 * s);
+  g.B.start_q = advanced(B->start_q, 4 * s);
+  g.B.inv_i = advanced(B->inv_i, 6 * s);
+  g.B.inv_mass = advanced(B->inv_mass, s);
+  g.B.inertia = advanced(B->inertia, 3 * s);
+  g.B.inv_inertia = advanced(B->inv_inertia, 3 * s);
+  g.B.dims = advanced(B->dims, 3 * s);
+  g.B.damping = advanced(B->damping, s);
+  g.B.angular_damping = advanced(B->angular_damping, s);
+  g.B.gravity_scale = advanced(B->gravity_scale, s);
+  g.B.type = advanced(B->type, s);
+  g.B.shape = advanced(B->shape, s);
+  g.B.frozen = advanced(B->frozen, s);
+  g.B.framed = advanced(B->framed, s);
+  g.B.lock = advanced(B->lock, s);
+  g.B.joint_head = advanced(B->joint_head, s);
+  g.R = *R;
+  g.R.count = g.row_offset.back();
+  g.R.row = advanced(R->row, r);
+  g.R.a = advanced(R->a, r);
+  g.R.b = advanced(R->b, r);
+  g.R.points = advanced(R->points, r);
+  g.R.normal = advanced(R->normal, 3 * r);
+  g.R.t1 = advanced(R->t1, 3 * r);
+  g.R.t2 = advanced(R->t2, 3 * r);
+  g.R.friction = advanced(R->friction, r);
+  g.R.restitution = advanced(R->restitution, r);
+  g.R.tolerance = advanced(R->tolerance, r);
+  g.R.patch = advanced(R->patch, r);
+  g.R.separation = advanced(R->separation, 4 * r);
+  g.R.point = advanced(R->point, 12 * r);
+  g.R.shift = advanced(R->shift, 12 * r);
+  g.R.normal_impulse = advanced(R->normal_impulse, 4 * r);
+  g.R.tangent_impulse1 = advanced(R->tangent_impulse1, r);
+  g.R.tangent_impulse2 = advanced(R->tangent_impulse2, r);
+  g.R.roll_impulse1 = advanced(R->roll_impulse1, r);
+  g.R.roll_impulse2 = advanced(R->roll_impulse2, r);
+  g.R.spin_impulse = advanced(R->spin_impulse, r);
+  g.R.drift1 = advanced(R->drift1, r);
+  g.R.drift2 = advanced(R->drift2, r);
+  g.R.gap = advanced(R->gap, r);
+  g.R.max_normal_impulse = advanced(R->max_normal_impulse, 4 * r);
+  g.R.relative_velocity = advanced(R->relative_velocity, 4 * r);
+  g.R.sliding = advanced(R->sliding, r);
+  g.R.anchor_a = advanced(R->anchor_a, 3 * r);
+  g.R.anchor_b = advanced(R->anchor_b, 3 * r);
+  g.W.count = w1 - w0;
+  g.W.body_offset = g.body_offset.data();
+  g.W.awake_offset = g.awake_offset.data();
+  g.W.row_offset = g.row_offset.data();
+  g.W.starts = W->starts + static_cast<size_t>(bg::NSTARTS) * static_cast<size_t>(w0);
+  g.W.gravity = advanced(W->gravity, 3 * static_cast<size_t>(w0));
+}
+
+// How many groups bg_batch_solve_step splits a batch into: by its rows unless the caller chose.
+int groups_for(const bg_ctx* c, const bg_rows* R, const bg_worlds* W) {
+  if (R == nullptr || W == nullptr || W->count < 2) return 1;
+  int g = c->batch_groups;
+  // Page-locked columns go straight to the device, so more groups overlap more; pageable ones are
+  // gathered by host threads, and the groups' gathers and scatters then compete for the host's
+  // memory bandwidth (4,096 worlds, 845,037 rows: page-locked 36 ms in one piece, 24 ms in 4-6
+  // groups; pageable 42 ms, 35 ms in 2-3 groups, 43 ms in 8).
+  if (g == 0) {
+    const int64_t per = host_pinned(R->normal) ? kRowsPerGroup : 2 * static_cast<int64_t>(kRowsPerGroup);
+    g = static_cast<int>(std::min<int64_t>(BG_MAX_BATCH_GROUPS, R->count / per));
+  }
+  return std::max(1, std::min(g, W->count));
+}
+
+// bg_batch_solve_step in groups of whole worlds, each on a context of its own: group g+1's columns
+// are gathered and copied in while group g solves, and group g's results go back (on a thread of
+// their own) while later groups solve.  Worlds are independent, so each world's results are the
+// ones a single launch gives.  The whole batch is checked first, so a refused batch writes nothing.
+int batch_in_groups(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_worlds* W, const bg_step* step, int groups) {
+  std::vector<bg::WorldDesc> worlds;
+  int rc = batch_worlds(c, B, R, W, worlds);
+  if (rc != BG_OK) return rc;
+  if (step == nullptr || !(step->dt > 0) || step->substeps < 1) {
+    set_error(c, "step: dt must be positive and substeps at least 1");
+    return BG_EINVAL;
+  }
+  while (static_cast<int>(c->kids.size()) < groups) {
+    bg_ctx* k = bg_create(c->device, c->flags);
+    if (k == nullptr) {
+      set_error(c, "batch: no context for a group of worlds");
+      return BG_ENOMEM;
+    }
+    c->kids.push_back(k);
+  }
+  // Whole worlds, split where the running count of rows and slots passes each group's share.
+  const int nw = W->count;
+  const double total = static_cast<double>(R->count) + static_cast<double>(B->capacity);
+  std::vector<int> first(1, 0);
+  for (int i = 1; i < nw && static_cast<int>(first.size()) < groups; i++) {
+    const double upto = static_cast<double>(W->row_offset[i]) + static_cast<double>(W->body_offset[i]);
+    if (upto >= total * static_cast<double>(first.size()) / groups) first.push_back(i);
+  }
+  first.push_back(nw);
+  const int n = static_cast<int>(first.size()) - 1;
+  std::vector<Group> part(static_cast<size_t>(n));
+  for (int g = 0; g < n; g++) make_group(part[static_cast<size_t>(g)], B, R, W, first[static_cast<size_t>(g)], first[static_cast<size_t>(g) + 1]);
+  c->uploaded = false;   // what the context held is not this batch
+  c->last_launches = 0;
+  std::vector<int> rcs(static_cast<size_t>(n), BG_OK);
+  std::vector<std::thread> downloads;
+  int failed = -1;
+  for (int g = 0; g < n && failed < 0; g++) {
+    bg_ctx* k = c->kids[static_cast<size_t>(g)];
+    Group& p = part[static_cast<size_t>(g)];
+    k->budget = c->budget;
+    if (c->block_threads != 0) k->block_threads = c->block_threads;
+    int r = bg_batch_upload(k, &p.B, &p.R, &p.W);
+    if (r == BG_OK) r = bg_batch_solve(k, step);
+    if (r != BG_OK) {
+      rcs[static_cast<size_t>(g)] = r;
+      failed = g;
+      break;
+    }
+    downloads.emplace_back([k, &p, &rcs, g] { rcs[static_cast<size_t>(g)] = bg_batch_download(k, &p.B, &p.R); });
+  }
+  for (std::thread& t : downloads) t.join();
+  cudaSetDevice(c->device);
+  for (int g = 0; g < n; g++) {
+    bg_ctx* k = c->kids[static_cast<size_t>(g)];
+    c->last_launches += k->last_launches;
+    if (rcs[static_cast<size_t>(g)] != BG_OK && rc == BG_OK) {
+      rc = rcs[static_cast<size_t>(g)];
+      set_error(c, "batch group %d of %d: %s", g, n, k->error.c_str());
+    }
+  }
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
 int32_t bg_batch_solve_step(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_worlds* W, const bg_step* step) {
+  if (c == nullptr) return BG_EINVAL;
+  cudaSetDevice(c->device);
+  const int groups = groups_for(c, R, W);
+  if (groups > 1) return batch_in_groups(c, B, R, W, step, groups);
   int rc = bg_batch_upload(c, B, R, W);
   if (rc != BG_OK) return rc;
   rc = bg_batch_solve(c, step);

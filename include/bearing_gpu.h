@@ -200,7 +200,11 @@ int32_t bg_restore(bg_ctx* ctx);
 int32_t bg_solve(bg_ctx* ctx, const bg_step* step);
 int32_t bg_download(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows);
 
-/* Batched worlds: one CTA per small world, the same solve stage, one launch for all. */
+/* Batched worlds: one CTA per small world (or every world on the persistent grid), the same solve
+ * stage, one launch for all.  bg_batch_solve_step moves a large batch in groups of whole worlds
+ * (bg_set_batch_groups): each group is copied in while the one before it solves, and its results
+ * copied back while the next solves.  A batch split so leaves nothing uploaded on the context
+ * (bg_restore and bg_batch_solve then return BG_EINVAL until the next upload). */
 int32_t bg_batch_solve_step(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows,
                             const bg_worlds* worlds, const bg_step* step);
 int32_t bg_batch_upload(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows, const bg_worlds* worlds);
@@ -226,6 +230,12 @@ int32_t bg_set_wait_budget(bg_ctx* ctx, int64_t iterations);
 int32_t bg_set_block_threads(bg_ctx* ctx, int32_t threads);
 /* What batched solves use now (0 until tuned). */
 int32_t bg_block_threads(const bg_ctx* ctx);
+/* How many groups of whole worlds bg_batch_solve_step splits a batch into, 1 to
+ * BG_MAX_BATCH_GROUPS (1: never split), or 0 (the default): one group per 131,072 rows when the
+ * row columns are in page-locked memory, per 262,144 rows otherwise, and a smaller batch unsplit.
+ * A group never holds less than one world.  Results never depend on it. */
+#define BG_MAX_BATCH_GROUPS 8
+int32_t bg_set_batch_groups(bg_ctx* ctx, int32_t groups);
 
 /*
  * The solve stage without allocating: no counterpart in the reference.

@@ -188,6 +188,15 @@ class BatchCopy:
     def fill(self, other):
         self.stage.fill(other.stage)
 
+    def pinned(self):
+        """The same batch with its columns in page-locked host memory (see StageCopy.pinned)."""
+        c = BatchCopy.__new__(BatchCopy)
+        c.stage = self.stage.pinned()
+        c.worlds = self.worlds
+        for k in ("body_offset", "awake_offset", "row_offset", "starts"):
+            setattr(c, k, getattr(self, k).copy())
+        return c
+
     def views(self):
         B, R, S = self.stage.views()
         W = _ffi.Worlds(self.worlds, _ptr(self.body_offset, np.int32), _ptr(self.awake_offset, np.int32),
