@@ -101,6 +101,22 @@ def algorithmic_bytes(copy):
     return int(total)
 
 
+def batch_algorithmic_bytes(batch):
+    """algorithmic_bytes over every world of a batch (a BatchCopy): each world's solved rows are
+    its first starts[33] rows, and every awake body of every world takes the body passes."""
+    import numpy as np
+    st = batch.stage
+    pts = np.concatenate([st.rows["points"][int(batch.row_offset[w]): int(batch.row_offset[w]) + int(batch.starts[35 * w + 33])]
+                          for w in range(batch.worlds)]).astype(np.int64)
+
+    class Solved:
+        rows = {"points": pts}
+        solved = int(pts.size)
+        awake_count = st.awake_count
+
+    return algorithmic_bytes(Solved)
+
+
 # ---- clocks -------------------------------------------------------------------------------
 
 class Clocks:
@@ -332,6 +348,7 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
     batch.destroy()
     ms_res, ms_bat, ms_loop = statistics.mean(resident), statistics.mean(batched), min(loop)
     ms_lock = statistics.mean(batched_locked)
+    algo = batch_algorithmic_bytes(base)   # this rank's worlds
     slots, rows = int(base.stage.capacity), int(base.stage.count)
     solved = int(sum(int(base.starts[k * 35 + 33]) for k in range(base.worlds)))
     if dist:
@@ -351,7 +368,40 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
             "batched_e2e": {"value": n / (ms_bat / 1000), "ms_per_step": ms_bat, "host_memory": "pageable"},
             "batched_e2e_page_locked": {"value": n / (ms_lock / 1000), "ms_per_step": ms_lock},
             "per_world_loop_e2e": {"value": n / (ms_loop / 1000), "ms_per_step": ms_loop},
-            "speedup_e2e": ms_loop / ms_bat, "bit_identical": same, "cta_threads": cta_threads}
+            "speedup_e2e": ms_loop / ms_bat, "bit_identical": same, "cta_threads": cta_threads,
+            "roofline": batch_roofline(algo, ms_res)}
+
+
+def batch_roofline(algo, ms):
+    """The batched kernel's roofline line: this rank's algorithmic bytes over the resident solve's
+    time (the max over ranks), against the measured HBM copy rate; DRAM traffic scaled from the
+    committed capture of 1,024 of the same worlds by algorithmic bytes."""
+    hbm, peak_source = hbm_peak()
+    achieved = algo / (ms / 1000) / 1e9
+    traffic = None
+    try:
+        got = {}
+        for line in open(os.path.join(ROOT, "profiles", "stage_grid_batch_1024worlds.md")):
+            key, _, value = line.partition(":")
+            if key in ("traffic_bytes_per_launch", "algorithmic_bytes_per_launch"):
+                got[key] = int(value)
+        traffic = int(round(got["traffic_bytes_per_launch"] * algo / got["algorithmic_bytes_per_launch"]))
+    except (OSError, ValueError, KeyError):
+        pass
+    return {"bound": "hbm", "kernel": "stage_grid_batch", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "algorithmic_bytes": algo, "traffic": traffic,
+            "traffic_source": "ncu capture of 1,024 of the worlds, scaled by algorithmic bytes",
+            "peak_source": peak_source}
+
+
+def hbm_peak():
+    """The HBM denominator: the measured copy rate in MEASURED_PEAKS.json where that file exists,
+    else the earlier measurement of this GPU type's copy rate, 6,650 GB/s."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), \
+            "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "6,650 GB/s, an earlier copy-rate measurement on B200 (of fallback; no MEASURED_PEAKS.json)"
 
 
 def host_threads():
@@ -446,12 +496,7 @@ def main():
     rows_per_stage = copy.solved * SUBSTEPS * 3
     value = world_size * rows_per_stage / (ms / 1000)
     e2e = world_size * rows_per_stage / (ms_e2e / 1000)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    hbm, peak_source = hbm_peak()
     achieved = algo / (ms_stage / 1000) / 1e9
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu and not args.resident_only:
@@ -479,7 +524,7 @@ def main():
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": measured_traffic(args.bodies, algo),
                              "traffic_source": "ncu capture at step 101, scaled by algorithmic bytes", "kernel_ms": ms_stage,
-                             "algorithmic_bytes": algo, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                             "algorithmic_bytes": algo, "peak_source": peak_source},
                 "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches, "batch": batch}
         print(json.dumps(line), flush=True)
     lib.bg_destroy(ctx)
