@@ -369,10 +369,10 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
             "batched_e2e_page_locked": {"value": n / (ms_lock / 1000), "ms_per_step": ms_lock},
             "per_world_loop_e2e": {"value": n / (ms_loop / 1000), "ms_per_step": ms_loop},
             "speedup_e2e": ms_loop / ms_bat, "bit_identical": same, "cta_threads": cta_threads,
-            "roofline": batch_roofline(algo, ms_res)}
+            "roofline": batch_roofline(algo, ms_res, cta_threads)}
 
 
-def batch_roofline(algo, ms):
+def batch_roofline(algo, ms, cta_threads):
     """The batched kernel's roofline line: this rank's algorithmic bytes over the resident solve's
     time (the max over ranks), against the measured HBM copy rate; DRAM traffic scaled from the
     committed capture of 1,024 of the same worlds by algorithmic bytes."""
@@ -388,7 +388,8 @@ def batch_roofline(algo, ms):
         traffic = int(round(got["traffic_bytes_per_launch"] * algo / got["algorithmic_bytes_per_launch"]))
     except (OSError, ValueError, KeyError):
         pass
-    return {"bound": "hbm", "kernel": "stage_grid_batch", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+    kernel = "stage_grid_batch" if cta_threads == 1 else f"stage_block ({cta_threads} threads a world)"
+    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "algorithmic_bytes": algo, "traffic": traffic,
             "traffic_source": "ncu capture of 1,024 of the worlds, scaled by algorithmic bytes",
             "peak_source": peak_source}
