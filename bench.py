@@ -263,8 +263,9 @@ def measured_traffic(bodies, algorithmic):
 
 
 def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None):
-    """Config 4: many small independent worlds solved in one launch (bg_batch_*, one CTA a world)
-    against the plain path called world by world (bg_solve_step).  The worlds (a pyramid, a box
+    """Batched worlds: many small independent worlds solved in one launch (bg_batch_*: one CTA a
+    world or all of them on the persistent grid, as the library's tuner picks), against the plain
+    path called world by world (bg_solve_step).  The worlds (a pyramid, a box
     stack or a sphere pile of 8..512 bodies each, friction U(0.3, 0.8), restitution U(0, 0.4)) are
     stepped together to step `batch_at`; then that step's solve stage is timed: batched with its
     input resident, batched through bg_batch_solve_step with host arrays, and as a loop of

@@ -237,7 +237,7 @@ def test_pyramid_on_the_grid_path():
 
 @pytest.mark.parametrize("config", ["pyramid", "rain"])
 def test_gpu_world_matches_oracle_world_over_600_steps(config):
-    # The whole loop at the survey's configs 1 and 2: the 20-row pyramid (210 boxes) and 2,000
+    # The whole loop on the two parity workloads: the 20-row pyramid (210 boxes) and 2,000
     # spheres raining into a walled container, 600 steps each, a World on the GPU against the
     # same World on the oracle, state and transforms identical after every step while the
     # oracle's world stays finite.  The rain goes non-finite in the reference's own arithmetic
