@@ -1525,14 +1525,29 @@ int batch_in_groups(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_wo
     Group& p = part[static_cast<size_t>(g)];
     k->budget = c->budget;
     if (c->block_threads != 0) k->block_threads = c->block_threads;
-    int r = bg_batch_upload(k, &p.B, &p.R, &p.W);
-    if (r == BG_OK) r = bg_batch_solve(k, step);
+    int r = BG_ENOMEM;
+    try {   // nothing may leave this loop by an exception while download threads run
+      r = bg_batch_upload(k, &p.B, &p.R, &p.W);
+      if (r == BG_OK) r = bg_batch_solve(k, step);
+    } catch (const std::exception&) {
+      set_error(k, "out of host memory");
+    }
     if (r != BG_OK) {
       rcs[static_cast<size_t>(g)] = r;
       failed = g;
       break;
     }
-    downloads.emplace_back([k, &p, &rcs, g] { rcs[static_cast<size_t>(g)] = bg_batch_download(k, &p.B, &p.R); });
+    try {
+      downloads.emplace_back([k, &p, &rcs, g] {
+        try {
+          rcs[static_cast<size_t>(g)] = bg_batch_download(k, &p.B, &p.R);
+        } catch (const std::exception&) {
+          rcs[static_cast<size_t>(g)] = BG_ENOMEM;
+        }
+      });
+    } catch (const std::exception&) {   // no thread to be had: this group's results come back now
+      rcs[static_cast<size_t>(g)] = bg_batch_download(k, &p.B, &p.R);
+    }
   }
   for (std::thread& t : downloads) t.join();
   cudaSetDevice(c->device);
@@ -1555,7 +1570,14 @@ int32_t bg_batch_solve_step(bg_ctx* c, const bg_bodies* B, const bg_rows* R, con
   if (c == nullptr) return BG_EINVAL;
   cudaSetDevice(c->device);
   const int groups = groups_for(c, R, W);
-  if (groups > 1) return batch_in_groups(c, B, R, W, step, groups);
+  if (groups > 1) {
+    try {
+      return batch_in_groups(c, B, R, W, step, groups);
+    } catch (const std::bad_alloc&) {
+      set_error(c, "batch: out of host memory");
+      return BG_ENOMEM;
+    }
+  }
   int rc = bg_batch_upload(c, B, R, W);
   if (rc != BG_OK) return rc;
   rc = bg_batch_solve(c, step);
