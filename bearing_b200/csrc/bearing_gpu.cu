@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <condition_variable>
 #include <cstdarg>
@@ -45,7 +46,7 @@ constexpr long long kDefaultBudget = 1LL << 24;
 
 struct BodyStage {
   const double* position; const double* rotation; const double* velocity; const double* angular;
-  const double* tumbled; const double* ceiling; const double* start; const double* inv_mass;
+  const double* tumbled; const double* ceiling; const double* start; const double* start_q; const double* inv_mass;
   const double* inertia; const double* inv_inertia; const double* dims; const double* damping;
   const double* angular_damping; const double* gravity_scale;
   const uint8_t* type; const uint8_t* shape; const uint8_t* frozen; const uint8_t* framed;
@@ -99,7 +100,7 @@ __global__ void unpack_bodies(BodyStage in, bg::BodiesDev B, int n, const int32_
     B.vw[8 * s + 6] = 0; B.vw[8 * s + 7] = 0;
     B.pq[8 * s + 3] = 0;
     B.st[4 * s + 3] = 0;
-    for (int k = 0; k < 4; k++) { B.pq[8 * s + 4 + k] = in.rotation[4 * s + k]; B.sq[4 * s + k] = 0; }
+    for (int k = 0; k < 4; k++) { B.pq[8 * s + 4 + k] = in.rotation[4 * s + k]; B.sq[4 * s + k] = in.start_q[4 * s + k]; }
     B.tc[4 * s + 3] = in.ceiling[s];
     B.pr[12 * s + 9] = in.damping[s];
     B.pr[12 * s + 10] = in.angular_damping[s];
@@ -542,6 +543,7 @@ Plan plan_in(bg_ctx* c, const bg_bodies* B, const bg_rows* R, size_t b, size_t r
   s.tumbled = P.in<double>(B ? B->tumbled : nullptr, 3 * b, "tumbled");
   s.ceiling = P.in<double>(B ? B->ceiling : nullptr, b, "ceiling");
   s.start = P.in<double>(B ? B->start : nullptr, 3 * b, "start");
+  s.start_q = P.in<double>(B ? B->start_q : nullptr, 4 * b, "start_q");
   s.inv_mass = P.in<double>(B ? B->inv_mass : nullptr, b, "inv_mass");
   s.inertia = P.in<double>(B ? B->inertia : nullptr, 3 * b, "inertia");
   s.inv_inertia = P.in<double>(B ? B->inv_inertia : nullptr, 3 * b, "inv_inertia");
@@ -723,22 +725,71 @@ int validate(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
   return BG_OK;
 }
 
-int validate_world(bg_ctx* c, int nbodies, int nrows, const int32_t* starts, int solved) {
-  if (starts[0] != 0) {
-    set_error(c, "rows.starts[0] must be 0");
-    return BG_EINVAL;
-  }
+// What is wrong with a world's colour starts (src/contact.js:161, src/graph.js:178-214), or NULL:
+// they begin at 0, never decrease, the resting run begins at `solved`, and none passes `nrows`.
+const char* starts_problem(int nrows, const int32_t* starts, int solved) {
+  if (starts[0] != 0) return "rows.starts[0] must be 0";
   for (int k = 0; k < bg::NSTARTS - 1; k++)
-    if (starts[k + 1] < starts[k]) {
-      set_error(c, "rows.starts must not decrease");
-      return BG_EINVAL;
-    }
-  if (starts[bg::RESTING_RUN] != solved || solved > nrows || starts[bg::NSTARTS - 1] > nrows) {
-    set_error(c, "rows.solved must equal starts[33] and be at most count");
+    if (starts[k + 1] < starts[k]) return "rows.starts must not decrease";
+  if (starts[bg::RESTING_RUN] != solved || solved > nrows || starts[bg::NSTARTS - 1] > nrows)
+    return "rows.solved must equal starts[33] and be at most count";
+  return nullptr;
+}
+
+int validate_world(bg_ctx* c, int nbodies, int nrows, const int32_t* starts, int solved) {
+  const char* why = starts_problem(nrows, starts, solved);
+  if (why != nullptr) {
+    set_error(c, "%s", why);
     return BG_EINVAL;
   }
   (void)nbodies;
   return BG_OK;
+}
+
+// Every index the caller hands over for worlds [w0, w1), checked before any of them addresses
+// memory (host tables or device records): each row's a and b among its world's slots, its point
+// count 1..P, row[] a permutation of the world's rows (the found order, src/graph.js:205-214), and
+// each awake entry among the world's slots.  `seen` has one byte per row of the whole upload,
+// zero over these worlds' rows.  Returns NULL, or what is wrong (with the row or entry in `why`).
+const char* index_problem(const bg_bodies* B, const bg_rows* R, const std::vector<bg::WorldDesc>& worlds, size_t w0,
+                          size_t w1, uint8_t* seen, char* why, size_t why_len) {
+  if (R->count > 0 && (R->a == nullptr || R->b == nullptr || R->points == nullptr || R->row == nullptr))
+    return "rows.a, rows.b, rows.points and rows.row must be given";
+  if (B->awake_count > 0 && B->awake_list == nullptr) return "bodies.awake_list must be given";
+  for (size_t wi = w0; wi < w1; wi++) {
+    const bg::WorldDesc& w = worlds[wi];
+    const int32_t* a = R->a + w.row0;
+    const int32_t* b = R->b + w.row0;
+    const uint8_t* pts = R->points + w.row0;
+    for (int m = 0; m < w.nrows; m++) {
+      if (static_cast<uint32_t>(a[m]) >= static_cast<uint32_t>(w.nbodies) ||
+          static_cast<uint32_t>(b[m]) >= static_cast<uint32_t>(w.nbodies)) {
+        snprintf(why, why_len, "rows.a / rows.b of row %d (world %zu) is not one of its %d slots", m, wi, w.nbodies);
+        return why;
+      }
+      if (pts[m] < 1 || pts[m] > bg::P) {
+        snprintf(why, why_len, "rows.points of row %d (world %zu) is %d, not 1..%d", m, wi, pts[m], bg::P);
+        return why;
+      }
+    }
+    const int32_t* row = R->row + w.row0;
+    uint8_t* mark = seen + w.row0;
+    for (int f = 0; f < w.nrows; f++) {
+      const int32_t x = row[f];
+      if (static_cast<uint32_t>(x) >= static_cast<uint32_t>(w.nrows) || mark[x] != 0) {
+        snprintf(why, why_len, "rows.row is not a permutation of the rows (entry %d of world %zu)", f, wi);
+        return why;
+      }
+      mark[x] = 1;
+    }
+    const int32_t* awake = B->awake_list + w.awake0;
+    for (int i = 0; i < w.nawake; i++)
+      if (static_cast<uint32_t>(awake[i]) >= static_cast<uint32_t>(w.nbodies)) {
+        snprintf(why, why_len, "bodies.awake_list entry %d (world %zu) is not one of its %d slots", i, wi, w.nbodies);
+        return why;
+      }
+  }
+  return nullptr;
 }
 
 // Copies the caller's columns for `nb` slots / `nr` rows / `na` awake entries to the device.  A
@@ -790,7 +841,22 @@ int upload_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R, int nb, int 
 // colour's rows share no body the solve moves, so their order changes no result, src/graph.js:1-33),
 // which keeps a warp's 32 rows on one code path.  The overflow and resting runs keep their order
 // (the overflow is solved in row order, src/contact.js:1794-1795).
-int order_rows(bg_ctx* c, const uint8_t* points, const int32_t* a, const int32_t* b, const double* inv_mass) {
+// Every caller index is checked first (index_problem), so nothing here or on the device reads
+// through a bad one; a refusal comes back in `err`, since this runs beside the caller's thread.
+int order_rows(bg_ctx* c, const bg_bodies* B, const bg_rows* R, std::string& err) {
+  {
+    std::vector<uint8_t> seen(static_cast<size_t>(c->nrows), 0);
+    char why[256];
+    const char* bad = index_problem(B, R, c->worlds, 0, c->worlds.size(), seen.data(), why, sizeof why);
+    if (bad != nullptr) {
+      err = bad;
+      return BG_EINVAL;
+    }
+  }
+  const uint8_t* points = R->points;
+  const int32_t* a = R->a;
+  const int32_t* b = R->b;
+  const double* inv_mass = B->inv_mass;
   const int n = c->nrows;
   c->perm.resize(static_cast<size_t>(n));
   c->iperm.resize(static_cast<size_t>(n));
@@ -913,11 +979,27 @@ int upload_and_order(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
     return BG_EINVAL;
   }
   int order_rc = BG_OK;
-  std::thread orderer([&] { order_rc = order_rows(c, R->points, R->a, R->b, B->inv_mass); });
+  std::string order_err;
+  std::thread orderer([&] {
+    try {
+      order_rc = order_rows(c, B, R, order_err);
+    } catch (const std::exception&) {
+      order_rc = BG_ENOMEM;
+      order_err = "upload: out of host memory";
+    }
+  });
   const int rc = upload_columns(c, B, R, c->nbodies, c->nrows, c->nawake);
   orderer.join();
+  if (order_rc != BG_OK) {
+    // A refused index: no kernel has run on this input.  The copies already issued only read the
+    // caller's columns; they finish before the call returns, and the context is left with nothing
+    // uploaded (the caller's arrays are untouched).
+    cudaStreamSynchronize(c->stream);
+    c->in_pending = false;
+    set_error(c, "%s", order_err.c_str());
+    return order_rc;
+  }
   if (rc != BG_OK) return rc;
-  if (order_rc != BG_OK) return order_rc;
   return send_order(c);
 }
 
@@ -1175,6 +1257,7 @@ int32_t bg_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
   rc = validate_world(c, B->capacity, R->count, R->starts, R->solved);
   if (rc != BG_OK) return rc;
   c->last_launches = 0;
+  c->uploaded = false;   // until this upload has passed every check
   if (!ensure(c, B->capacity, R->count, B->awake_count, 1)) return BG_ENOMEM;
   c->nbodies = B->capacity;
   c->nrows = R->count;
@@ -1287,6 +1370,7 @@ int32_t bg_batch_upload(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const b
   if (rc != BG_OK) return rc;
   const int nw = W->count;
   c->last_launches = 0;
+  c->uploaded = false;   // until this upload has passed every check
   if (!ensure(c, B->capacity, R->count, B->awake_count, nw)) return BG_ENOMEM;
   c->nbodies = B->capacity;
   c->nrows = R->count;
@@ -1495,6 +1579,30 @@ int batch_in_groups(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_wo
     set_error(c, "step: dt must be positive and substeps at least 1");
     return BG_EINVAL;
   }
+  {
+    // Every world's indices before any group runs, so that a refused batch writes nothing: the
+    // pool checks runs of whole worlds (their rows, hence their marks, never overlap).
+    std::vector<uint8_t> seen(static_cast<size_t>(R->count), 0);
+    HostPool* pool = pool_of(c);
+    const int tasks = std::max(1, std::min(static_cast<int>(worlds.size()), 4 * pool->size()));
+    std::vector<std::array<char, 256>> why(static_cast<size_t>(tasks));
+    std::vector<int> bad(static_cast<size_t>(tasks), 0);
+    pool->run(tasks, [&](int t) {
+      const size_t n = worlds.size(), lo = n * static_cast<size_t>(t) / static_cast<size_t>(tasks),
+                   hi = n * static_cast<size_t>(t + 1) / static_cast<size_t>(tasks);
+      char* out = why[static_cast<size_t>(t)].data();
+      const char* p = index_problem(B, R, worlds, lo, hi, seen.data(), out, 256);
+      if (p != nullptr) {
+        if (p != out) snprintf(out, 256, "%s", p);
+        bad[static_cast<size_t>(t)] = 1;
+      }
+    });
+    for (int t = 0; t < tasks; t++)
+      if (bad[static_cast<size_t>(t)]) {
+        set_error(c, "%s", why[static_cast<size_t>(t)].data());
+        return BG_EINVAL;
+      }
+  }
   while (static_cast<int>(c->kids.size()) < groups) {
     bg_ctx* k = bg_create(c->device, c->flags);
     if (k == nullptr) {
@@ -1614,6 +1722,9 @@ constexpr size_t kStaticBytes =
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 
+// The status word's value when the kernel refused the caller's indices (1 is a wait past its budget).
+constexpr int32_t kStaticRefused = 2;
+
 // The scratch array's device address, per device: set up by the first call on that device.
 void* g_static_addr[64] = {};
 std::mutex g_static_mutex;
@@ -1662,9 +1773,35 @@ __global__ void __launch_bounds__(kBlockThreads) stage_static(StaticIn in, unsig
   uint8_t* u = reinterpret_cast<uint8_t*>(q);
   R.points = u; u += cap;
   R.sliding = u; u += cap;
+  // The caller's indices first, before anything is written (they are in device memory, which the
+  // host side cannot read): each row's a and b among the slots, its point count 1..P, row[] a
+  // permutation of the rows (no entry out of range, none twice), each awake entry among the slots.
+  __shared__ uint32_t seen[kStaticRows / 32];
+  __shared__ int refused;
+  if (threadIdx.x == 0) refused = 0;
+  for (int i = threadIdx.x; i < kStaticRows / 32; i += blockDim.x) seen[i] = 0;
+  __syncthreads();
+  for (int m = threadIdx.x; m < nr; m += blockDim.x) {
+    const int32_t a = Ri.a[m], b = Ri.b[m], x = Ri.row[m];
+    const int pc = Ri.points[m];
+    bool bad = static_cast<uint32_t>(a) >= static_cast<uint32_t>(nb) || static_cast<uint32_t>(b) >= static_cast<uint32_t>(nb) ||
+               pc < 1 || pc > bg::P || static_cast<uint32_t>(x) >= static_cast<uint32_t>(nr);
+    if (!bad) {
+      const uint32_t bit = 1u << (x & 31);
+      if (atomicOr(&seen[x >> 5], bit) & bit) bad = true;
+    }
+    if (bad) atomicExch(&refused, 1);
+  }
+  for (int i = threadIdx.x; i < na; i += blockDim.x)
+    if (static_cast<uint32_t>(Bi.awake_list[i]) >= static_cast<uint32_t>(nb)) atomicExch(&refused, 1);
+  __syncthreads();
+  if (refused) {
+    if (threadIdx.x == 0) *status = kStaticRefused;
+    return;
+  }
   if (threadIdx.x == 0) *status = 0;
   // The caller's layout in: what every call must set afresh, since the array keeps the last
-  // call's contents.
+  // call's contents (the records' pad entries included, as unpack_bodies leaves them).
   for (int s = threadIdx.x; s < nb; s += blockDim.x) {
     for (int k = 0; k < 3; k++) {
       B.vw[8 * s + k] = Bi.velocity[3 * s + k];
@@ -1676,13 +1813,17 @@ __global__ void __launch_bounds__(kBlockThreads) stage_static(StaticIn in, unsig
       B.pr[12 * s + 3 + k] = Bi.inv_inertia[3 * s + k];
       B.pr[12 * s + 6 + k] = Bi.dims[3 * s + k];
     }
-    for (int k = 0; k < 4; k++) { B.pq[8 * s + 4 + k] = Bi.rotation[4 * s + k]; B.sq[4 * s + k] = 0; }
+    B.vw[8 * s + 6] = 0; B.vw[8 * s + 7] = 0;
+    B.pq[8 * s + 3] = 0;
+    B.st[4 * s + 3] = 0;
+    for (int k = 0; k < 4; k++) { B.pq[8 * s + 4 + k] = Bi.rotation[4 * s + k]; B.sq[4 * s + k] = Bi.start_q[4 * s + k]; }
     B.tc[4 * s + 3] = Bi.ceiling[s];
     B.pr[12 * s + 9] = Bi.damping[s];
     B.pr[12 * s + 10] = Bi.angular_damping[s];
     B.pr[12 * s + 11] = Bi.gravity_scale[s];
     B.mi[8 * s] = Bi.inv_mass[s];
     for (int k = 0; k < 6; k++) B.mi[8 * s + 1 + k] = Bi.inv_i[6 * s + k];
+    B.mi[8 * s + 7] = 0;
     uint32_t f = static_cast<uint32_t>(Bi.type[s]) & bg::F_TYPE;
     f |= (static_cast<uint32_t>(Bi.shape[s]) & 3u) << bg::F_SHAPE_SHIFT;
     if (Bi.frozen[s]) f |= bg::F_FROZEN;
@@ -1780,14 +1921,37 @@ __global__ void __launch_bounds__(kBlockThreads) stage_static(StaticIn in, unsig
   }
 }
 
+// Whether every column the static stage reads or writes is given (anchor_a / anchor_b may be NULL).
+bool static_columns_given(const bg_bodies* B, const bg_rows* R) {
+  const bool bodies = B->capacity == 0 ||
+      (B->awake != nullptr && B->position != nullptr && B->rotation != nullptr && B->velocity != nullptr &&
+       B->angular != nullptr && B->tumbled != nullptr && B->ceiling != nullptr && B->start != nullptr &&
+       B->start_q != nullptr && B->inv_i != nullptr && B->inv_mass != nullptr && B->inertia != nullptr &&
+       B->inv_inertia != nullptr && B->dims != nullptr && B->damping != nullptr && B->angular_damping != nullptr &&
+       B->gravity_scale != nullptr && B->type != nullptr && B->shape != nullptr && B->frozen != nullptr &&
+       B->framed != nullptr && B->lock != nullptr && B->joint_head != nullptr);
+  const bool awake = B->awake_count == 0 || B->awake_list != nullptr;
+  const bool rows = R->count == 0 ||
+      (R->row != nullptr && R->a != nullptr && R->b != nullptr && R->points != nullptr && R->normal != nullptr &&
+       R->t1 != nullptr && R->t2 != nullptr && R->friction != nullptr && R->restitution != nullptr &&
+       R->tolerance != nullptr && R->patch != nullptr && R->separation != nullptr && R->point != nullptr &&
+       R->shift != nullptr && R->normal_impulse != nullptr && R->tangent_impulse1 != nullptr &&
+       R->tangent_impulse2 != nullptr && R->roll_impulse1 != nullptr && R->roll_impulse2 != nullptr &&
+       R->spin_impulse != nullptr && R->drift1 != nullptr && R->drift2 != nullptr && R->gap != nullptr &&
+       R->max_normal_impulse != nullptr && R->relative_velocity != nullptr && R->sliding != nullptr);
+  return bodies && awake && rows;
+}
+
 }  // namespace
 
 extern "C" int32_t bg_solve_step_static(const bg_bodies* bodies, const bg_rows* rows, const bg_step* step, void* stream) {
   if (bodies == nullptr || rows == nullptr || step == nullptr) return BG_EINVAL;
+  // The same checks bg_solve_step makes of the counts and colour starts; the index columns are
+  // device memory, so the kernel checks those before it writes anything.
   if (bodies->capacity < 0 || bodies->capacity > BG_STATIC_MAX_BODIES || bodies->awake_count < 0 ||
       bodies->awake_count > bodies->capacity || rows->count < 0 || rows->count > BG_STATIC_MAX_ROWS ||
-      rows->solved < 0 || rows->solved > rows->count || rows->starts[bg::RESTING_RUN] != rows->solved ||
-      !(step->dt > 0) || step->substeps < 1)
+      rows->solved < 0 || starts_problem(rows->count, rows->starts, rows->solved) != nullptr ||
+      !static_columns_given(bodies, rows) || !(step->dt > 0) || step->substeps < 1)
     return BG_EINVAL;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return BG_ECUDA;
@@ -1811,5 +1975,5 @@ extern "C" int32_t bg_solve_step_static(const bg_bodies* bodies, const bg_rows* 
   int32_t status = 0;
   if (cudaMemcpyAsync(&status, base, sizeof status, cudaMemcpyDeviceToHost, s) != cudaSuccess) return BG_ECUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return BG_ECUDA;
-  return status == 0 ? BG_OK : BG_ETIMEOUT;
+  return status == 0 ? BG_OK : status == kStaticRefused ? BG_EINVAL : BG_ETIMEOUT;
 }

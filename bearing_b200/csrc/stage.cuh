@@ -1179,6 +1179,14 @@ __device__ __forceinline__ void solve_biased(const StageParams& p, int m, double
   else solve_row<true, false>(p, m, h, gate);
 }
 
+// Whether any of six doubles differs in its bits from what is stored at q.
+__device__ __forceinline__ bool changed6(const double* v, const double* q) {
+  bool any = false;
+  for (int c = 0; c < 6; c++)
+    any |= __double_as_longlong(v[c]) != __double_as_longlong(ldm(q + c));
+  return any;
+}
+
 // Whether row m has a point restitution() works on: src/contact.js:2233-2241.  What it reads
 // (relativeVelocity, maxNormalImpulse) restitution() never changes, so this holds throughout.
 __device__ __forceinline__ bool bouncy(const StageParams& p, int m, int solved_end, double gravity) {
@@ -1195,9 +1203,17 @@ __device__ __forceinline__ bool bouncy(const StageParams& p, int m, int solved_e
   return false;
 }
 
-// restitution for row m: src/contact.js:2234-2250 (closing 2216-2220, push 1743-1749).  A body
-// with inverse mass 0 gains nothing from push(); its velocities are left unwritten.
-__device__ void bounce_row(const StageParams& p, int m, double gravity) {
+// restitution for row m: src/contact.js:2234-2250 (closing 2216-2220, push 1743-1749).
+//
+// push() also writes a body with inverse mass 0 (a static or kinematic one): v -= 0 * px, which
+// leaves its bits alone unless px is not finite (0 * inf is NaN) or a -0 component meets a -0
+// product.  Rows of one round share such bodies, so the rounds (EXACT false) leave them unwritten
+// and instead raise *redo where push() would have changed one: restitution_stage then redoes the
+// world's restitution one row at a time in found order (EXACT true), writing every body as push()
+// does.  Until a push would change such a body, both ways give the same bits (each dynamic body
+// sees its pushes in found order either way).
+template <bool EXACT>
+__device__ void bounce_row(const StageParams& p, int m, double gravity, int* redo) {
   const RowsDev& R = p.R;
   const BodiesDev& B = p.B;
   const int64_t cap = R.cap;
@@ -1229,8 +1245,15 @@ __device__ void bounce_row(const StageParams& p, int m, double gravity) {
     va[3] -= ldm(jac + 6 * cap) * d; va[4] -= ldm(jac + 7 * cap) * d; va[5] -= ldm(jac + 8 * cap) * d;
     vb[3] += ldm(jac + 9 * cap) * d; vb[4] += ldm(jac + 10 * cap) * d; vb[5] += ldm(jac + 11 * cap) * d;
   }
+  if (EXACT) {
+    for (int c = 0; c < 6; c++) stm(pa + c, va[c]);
+    for (int c = 0; c < 6; c++) stm(pb + c, vb[c]);
+    return;
+  }
   if (ima != 0) for (int c = 0; c < 6; c++) stm(pa + c, va[c]);
+  else if (changed6(va, pa)) *redo = 1;
   if (imb != 0) for (int c = 0; c < 6; c++) stm(pb + c, vb[c]);
+  else if (changed6(vb, pb)) *redo = 1;
 }
 
 // turned: src/contact.js:1168-1182.
@@ -1359,10 +1382,26 @@ __device__ bool restitution_stage(const StageParams& p, const WorldDesc& w, cons
       for (int k = 0; k < nblocks; k++) total += Team::kGrid ? ldm(counts + k) : counts[k];
       s_total = total;
     }
+    __shared__ int s_redo;
+    if (threadIdx.x == 0) s_redo = 0;
     __syncthreads();
     int n = s_total;
     int32_t* list = R.active + w.row0;
     int32_t* next = R.pending + w.row0;
+    // What a redo starts from: each listed row's two bodies' velocities and its normal impulses as
+    // restitution begins, kept in the row's la and now columns (read only by the substeps' passes,
+    // which are over).
+    const int64_t cap = R.cap;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int m = ldm(list + i);
+      const int a = ldi(R.a + m), b = ldi(R.b + m);
+      for (int c = 0; c < 6; c++) {
+        stm(R.la + c * cap + m, ldm(B.vw + 8 * a + c));
+        stm(R.la + (6 + c) * cap + m, ldm(B.vw + 8 * b + c));
+      }
+      for (int k = 0; k < P; k++) stm(R.now + k * cap + m, ldm(R.ni + k * cap + m));
+    }
+    __syncthreads();
     int guard = 0;
     while (n > 0 && guard++ < nrows + 1) {
       // every pending row bids for its dynamic bodies with its place in the list
@@ -1379,7 +1418,7 @@ __device__ bool restitution_stage(const StageParams& p, const WorldDesc& w, cons
         const int a = ldi(R.a + m), b = ldi(R.b + m);
         const bool ra = ldm(B.mi + 8 * a) == 0 || ldm(B.head + a) == i;
         const bool rb = ldm(B.mi + 8 * b) == 0 || ldm(B.head + b) == i;
-        if (ra && rb) bounce_row(p, m, gravity);
+        if (ra && rb) bounce_row<false>(p, m, gravity, &s_redo);
       }
       __syncthreads();
       // the rows not taken, in order, become the next list; the bids are cleared
@@ -1422,6 +1461,25 @@ __device__ bool restitution_stage(const StageParams& p, const WorldDesc& w, cons
       next = tmp;
       __syncthreads();
     }
+    // A push would have changed a body of inverse mass 0: back to the snapshot, then the
+    // reference's own order, one row after another, on one thread.
+    if (s_redo && threadIdx.x == 0) {
+      for (int f = 0; f < nrows; f++) {
+        const int m = ldi(R.row + w.row0 + f);
+        if (!bouncy(p, m, solved_end, gravity)) continue;
+        const int a = ldi(R.a + m), b = ldi(R.b + m);
+        for (int c = 0; c < 6; c++) {
+          stm(B.vw + 8 * a + c, ldm(R.la + c * cap + m));
+          stm(B.vw + 8 * b + c, ldm(R.la + (6 + c) * cap + m));
+        }
+        for (int k = 0; k < P; k++) stm(R.ni + k * cap + m, ldm(R.now + k * cap + m));
+      }
+      for (int f = 0; f < nrows; f++) {
+        const int m = ldi(R.row + w.row0 + f);
+        if (bouncy(p, m, solved_end, gravity)) bounce_row<true>(p, m, gravity, nullptr);
+      }
+    }
+    __syncthreads();
   }
   return t.sync(p);
 }

@@ -1,7 +1,8 @@
 // Node N-API addon: Bearing's World calls the B200 solve stage through libbearing_gpu.so.
 //
 // Not built in this repository: node_api.h is not available here.  A maintainer builds it with
-// node-gyp against include/bearing_gpu.h and links libbearing_gpu.so.  Every
+// node-gyp against include/bearing_gpu.h and links libbearing_gpu.so, with a binding.gyp whose
+// one target lists this file, the include directory and the library's directory.  Every
 // array handed over is one of World's or Contacts' own typed arrays (src/world.js:228-311,
 // src/contact.js:184-248), passed by pointer with no copy.
 #include <node_api.h>

@@ -195,13 +195,31 @@ class World:
         return {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
 
     def state(self) -> dict:
-        """FP64 body state by slot (position, rotation, velocity, angular), copies."""
+        """Every FP64 body column the solve stage writes, by slot (copies): position, rotation,
+        velocity, angular, the tumble state (tumbled, ceiling), the step's start pose (start,
+        start_q) and the world inverse inertia (inv_i)."""
         B, _, _ = self.views()
         n = self._count
         def arr(p, k):
             return np.ctypeslib.as_array(p, shape=(k * n,)).copy() if n else np.zeros(0)
         return {"position": arr(B.position, 3), "rotation": arr(B.rotation, 4),
-                "velocity": arr(B.velocity, 3), "angular": arr(B.angular, 3)}
+                "velocity": arr(B.velocity, 3), "angular": arr(B.angular, 3),
+                "tumbled": arr(B.tumbled, 3), "ceiling": arr(B.ceiling, 1), "start": arr(B.start, 3),
+                "start_q": arr(B.start_q, 4), "inv_i": arr(B.inv_i, 6)}
+
+    def contacts(self) -> dict:
+        """The last step's manifolds as the solve stage left them (copies, in colour order): the
+        impulses, drift, gaps, max impulses and relative velocities."""
+        _, R, _ = self.views()
+        n = R.count
+        def arr(p, k):
+            return np.ctypeslib.as_array(p, shape=(k * n,)).copy() if n else np.zeros(0)
+        return {"normal_impulse": arr(R.normal_impulse, 4), "tangent_impulse1": arr(R.tangent_impulse1, 1),
+                "tangent_impulse2": arr(R.tangent_impulse2, 1), "roll_impulse1": arr(R.roll_impulse1, 1),
+                "roll_impulse2": arr(R.roll_impulse2, 1), "spin_impulse": arr(R.spin_impulse, 1),
+                "drift1": arr(R.drift1, 1), "drift2": arr(R.drift2, 1), "gap": arr(R.gap, 1),
+                "max_normal_impulse": arr(R.max_normal_impulse, 4),
+                "relative_velocity": arr(R.relative_velocity, 4)}
 
     def destroy(self):
         if self._w:

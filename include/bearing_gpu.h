@@ -27,8 +27,12 @@
  * operation order, so results are bit-identical to the reference's CPU solve over the same rows.
  *
  * Return codes: BG_OK (0) or a negative BG_E* code; bg_last_error() says why.  A failed
- * validation changes no state.  A device wait that runs past its budget returns BG_ETIMEOUT,
- * which the caller treats as src/core/jobs.js:384-391 treats a lost step: fall back to the CPU.
+ * validation (BG_EINVAL) writes none of the caller's arrays and runs no kernel: the counts, the
+ * colour starts and every index the caller passes are checked first (each row's a and b among
+ * its world's slots, points 1..BG_POINTS, row[] a permutation of the world's rows, each awake
+ * entry among the world's slots); a refused upload leaves the context with nothing uploaded.
+ * A device wait that runs past its budget returns BG_ETIMEOUT, which the caller treats as
+ * src/core/jobs.js:384-391 treats a lost step: fall back to the CPU.
  */
 #ifndef BEARING_GPU_H
 #define BEARING_GPU_H
@@ -252,11 +256,16 @@ int32_t bg_set_batch_groups(bg_ctx* ctx, int32_t groups);
  * GPU that loads the library holds until the process exits; so a world may have at most
  * BG_STATIC_MAX_BODIES slots and BG_STATIC_MAX_ROWS rows, and larger ones are refused with
  * BG_EINVAL (use bg_solve_step for those).  The first call on a device looks up that array's
- * device address with the device current; make that first call before any stream capture.  All
- * calls share the one array: calls that overlap on the GPU (other streams, other host threads)
- * race, so run them one after another.  It calls no cudaMalloc or cudaFree.
- * Returns BG_OK, BG_EINVAL, BG_ECUDA, or BG_ETIMEOUT as bg_solve_step does; there is no context,
- * so no bg_last_error text.
+ * device address with the device current, in the device's primary context (the CUDA runtime's
+ * own), and keeps it for later calls on that device; make that first call before any stream
+ * capture, and do not call this again on a device after cudaDeviceReset.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other host threads) race, so run them one
+ * after another.  Each call waits for `stream` to finish its work before it returns.  It calls no
+ * cudaMalloc or cudaFree.
+ * The counts and colour starts are checked on the host as bg_solve_step checks them; the index
+ * columns (device memory) are checked by the kernel before it writes anything.  Either refusal
+ * returns BG_EINVAL and leaves the caller's arrays untouched.  Otherwise it returns BG_OK,
+ * BG_ECUDA, or BG_ETIMEOUT as bg_solve_step does; there is no context, so no bg_last_error text.
  */
 #define BG_STATIC_MAX_BODIES 512
 #define BG_STATIC_MAX_ROWS 2048

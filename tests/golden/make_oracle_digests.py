@@ -1,6 +1,6 @@
-"""Writes oracle_digests.json: per-step SHA-256 digests of the oracle's full FP64 body state for
-two of the reference's own test scenes, stepped through the host side of the step and the oracle's
-solve stage (tests/test_golden.py checks them).
+"""Writes oracle_digests.json: per-step SHA-256 digests of the oracle's full FP64 body state and
+contact columns for two of the reference's own test scenes, stepped through the host side of the
+step and the oracle's solve stage (tests/test_golden.py checks them).
 
 The reference stores no numeric vectors of its own (its tests check behaviour with tolerances),
 so these pin this repository's CPU restatement against unintended change, not against the
@@ -29,8 +29,9 @@ def digests(scene, steps, workers=0):
     out = []
     for _ in range(steps):
         w.step(1 / 60)
-        st = w.state()
-        out.append(hashlib.sha256(b"".join(st[k].tobytes() for k in sorted(st))).hexdigest())
+        st, ct = w.state(), w.contacts()
+        out.append(hashlib.sha256(b"".join(st[k].tobytes() for k in sorted(st))
+                                  + b"".join(ct[k].tobytes() for k in sorted(ct))).hexdigest())
     w.destroy()
     return out
 

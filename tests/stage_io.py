@@ -36,7 +36,7 @@ ROW_COLUMNS = [
     ("anchor_a", np.float64, 3), ("anchor_b", np.float64, 3),
 ]
 # What the solve stage writes.
-BODY_OUT = ["position", "rotation", "velocity", "angular", "tumbled", "ceiling", "start", "inv_i"]
+BODY_OUT = ["position", "rotation", "velocity", "angular", "tumbled", "ceiling", "start", "start_q", "inv_i"]
 ROW_OUT = ["normal_impulse", "tangent_impulse1", "tangent_impulse2", "roll_impulse1", "roll_impulse2",
            "spin_impulse", "drift1", "drift2", "gap", "max_normal_impulse", "relative_velocity"]
 # Written for solved rows only.
@@ -130,26 +130,37 @@ class StageCopy:
         return B, R, S
 
 
+def _first_unequal(x, y):
+    """Index of the first entry where x and y differ, or None.  Floats compare bit for bit, except
+    that a NaN matches any NaN: the CPU's and the GPU's default NaN payloads differ, and a NaN's
+    payload is not a result."""
+    if x.dtype == np.float64:
+        nx, ny = np.isnan(x), np.isnan(y)
+        unequal = (x.view(np.uint64) != y.view(np.uint64)) & ~(nx & ny)
+    else:
+        unequal = x != y
+    hit = np.flatnonzero(unequal)
+    return int(hit[0]) if hit.size else None
+
+
 def first_difference(a: StageCopy, b: StageCopy):
-    """None if every column the solve stage writes is bit-identical; else a description."""
+    """None if every column the solve stage writes is bit-identical (NaN matching NaN); else a
+    description of the first difference."""
     for f in BODY_OUT:
-        x, y = a.body[f], b.body[f]
-        if x.tobytes() != y.tobytes():
-            i = int(np.flatnonzero(x.view(np.uint64) != y.view(np.uint64))[0])
-            return f"body {f}[{i}]: {x[i]!r} vs {y[i]!r}"
+        i = _first_unequal(a.body[f], b.body[f])
+        if i is not None:
+            return f"body {f}[{i}]: {a.body[f][i]!r} vs {b.body[f][i]!r}"
     per = dict((f, p) for f, _, p in ROW_COLUMNS)
     for f in ROW_OUT:
-        x, y = a.rows[f], b.rows[f]
-        if x.tobytes() != y.tobytes():
-            i = int(np.flatnonzero(x.view(np.uint64) != y.view(np.uint64))[0])
-            return f"row {f}[{i}] (row {i // per[f]}): {x[i]!r} vs {y[i]!r}"
+        i = _first_unequal(a.rows[f], b.rows[f])
+        if i is not None:
+            return f"row {f}[{i}] (row {i // per[f]}): {a.rows[f][i]!r} vs {b.rows[f][i]!r}"
     n = a.solved
     for f in ROW_OUT_SOLVED:
         k = per[f]
         x, y = a.rows[f][: k * n], b.rows[f][: k * n]
-        if x.tobytes() != y.tobytes():
-            i = int(np.flatnonzero(x.view(np.uint8 if x.dtype == np.uint8 else np.uint64)
-                                   != y.view(np.uint8 if y.dtype == np.uint8 else np.uint64))[0])
+        i = _first_unequal(x, y)
+        if i is not None:
             return f"row {f}[{i}] (row {i // k}): {x[i]!r} vs {y[i]!r}"
     return None
 

@@ -112,3 +112,41 @@ def test_mass_and_inertia_follow_the_shape():
     assert [B.inertia[3 * box + k] for k in range(3)] == [m * (4 + 9) / 12, m * (1 + 9) / 12, m * (1 + 4) / 12]
     assert B.dims[3 * cap] == 0.25 and B.dims[3 * cap + 1] == 1.5
     w.destroy()
+
+
+def test_static_entry_point_refuses_bad_counts_and_starts_before_touching_a_device():
+    # bg_solve_step_static checks the counts and the colour starts on the host, as bg_solve_step
+    # does, and returns before any CUDA call: these run without a GPU.
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_io
+    from bearing_b200 import scenes
+    from stage_io import StageCopy
+    w = World({}, solver=oracle_io.solver(0))
+    scenes.pyramid(w, rows=6)
+    for _ in range(3):
+        w.step(1 / 60)
+    w.begin_step(1 / 60)
+    base = StageCopy(w)
+    g = _ffi.gpu()
+    for bad in ("starts[0]", "decreasing", "past count", "solved", "bodies", "rows", "dt", "null column"):
+        work = base.copy()
+        B, R, S = work.views()
+        if bad == "starts[0]":
+            R.starts[0] = 1
+        elif bad == "decreasing":
+            R.starts[1] = R.starts[2] + 1
+        elif bad == "past count":
+            R.starts[34] = R.count + 5000
+        elif bad == "solved":
+            R.solved = R.starts[33] + 1
+        elif bad == "bodies":
+            B.capacity = _ffi.BG_STATIC_MAX_BODIES + 1
+        elif bad == "rows":
+            R.count = _ffi.BG_STATIC_MAX_ROWS + 1
+        elif bad == "dt":
+            S.dt = 0.0
+        else:
+            R.normal = None
+        assert g.bg_solve_step_static(C.byref(B), C.byref(R), C.byref(S), None) == _ffi.BG_EINVAL, bad
+    w.destroy()

@@ -1,6 +1,7 @@
 """The oracle against its committed digests (tests/golden/oracle_digests.json, made by
 tests/golden/make_oracle_digests.py): the pyramid and the 10-box stack, every step's FP64 body
-state, with the single-threaded solve and with worker threads (which must not change a bit)."""
+state and contact columns, with the single-threaded solve and with worker threads (which must not
+change a bit)."""
 import json
 import os
 import sys
@@ -35,8 +36,9 @@ def gpu_digests(scene, steps, flags):
     out = []
     for _ in range(steps):
         w.step(1 / 60)
-        st = w.state()
-        out.append(hashlib.sha256(b"".join(st[k].tobytes() for k in sorted(st))).hexdigest())
+        st, ct = w.state(), w.contacts()
+        out.append(hashlib.sha256(b"".join(st[k].tobytes() for k in sorted(st))
+                                  + b"".join(ct[k].tobytes() for k in sorted(ct))).hexdigest())
     w.destroy()
     return out
 

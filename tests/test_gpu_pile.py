@@ -1,7 +1,8 @@
 """The headline workload end to end: the 50,000-body mixed pile stepped 300 times by a World whose
 solve stage runs on the GPU, and by the same World on the oracle (every host thread), compared by
-a digest of the full FP64 body state every 50 steps (the pile lands, peaks at ~145k rows near step
-100 and settles to ~123k by step 300).  About two minutes on one B200 and its host."""
+a digest of every FP64 body column the stage writes and the step's contact columns every 50 steps
+(the pile lands, peaks at ~145k rows near step 100 and settles to ~123k by step 300).  About two
+minutes on one B200 and its host."""
 import hashlib
 import os
 
@@ -15,8 +16,10 @@ pytestmark = pytest.mark.gpu
 
 
 def digest(w):
-    st = w.state()
-    return hashlib.sha256(b"".join(st[k].tobytes() for k in sorted(st))).hexdigest()
+    """Every FP64 body column the stage writes, and the last step's contact columns."""
+    st, ct = w.state(), w.contacts()
+    return hashlib.sha256(b"".join(st[k].tobytes() for k in sorted(st))
+                          + b"".join(ct[k].tobytes() for k in sorted(ct))).hexdigest()
 
 
 def test_pile_of_50k_bodies_300_steps_bit_identical_to_the_oracle():
