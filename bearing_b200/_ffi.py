@@ -125,6 +125,21 @@ class Worlds(C.Structure):
     ]
 
 
+class RowMemory(C.Structure):
+    """bw_row_memory: per row, what narrow() used besides the row's columns."""
+
+    _fields_ = [
+        ("pid", C.POINTER(C.c_uint32)),
+        ("margin", _d),
+        ("remembered", _u8),
+        ("memory_pid", C.POINTER(C.c_uint32)),
+        ("memory", _d),
+    ]
+
+
+BW_MEMORY = 16
+
+
 class Options(C.Structure):
     _fields_ = [("gravity", C.c_double * 3), ("substeps", C.c_int32)]
 
@@ -204,9 +219,14 @@ def host() -> C.CDLL:
         lib.bw_batch_begin_step.argtypes = [C.c_void_p, C.c_double, C.c_int32]
         lib.bw_batch_views.argtypes = [C.c_void_p, C.POINTER(Bodies), C.POINTER(Rows), C.POINTER(Worlds), C.POINTER(Step)]
         lib.bw_batch_end_step.argtypes = [C.c_void_p, C.c_int32]
+        lib.bw_row_memory_get.argtypes = [C.c_void_p, C.POINTER(RowMemory)]
+        lib.bw_batch_row_memory.argtypes = [C.c_void_p, C.POINTER(RowMemory)]
+        lib.bw_clone.restype = C.c_void_p
+        lib.bw_clone.argtypes = [C.c_void_p]
+        lib.bw_copy.argtypes = [C.c_void_p, C.c_void_p]
         for f in ("bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step", "bw_end_step",
                   "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_stats_get", "bw_batch_begin_step",
-                  "bw_batch_views", "bw_batch_end_step"):
+                  "bw_batch_views", "bw_batch_end_step", "bw_row_memory_get", "bw_batch_row_memory", "bw_copy"):
             getattr(lib, f).restype = C.c_int32
         _host = lib
     return _host
@@ -270,4 +290,5 @@ HOST_SYMBOLS = [
     "bw_create", "bw_destroy", "bw_last_error", "bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step",
     "bw_end_step", "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_transforms", "bw_stats_get",
     "bw_batch_create", "bw_batch_destroy", "bw_batch_begin_step", "bw_batch_views", "bw_batch_end_step",
+    "bw_row_memory_get", "bw_batch_row_memory", "bw_clone", "bw_copy",
 ]

@@ -25,7 +25,7 @@ GPU_SOURCES = [os.path.join(PKG, "csrc", "bearing_gpu.cu")]
 GPU_DEPS = [os.path.join(PKG, "csrc", f) for f in ("layout.cuh", "stage.cuh")] + [
     os.path.join(ROOT, "include", "bearing_gpu.h")]
 HOST_SOURCES = [os.path.join(PKG, "host", "world.cpp"), os.path.join(PKG, "host", "collide.cpp")]
-HOST_DEPS = [os.path.join(PKG, "host", "collide.hpp"), os.path.join(ROOT, "include", "bearing_world.h"),
+HOST_DEPS = [os.path.join(PKG, "host", "collide.hpp"), os.path.join(PKG, "host", "collide_impl.hpp"), os.path.join(ROOT, "include", "bearing_world.h"),
              os.path.join(ROOT, "include", "bearing_gpu.h")]
 ORACLE_SOURCES = [os.path.join(ROOT, "oracle", "solve_stage.cpp")]
 
@@ -69,7 +69,9 @@ def build_host(force=False):
 
 def build_oracle(force=False):
     os.makedirs(os.path.dirname(ORACLE_LIB), exist_ok=True)
-    if force or _stale(ORACLE_LIB, ORACLE_SOURCES + [os.path.join(ROOT, "include", "bearing_gpu.h")]):
+    deps = [os.path.join(ROOT, "include", f) for f in ("bearing_gpu.h", "bearing_world.h")] + [
+        os.path.join(ROOT, "oracle", "dual.hpp"), os.path.join(PKG, "host", "collide_impl.hpp")]
+    if force or _stale(ORACLE_LIB, ORACLE_SOURCES + deps):
         _run([CXX] + CXX_FLAGS + ["-o", ORACLE_LIB] + ORACLE_SOURCES + ["-lpthread"])
     return ORACLE_LIB
 

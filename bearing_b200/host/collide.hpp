@@ -10,26 +10,31 @@ namespace bearing {
 // Shape kinds in dispatch order: src/collide.js:44 (a pair is handled lower kind first).
 enum Kind { K_SPHERE = 0, K_CAPSULE = 1, K_BOX = 2 };
 
-// One placed shape: src/collide.js:52-93.
-struct Shape {
+// One placed shape: src/collide.js:52-93.  T is the scalar (double for the step itself; see
+// collide_impl.hpp).
+template <class T>
+struct ShapeT {
   int kind = K_BOX;
-  double center[3] = {0, 0, 0};
-  double axes[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-  double half[3] = {0, 0, 0};
-  double weight[3] = {0, 0, 0};
+  T center[3] = {0, 0, 0};
+  T axes[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  T half[3] = {0, 0, 0};
+  T weight[3] = {0, 0, 0};
 };
+using Shape = ShapeT<double>;
 
 constexpr int MAX_POINTS = 4;
 
 // src/collide.js:181-197.
-struct Manifold {
+template <class T>
+struct ManifoldT {
   int count = 0;
-  double normal[3] = {0, 0, 0};
-  double points[3 * MAX_POINTS] = {};
-  double separations[MAX_POINTS] = {};
+  T normal[3] = {0, 0, 0};
+  T points[3 * MAX_POINTS] = {};
+  T separations[MAX_POINTS] = {};
   uint32_t ids[MAX_POINTS] = {};
-  double loss = 0;
+  T loss = 0;
 };
+using Manifold = ManifoldT<double>;
 
 // collide(a, b, margin, tolerance, out): src/collide.js:204-218.  Returns the point count.
 int collide(const Shape& a, const Shape& b, double margin, double tolerance, Manifold& out);

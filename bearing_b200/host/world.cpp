@@ -615,6 +615,25 @@ struct bw_world {
     }
   }
 
+  // Per row after begin_step: what narrow() used besides the row's columns (bw_row_memory).
+  void rowMemory(int m, uint32_t* pidOut, double* marginOut, uint8_t* rememberedOut, uint32_t* memPid,
+                 double* memory) const {
+    const int p = c.pair[m], a = c.a[m], b = c.b[m];
+    for (int k = 0; k < P; k++) pidOut[k] = k < c.points[m] ? c.pid[m * P + k] : 0;
+    *marginOut = motion[a] + motion[b] + c.tolerance[m];
+    *rememberedOut = pairs.points[p];
+    for (int k = 0; k < P; k++) {
+      memPid[k] = pairs.pid[p * P + k];
+      memory[k] = pairs.normalImpulse[p * P + k];
+    }
+    for (int k = 0; k < 3; k++) {
+      memory[4 + k] = pairs.friction[3 * p + k];
+      memory[7 + k] = pairs.twist[3 * p + k];
+      memory[10 + k] = pairs.slip[3 * p + k];
+    }
+    memory[13] = memory[14] = memory[15] = 0;
+  }
+
   void fillBodies(bg_bodies* B) {
     B->capacity = n;
     B->awake_count = awakeCount;
@@ -828,6 +847,38 @@ int32_t bw_end_step(bw_world* w) {
   st.overflow = c.count > 0 ? c.starts[OVERFLOW_ + 1] - c.starts[OVERFLOW_] : 0;
   st.step = w->stepCount;
   w->stepDt = 0;
+  return BG_OK;
+}
+
+int32_t bw_row_memory_get(const bw_world* w, bw_row_memory* out) {
+  if (w == nullptr || out == nullptr || !w->begun) return BG_EINVAL;
+  const int n = w->c.count;
+  if (n > 0 && (out->pid == nullptr || out->margin == nullptr || out->remembered == nullptr ||
+                out->memory_pid == nullptr || out->memory == nullptr))
+    return BG_EINVAL;
+  for (int m = 0; m < n; m++)
+    w->rowMemory(m, out->pid + P * m, out->margin + m, out->remembered + m, out->memory_pid + P * m,
+                 out->memory + BW_MEMORY * m);
+  return BG_OK;
+}
+
+bw_world* bw_clone(const bw_world* w) {
+  if (w == nullptr) return nullptr;
+  try {
+    return new bw_world(*w);
+  } catch (const std::exception&) {
+    return nullptr;
+  }
+}
+
+int32_t bw_copy(bw_world* dst, const bw_world* src) {
+  if (dst == nullptr || src == nullptr) return BG_EINVAL;
+  if (dst == src) return BG_OK;
+  try {
+    *dst = *src;
+  } catch (const std::exception&) {
+    return BG_ENOMEM;
+  }
   return BG_OK;
 }
 
@@ -1061,6 +1112,19 @@ int32_t bw_batch_views(bw_batch* b, bg_bodies* B, bg_rows* R, bg_worlds* W, bg_s
   W->gravity = nullptr;
   bw_step_params(b->worlds[0], S);
   S->dt = b->dt;
+  return BG_OK;
+}
+
+int32_t bw_batch_row_memory(const bw_batch* b, bw_row_memory* out) {
+  if (b == nullptr || !b->begun || out == nullptr) return BG_EINVAL;
+  const size_t n = b->worlds.size();
+  for (size_t i = 0; i < n; i++) {
+    const size_t r = static_cast<size_t>(b->row_off[i]);
+    bw_row_memory part = {out->pid + P * r, out->margin + r, out->remembered + r, out->memory_pid + P * r,
+                          out->memory + BW_MEMORY * r};
+    const int32_t rc = bw_row_memory_get(b->worlds[i], &part);
+    if (rc != BG_OK) return rc;
+  }
   return BG_OK;
 }
 

@@ -105,6 +105,29 @@ int32_t bw_batch_begin_step(bw_batch* batch, double dt, int32_t threads);
 int32_t bw_batch_views(bw_batch* batch, bg_bodies* bodies, bg_rows* rows, bg_worlds* worlds, bg_step* step);
 int32_t bw_batch_end_step(bw_batch* batch, int32_t threads);
 
+/*
+ * What the host side of a step knows of each row beyond the solve stage's columns: for the
+ * adjoint's replay of the row's narrowphase, emit, basis and carry (src/contact.js:889-1036), and
+ * for the tests' checker, which recomputes them.  Filled after bw_begin_step, per row in the rows'
+ * (colour) order; the row's pair is rows.a / rows.b.
+ */
+typedef struct bw_row_memory {
+  uint32_t* pid;          /* 4 per row: each point's feature id (Contacts.pid) */
+  double* margin;         /* 1 per row: the narrowphase margin, motion[a] + motion[b] + tolerance */
+  uint8_t* remembered;    /* 1 per row: points the pair remembered from the last step (0: none carried) */
+  uint32_t* memory_pid;   /* 4 per row: those points' feature ids */
+  double* memory;         /* BW_MEMORY per row: normalImpulse[4], friction[3], twist[3], slip[3], 3 unused */
+} bw_row_memory;
+#define BW_MEMORY 16
+int32_t bw_row_memory_get(const bw_world* world, bw_row_memory* out);
+/* The same for a batch after bw_batch_begin_step, rows end to end as bw_batch_views lays them. */
+int32_t bw_batch_row_memory(const bw_batch* batch, bw_row_memory* out);
+
+/* A deep copy of a world (its bodies, pairs with their memory, broadphase and step count), for
+ * checkpoints; bw_destroy frees it.  NULL if out of memory.  bw_copy makes dst a copy of src. */
+bw_world* bw_clone(const bw_world* world);
+int32_t bw_copy(bw_world* dst, const bw_world* src);
+
 /* World.transforms: 7 floats per slot (position, rotation x y z w). */
 const float* bw_transforms(const bw_world* world);
 int32_t bw_stats_get(const bw_world* world, bw_stats* out);
