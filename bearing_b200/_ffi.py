@@ -125,6 +125,20 @@ class Worlds(C.Structure):
     ]
 
 
+class BodyGrads(C.Structure):
+    """bg_body_grads: adjoints of the body columns a step reads and writes."""
+
+    _fields_ = [(f, _d) for f in ("position", "rotation", "velocity", "angular", "tumbled", "ceiling")]
+
+
+class RowGrads(C.Structure):
+    """bg_row_grads: adjoints of the row columns a step reads and writes."""
+
+    _fields_ = [(f, _d) for f in ("normal_impulse", "tangent_impulse1", "tangent_impulse2", "roll_impulse1",
+                                  "roll_impulse2", "spin_impulse", "drift1", "drift2", "normal", "t1", "t2",
+                                  "friction", "restitution", "separation", "point")]
+
+
 class RowMemory(C.Structure):
     """bw_row_memory: per row, what narrow() used besides the row's columns."""
 
@@ -219,6 +233,10 @@ def host() -> C.CDLL:
         lib.bw_batch_begin_step.argtypes = [C.c_void_p, C.c_double, C.c_int32]
         lib.bw_batch_views.argtypes = [C.c_void_p, C.POINTER(Bodies), C.POINTER(Rows), C.POINTER(Worlds), C.POINTER(Step)]
         lib.bw_batch_end_step.argtypes = [C.c_void_p, C.c_int32]
+        lib.bw_materials.argtypes = [C.c_void_p, _d, _d]
+        lib.bw_keep_backward.argtypes = [C.POINTER(Rows), C.POINTER(Worlds), _d, C.POINTER(RowGrads)]
+        lib.bw_narrow_backward.argtypes = [C.POINTER(Bodies), C.POINTER(Rows), C.POINTER(Worlds), C.POINTER(RowMemory),
+                                           _d, _d, _d, C.POINTER(RowGrads), _d, _d, _d, _d, _d, C.c_int32]
         lib.bw_row_memory_get.argtypes = [C.c_void_p, C.POINTER(RowMemory)]
         lib.bw_batch_row_memory.argtypes = [C.c_void_p, C.POINTER(RowMemory)]
         lib.bw_clone.restype = C.c_void_p
@@ -226,7 +244,8 @@ def host() -> C.CDLL:
         lib.bw_copy.argtypes = [C.c_void_p, C.c_void_p]
         for f in ("bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step", "bw_end_step",
                   "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_stats_get", "bw_batch_begin_step",
-                  "bw_batch_views", "bw_batch_end_step", "bw_row_memory_get", "bw_batch_row_memory", "bw_copy"):
+                  "bw_batch_views", "bw_batch_end_step", "bw_row_memory_get", "bw_batch_row_memory", "bw_copy",
+                  "bw_keep_backward", "bw_narrow_backward", "bw_materials"):
             getattr(lib, f).restype = C.c_int32
         _host = lib
     return _host
@@ -269,6 +288,13 @@ def gpu() -> C.CDLL:
         lib.bg_block_threads.restype = C.c_int32
         lib.bg_set_batch_groups.argtypes = [C.c_void_p, C.c_int32]
         lib.bg_set_batch_groups.restype = C.c_int32
+        lib.bg_backward.argtypes = three + [C.POINTER(Worlds), C.POINTER(Step), C.POINTER(BodyGrads), C.POINTER(RowGrads),
+                                            C.POINTER(BodyGrads), C.POINTER(RowGrads)]
+        lib.bg_backward.restype = C.c_int32
+        lib.bg_backward_tape_peak.argtypes = [C.c_void_p]
+        lib.bg_backward_tape_peak.restype = C.c_int32
+        lib.bg_backward_ms.argtypes = [C.c_void_p]
+        lib.bg_backward_ms.restype = C.c_double
         lib.bg_solve_step_static.argtypes = [C.POINTER(Bodies), C.POINTER(Rows), C.POINTER(Step), C.c_void_p]
         lib.bg_solve_step_static.restype = C.c_int32
         for f in ("bg_solve_step", "bg_upload", "bg_restore", "bg_solve", "bg_download",
@@ -284,11 +310,13 @@ GPU_SYMBOLS = [
     "bg_create", "bg_destroy", "bg_last_error", "bg_version", "bg_solve_step", "bg_upload", "bg_restore",
     "bg_solve", "bg_download", "bg_batch_solve_step", "bg_batch_upload", "bg_batch_solve",
     "bg_batch_download", "bg_stream", "bg_last_launches", "bg_last_stage_ms", "bg_set_wait_budget", "bg_set_block_threads",
-    "bg_block_threads", "bg_set_batch_groups", "bg_solve_step_static",
+    "bg_block_threads", "bg_set_batch_groups", "bg_backward", "bg_backward_tape_peak", "bg_backward_ms",
+    "bg_solve_step_static",
 ]
 HOST_SYMBOLS = [
     "bw_create", "bw_destroy", "bw_last_error", "bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step",
     "bw_end_step", "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_transforms", "bw_stats_get",
     "bw_batch_create", "bw_batch_destroy", "bw_batch_begin_step", "bw_batch_views", "bw_batch_end_step",
-    "bw_row_memory_get", "bw_batch_row_memory", "bw_clone", "bw_copy",
+    "bw_row_memory_get", "bw_batch_row_memory", "bw_clone", "bw_copy", "bw_keep_backward", "bw_narrow_backward",
+    "bw_materials",
 ]

@@ -28,6 +28,7 @@
 #include "../../include/bearing_gpu.h"
 #include "layout.cuh"
 #include "stage.cuh"
+#include "adjoint.cuh"
 
 namespace {
 
@@ -484,6 +485,19 @@ struct bg_ctx {
   int nbodies = 0, nrows = 0, nawake = 0, nworlds = 0;
   bool uploaded = false;
   bool batch = false;
+  // bg_backward's own device memory (grown by doubling, freed with the context)
+  struct Adjoint {
+    std::vector<void*> allocs;
+    size_t bodies = 0, rows = 0, awake = 0, worlds = 0, threads = 0;
+    int substeps = 0;
+    unsigned char* in = nullptr;     // the step's input columns
+    unsigned char* work = nullptr;   // the recomputed state, records and adjoints
+    bgad::Tape* tapes = nullptr;
+    int32_t* status = nullptr;
+    cudaEvent_t begin = nullptr, end = nullptr;
+    int peak = 0;
+    bool timed = false;
+  } adj;
 };
 
 namespace {
@@ -1206,6 +1220,10 @@ void bg_destroy(bg_ctx* c) {
   for (bg_ctx* k : c->kids) bg_destroy(k);
   c->kids.clear();
   free_all(c);
+  for (void* p : c->adj.allocs) cudaFree(p);
+  c->adj.allocs.clear();
+  if (c->adj.begin) cudaEventDestroy(c->adj.begin);
+  if (c->adj.end) cudaEventDestroy(c->adj.end);
   c->pool.reset();
   if (c->in_free) cudaEventDestroy(c->in_free);
   for (cudaEvent_t e : c->out_ready)
@@ -1691,6 +1709,399 @@ int32_t bg_batch_solve_step(bg_ctx* c, const bg_bodies* B, const bg_rows* R, con
   rc = bg_batch_solve(c, step);
   if (rc != BG_OK) return rc;
   return bg_batch_download(c, B, R);
+}
+
+}  // extern "C"
+
+// ---- the adjoint of the solve stage (bg_backward) ------------------------------------------
+//
+// One warp a world: adjoint_step recomputes the world's step with records (bgadj::forward), then
+// sweeps it in reverse (bgadj::reverse), each lane replaying rows and bodies on a tape of its own.
+
+namespace bgad {
+// This block's tapes, one a thread, set as each block of the adjoint kernel starts.
+__shared__ Tape* s_block_tapes;
+#ifdef __CUDA_ARCH__
+__device__ Tape* thread_tape() { return s_block_tapes + threadIdx.x; }
+#else
+// Host code of this library never records (only the kernels do).
+Tape* thread_tape() { return nullptr; }
+#endif
+}  // namespace bgad
+
+namespace {
+
+constexpr int kAdjointThreads = 32;   // one warp a world
+
+struct WarpLane {
+  int id, n;
+  __device__ void sync() const { __syncwarp(); }
+};
+
+__global__ void adjoint_tapes(bgad::Tape* tapes, int threads, int32_t* pa, int32_t* pb, double* da, double* db,
+                              double* adj, int cap) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= threads) return;
+  const size_t o = static_cast<size_t>(t) * static_cast<size_t>(cap);
+  tapes[t] = bgad::Tape{0, cap, pa + o, pb + o, da + o, db + o, adj + o, 0, 0};
+}
+
+__global__ void __launch_bounds__(kAdjointThreads) adjoint_step(bgadj::AdjParams A, bgad::Tape* tapes) {
+  if (threadIdx.x == 0) bgad::s_block_tapes = tapes + static_cast<size_t>(blockIdx.x) * blockDim.x;
+  __syncthreads();
+  const WarpLane lane{static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x)};
+  for (int wi = blockIdx.x; wi < A.nworlds; wi += gridDim.x) {
+    const bgadj::AdjWorld W = A.worlds[wi];
+    bgadj::forward(A, W, lane);
+    bgadj::reverse(A, W, lane);
+  }
+}
+
+// The recomputed step's row results and the rows' adjoints, from the kernel's per-row state into
+// the caller's layout.
+struct AdjRowOut {
+  double *ni, *ti1, *ti2, *ri1, *ri2, *si, *gap, *maxni, *relvel, *anchor_a, *anchor_b;
+  uint8_t* sliding;
+  double *g_ni, *g_ti1, *g_ti2, *g_ri1, *g_ri2, *g_si;
+};
+
+__global__ void adjoint_pack(const double* st, const double* bst, const double* pr, AdjRowOut o, int n) {
+  using namespace bgadj;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+    const double* x = st + RSTATE * static_cast<int64_t>(m);
+    const double* g = bst + RSTATE * static_cast<int64_t>(m);
+    const double* q = pr + PREP * static_cast<int64_t>(m);
+    for (int k = 0; k < bg::P; k++) {
+      o.ni[4 * m + k] = x[RS_NI + k]; o.maxni[4 * m + k] = x[RS_MAXNI + k]; o.relvel[4 * m + k] = x[RS_RELVEL + k];
+      o.g_ni[4 * m + k] = g[RS_NI + k];
+    }
+    o.ti1[m] = x[RS_TI1]; o.ti2[m] = x[RS_TI2]; o.ri1[m] = x[RS_RI1]; o.ri2[m] = x[RS_RI2]; o.si[m] = x[RS_SI];
+    o.gap[m] = x[RS_GAP]; o.sliding[m] = static_cast<uint8_t>(x[RS_SLID] != 0);
+    o.g_ti1[m] = g[RS_TI1]; o.g_ti2[m] = g[RS_TI2]; o.g_ri1[m] = g[RS_RI1]; o.g_ri2[m] = g[RS_RI2]; o.g_si[m] = g[RS_SI];
+    for (int k = 0; k < 3; k++) { o.anchor_a[3 * m + k] = q[PR_ANA + k]; o.anchor_b[3 * m + k] = q[PR_ANB + k]; }
+  }
+}
+
+// A bump allocator over one device block: each piece starts on a 256-byte boundary.
+struct Carve {
+  unsigned char* base;
+  size_t end = 0;
+  template <class T>
+  T* take(size_t n) {
+    T* at = base == nullptr ? nullptr : reinterpret_cast<T*>(base + end);
+    end = (end + (n > 0 ? n : 1) * sizeof(T) + 255) & ~static_cast<size_t>(255);
+    return at;
+  }
+};
+
+// The adjoint kernel's arrays for nb slots, nr rows, na awake entries and nw worlds, carved from
+// `in` (the step's input, as the caller's columns) and `work` (state, records and adjoints).
+// Returns the two blocks' sizes; with NULL bases it only measures.
+struct AdjLayout {
+  bgadj::AdjParams A;
+  bgadj::AdjWorld* worlds;
+  // the step's input and seeds, where the caller's columns are copied to
+  double *p, *q, *v, *w, *tum, *ceil, *inv_mass, *inertia, *inv_inertia, *dims, *damping, *ang_damping, *grav_scale;
+  uint8_t *type, *shape, *framed, *awake, *points;
+  int32_t *awake_list, *row, *a, *b;
+  double *normal, *t1, *t2, *friction, *restitution, *tolerance, *patch, *separation, *point, *shift;
+  double *ni, *ti1, *ti2, *ri1, *ri2, *si, *drift1, *drift2, *maxni, *relvel, *gap;
+  double *seed_ni, *seed_ti1, *seed_ti2, *seed_ri1, *seed_ri2, *seed_si;
+  AdjRowOut out;
+  size_t in_bytes, work_bytes;
+};
+
+AdjLayout adj_layout(unsigned char* in, unsigned char* work, size_t nb, size_t nr, size_t na, size_t nw, int substeps) {
+  using namespace bgadj;
+  AdjLayout L = {};
+  Carve ci{in};
+  L.p = ci.take<double>(3 * nb); L.q = ci.take<double>(4 * nb); L.v = ci.take<double>(3 * nb);
+  L.w = ci.take<double>(3 * nb); L.tum = ci.take<double>(3 * nb); L.ceil = ci.take<double>(nb);
+  L.inv_mass = ci.take<double>(nb); L.inertia = ci.take<double>(3 * nb); L.inv_inertia = ci.take<double>(3 * nb);
+  L.dims = ci.take<double>(3 * nb); L.damping = ci.take<double>(nb); L.ang_damping = ci.take<double>(nb);
+  L.grav_scale = ci.take<double>(nb); L.type = ci.take<uint8_t>(nb); L.shape = ci.take<uint8_t>(nb);
+  L.framed = ci.take<uint8_t>(nb); L.awake = ci.take<uint8_t>(nb); L.awake_list = ci.take<int32_t>(na);
+  L.row = ci.take<int32_t>(nr); L.a = ci.take<int32_t>(nr); L.b = ci.take<int32_t>(nr); L.points = ci.take<uint8_t>(nr);
+  L.normal = ci.take<double>(3 * nr); L.t1 = ci.take<double>(3 * nr); L.t2 = ci.take<double>(3 * nr);
+  L.friction = ci.take<double>(nr); L.restitution = ci.take<double>(nr); L.tolerance = ci.take<double>(nr);
+  L.patch = ci.take<double>(nr); L.separation = ci.take<double>(4 * nr); L.point = ci.take<double>(12 * nr);
+  L.shift = ci.take<double>(12 * nr); L.ni = ci.take<double>(4 * nr); L.ti1 = ci.take<double>(nr);
+  L.ti2 = ci.take<double>(nr); L.ri1 = ci.take<double>(nr); L.ri2 = ci.take<double>(nr); L.si = ci.take<double>(nr);
+  L.drift1 = ci.take<double>(nr); L.drift2 = ci.take<double>(nr); L.maxni = ci.take<double>(4 * nr);
+  L.relvel = ci.take<double>(4 * nr); L.gap = ci.take<double>(nr);
+  L.seed_ni = ci.take<double>(4 * nr); L.seed_ti1 = ci.take<double>(nr); L.seed_ti2 = ci.take<double>(nr);
+  L.seed_ri1 = ci.take<double>(nr); L.seed_ri2 = ci.take<double>(nr); L.seed_si = ci.take<double>(nr);
+  L.worlds = ci.take<AdjWorld>(nw);
+  L.in_bytes = ci.end;
+  AdjParams& A = L.A;
+  A.in_p = L.p; A.in_q = L.q; A.in_v = L.v; A.in_w = L.w; A.in_tum = L.tum; A.in_ceil = L.ceil;
+  A.inv_mass = L.inv_mass; A.inertia = L.inertia; A.inv_inertia = L.inv_inertia; A.dims = L.dims; A.damping = L.damping;
+  A.ang_damping = L.ang_damping; A.grav_scale = L.grav_scale; A.type = L.type; A.shape = L.shape; A.framed = L.framed;
+  A.awake = L.awake; A.awake_list = L.awake_list; A.row = L.row; A.a = L.a; A.b = L.b; A.points = L.points;
+  A.normal = L.normal; A.t1 = L.t1; A.t2 = L.t2; A.friction = L.friction; A.restitution = L.restitution;
+  A.tolerance = L.tolerance; A.patch = L.patch; A.separation = L.separation; A.point = L.point; A.shift = L.shift;
+  A.in_ni = L.ni; A.in_ti1 = L.ti1; A.in_ti2 = L.ti2; A.in_ri1 = L.ri1; A.in_ri2 = L.ri2; A.in_si = L.si;
+  A.in_drift1 = L.drift1; A.in_drift2 = L.drift2; A.in_maxni = L.maxni; A.in_relvel = L.relvel; A.in_gap = L.gap;
+  A.seed_ni = L.seed_ni; A.seed_ti1 = L.seed_ti1; A.seed_ti2 = L.seed_ti2; A.seed_ri1 = L.seed_ri1;
+  A.seed_ri2 = L.seed_ri2; A.seed_si = L.seed_si;
+  A.worlds = L.worlds;
+  Carve cw{work};
+  A.p = cw.take<double>(3 * nb); A.q = cw.take<double>(4 * nb); A.v = cw.take<double>(3 * nb); A.w = cw.take<double>(3 * nb);
+  A.tum = cw.take<double>(3 * nb); A.ceil = cw.take<double>(nb); A.start = cw.take<double>(3 * nb);
+  A.startq = cw.take<double>(4 * nb); A.invI = cw.take<double>(6 * nb);
+  A.st = cw.take<double>(RSTATE * nr); A.pr = cw.take<double>(PREP * nr);
+  A.drift1 = cw.take<double>(nr); A.drift2 = cw.take<double>(nr);
+  A.rec_row = cw.take<double>(3 * static_cast<size_t>(substeps) * REC_ROW * nr);
+  A.rec_body = cw.take<double>(static_cast<size_t>(substeps) * REC_BODY * nb);
+  A.rec_rest = cw.take<double>(REC_REST * nr);
+  A.bp = cw.take<double>(3 * nb); A.bq = cw.take<double>(4 * nb); A.bv = cw.take<double>(3 * nb);
+  A.bw = cw.take<double>(3 * nb); A.btum = cw.take<double>(3 * nb); A.bceil = cw.take<double>(nb);
+  A.bstart = cw.take<double>(3 * nb); A.bstartq = cw.take<double>(4 * nb); A.binvI = cw.take<double>(6 * nb);
+  A.bst = cw.take<double>(RSTATE * nr); A.bpr = cw.take<double>(PREP * nr);
+  A.bdrift1 = cw.take<double>(nr); A.bdrift2 = cw.take<double>(nr); A.bnormal = cw.take<double>(3 * nr);
+  A.bt1 = cw.take<double>(3 * nr); A.bt2 = cw.take<double>(3 * nr); A.bfriction = cw.take<double>(nr);
+  A.brestitution = cw.take<double>(nr); A.bseparation = cw.take<double>(4 * nr); A.bpoint = cw.take<double>(12 * nr);
+  AdjRowOut& o = L.out;
+  o.ni = cw.take<double>(4 * nr); o.ti1 = cw.take<double>(nr); o.ti2 = cw.take<double>(nr); o.ri1 = cw.take<double>(nr);
+  o.ri2 = cw.take<double>(nr); o.si = cw.take<double>(nr); o.gap = cw.take<double>(nr); o.maxni = cw.take<double>(4 * nr);
+  o.relvel = cw.take<double>(4 * nr); o.anchor_a = cw.take<double>(3 * nr); o.anchor_b = cw.take<double>(3 * nr);
+  o.sliding = cw.take<uint8_t>(nr); o.g_ni = cw.take<double>(4 * nr); o.g_ti1 = cw.take<double>(nr);
+  o.g_ti2 = cw.take<double>(nr); o.g_ri1 = cw.take<double>(nr); o.g_ri2 = cw.take<double>(nr); o.g_si = cw.take<double>(nr);
+  L.work_bytes = cw.end;
+  return L;
+}
+
+// Grows bg_backward's device memory to hold the given sizes (by doubling, all blocks together).
+bool adj_ensure(bg_ctx* c, size_t nb, size_t nr, size_t na, size_t nw, int substeps, size_t threads) {
+  bg_ctx::Adjoint& d = c->adj;
+  if (d.in != nullptr && nb <= d.bodies && nr <= d.rows && na <= d.awake && nw <= d.worlds && substeps <= d.substeps &&
+      threads <= d.threads)
+    return true;
+  cudaStreamSynchronize(c->stream);
+  for (void* p : d.allocs) cudaFree(p);
+  d.allocs.clear();
+  d.in = nullptr;
+  d.bodies = grown(d.bodies, nb); d.rows = grown(d.rows, nr); d.awake = grown(d.awake, na);
+  d.worlds = grown(d.worlds, nw); d.threads = std::max(d.threads, threads);
+  d.substeps = std::max(d.substeps, substeps);
+  const AdjLayout size = adj_layout(nullptr, nullptr, d.bodies, d.rows, d.awake, d.worlds, d.substeps);
+  const size_t cap = BG_TAPE_NODES;
+  const size_t tape_bytes = d.threads * (sizeof(bgad::Tape) + cap * (2 * sizeof(int32_t) + 3 * sizeof(double)));
+  void* in = nullptr;
+  void* work = nullptr;
+  void* tapes = nullptr;
+  void* status = nullptr;
+  auto fail = [&](const char* what) {
+    set_error(c, "bg_backward: cudaMalloc of %s failed", what);
+    for (void* p : {in, work, tapes, status})
+      if (p) cudaFree(p);
+    d.bodies = d.rows = d.awake = d.worlds = d.threads = 0;
+    d.substeps = 0;
+    cudaGetLastError();
+    return false;
+  };
+  if (cudaMalloc(&in, size.in_bytes) != cudaSuccess) return fail("the step's input");
+  if (cudaMalloc(&work, size.work_bytes) != cudaSuccess) return fail("the records");
+  if (cudaMalloc(&tapes, tape_bytes) != cudaSuccess) return fail("the tapes");
+  if (cudaMalloc(&status, sizeof(int32_t)) != cudaSuccess) return fail("the status word");
+  d.allocs = {in, work, tapes, status};
+  d.in = static_cast<unsigned char*>(in);
+  d.work = static_cast<unsigned char*>(work);
+  d.tapes = static_cast<bgad::Tape*>(tapes);
+  d.status = static_cast<int32_t*>(status);
+  unsigned char* nodes = static_cast<unsigned char*>(tapes) + ((d.threads * sizeof(bgad::Tape) + 255) & ~size_t{255});
+  int32_t* pa = reinterpret_cast<int32_t*>(nodes);
+  int32_t* pb = pa + d.threads * cap;
+  double* da = reinterpret_cast<double*>(pb + d.threads * cap);
+  double* db = da + d.threads * cap;
+  double* adj = db + d.threads * cap;
+  const int blocks = static_cast<int>((d.threads + 255) / 256);
+  adjoint_tapes<<<blocks, 256, 0, c->stream>>>(d.tapes, static_cast<int>(d.threads), pa, pb, da, db, adj, static_cast<int>(cap));
+  return cuda_ok(c, cudaGetLastError(), "bg_backward tapes");
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t bg_backward(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_worlds* W, const bg_step* S,
+                    const bg_body_grads* bs, const bg_row_grads* rs, bg_body_grads* bg, bg_row_grads* rg) {
+  if (c == nullptr) return BG_EINVAL;
+  cudaSetDevice(c->device);
+  std::vector<bg::WorldDesc> worlds;
+  int rc = BG_OK;
+  if (W != nullptr) {
+    rc = batch_worlds(c, B, R, W, worlds);
+  } else {
+    rc = validate(c, B, R);
+    if (rc == BG_OK) rc = validate_world(c, B->capacity, R->count, R->starts, R->solved);
+    if (rc == BG_OK) {
+      bg::WorldDesc w = {};
+      w.nbodies = B->capacity; w.nawake = B->awake_count; w.nrows = R->count; w.solved = R->solved;
+      for (int k = 0; k < bg::NSTARTS; k++) w.starts[k] = R->starts[k];
+      worlds.assign(1, w);
+    }
+  }
+  if (rc != BG_OK) return rc;
+  if (S == nullptr || !(S->dt > 0) || S->substeps < 1 || bs == nullptr || rs == nullptr || bg == nullptr || rg == nullptr) {
+    set_error(c, "bg_backward: step, seeds and results must be given, dt positive, substeps at least 1");
+    return BG_EINVAL;
+  }
+  {
+    std::vector<uint8_t> seen(static_cast<size_t>(R->count), 0);
+    char why[256];
+    const char* bad = index_problem(B, R, worlds, 0, worlds.size(), seen.data(), why, sizeof why);
+    if (bad != nullptr) {
+      set_error(c, "%s", bad);
+      return BG_EINVAL;
+    }
+  }
+  const int nb = B->capacity, nr = R->count, na = B->awake_count, nw = static_cast<int>(worlds.size());
+  for (int s = 0; s < nb; s++)
+    if ((B->type[s] != BG_DYNAMIC && B->type[s] != BG_STATIC) || B->lock[s] != 0 || B->frozen[s] != 0 ||
+        B->joint_head[s] != 0 || B->shape[s] > BG_CAPSULE) {
+      set_error(c, "bg_backward: slot %d is kinematic, locked, frozen, jointed or not a box, sphere or capsule", s);
+      return BG_EUNSUPPORTED;
+    }
+  const size_t threads = static_cast<size_t>(std::min(nw, 4 * c->sms)) * kAdjointThreads;
+  if (!adj_ensure(c, static_cast<size_t>(nb), static_cast<size_t>(nr), static_cast<size_t>(na), static_cast<size_t>(nw),
+                  S->substeps, threads))
+    return BG_ENOMEM;
+  bg_ctx::Adjoint& d = c->adj;
+  AdjLayout L = adj_layout(d.in, d.work, d.bodies, d.rows, d.awake, d.worlds, d.substeps);
+  bgadj::AdjParams& A = L.A;
+  A.rows_total = nr;
+  A.bodies_total = nb;
+  A.dt = S->dt;
+  A.substeps = S->substeps;
+  const bg::Soft soft = make_soft(S->dt / S->substeps);
+  A.soft = bgadj::SoftK{soft.biasRate, soft.massScale, soft.impulseScale};
+  A.nworlds = nw;
+  A.status = d.status;
+  std::vector<bgadj::AdjWorld> aw(static_cast<size_t>(nw));
+  for (int i = 0; i < nw; i++) {
+    const bg::WorldDesc& w = worlds[static_cast<size_t>(i)];
+    bgadj::AdjWorld& x = aw[static_cast<size_t>(i)];
+    x.body0 = w.body0; x.nbodies = w.nbodies; x.awake0 = w.awake0; x.nawake = w.nawake; x.row0 = w.row0;
+    x.nrows = w.nrows; x.solved = w.solved;
+    for (int k = 0; k < bg::NSTARTS; k++) x.starts[k] = w.starts[k];
+    for (int k = 0; k < 3; k++) x.gravity[k] = W != nullptr && W->gravity != nullptr ? W->gravity[3 * i + k] : S->gravity[k];
+  }
+  cudaStream_t st = c->stream;
+  bool ok = true;
+  auto h2d = [&](void* dst, const void* src, size_t bytes, const char* what) {
+    if (!ok || bytes == 0) return;
+    if (src == nullptr) {
+      set_error(c, "bg_backward: %s is NULL", what);
+      ok = false;
+      return;
+    }
+    ok = cuda_ok(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st), what);
+  };
+  const size_t b8 = sizeof(double) * static_cast<size_t>(nb), r8 = sizeof(double) * static_cast<size_t>(nr);
+  h2d(L.p, B->position, 3 * b8, "position"); h2d(L.q, B->rotation, 4 * b8, "rotation");
+  h2d(L.v, B->velocity, 3 * b8, "velocity"); h2d(L.w, B->angular, 3 * b8, "angular");
+  h2d(L.tum, B->tumbled, 3 * b8, "tumbled"); h2d(L.ceil, B->ceiling, b8, "ceiling");
+  h2d(L.inv_mass, B->inv_mass, b8, "inv_mass"); h2d(L.inertia, B->inertia, 3 * b8, "inertia");
+  h2d(L.inv_inertia, B->inv_inertia, 3 * b8, "inv_inertia"); h2d(L.dims, B->dims, 3 * b8, "dims");
+  h2d(L.damping, B->damping, b8, "damping"); h2d(L.ang_damping, B->angular_damping, b8, "angular_damping");
+  h2d(L.grav_scale, B->gravity_scale, b8, "gravity_scale"); h2d(L.type, B->type, static_cast<size_t>(nb), "type");
+  h2d(L.shape, B->shape, static_cast<size_t>(nb), "shape"); h2d(L.framed, B->framed, static_cast<size_t>(nb), "framed");
+  h2d(L.awake, B->awake, static_cast<size_t>(nb), "awake");
+  h2d(L.awake_list, B->awake_list, sizeof(int32_t) * static_cast<size_t>(na), "awake_list");
+  h2d(L.row, R->row, sizeof(int32_t) * static_cast<size_t>(nr), "row"); h2d(L.a, R->a, sizeof(int32_t) * static_cast<size_t>(nr), "a");
+  h2d(L.b, R->b, sizeof(int32_t) * static_cast<size_t>(nr), "b"); h2d(L.points, R->points, static_cast<size_t>(nr), "points");
+  h2d(L.normal, R->normal, 3 * r8, "normal"); h2d(L.t1, R->t1, 3 * r8, "t1"); h2d(L.t2, R->t2, 3 * r8, "t2");
+  h2d(L.friction, R->friction, r8, "friction"); h2d(L.restitution, R->restitution, r8, "restitution");
+  h2d(L.tolerance, R->tolerance, r8, "tolerance"); h2d(L.patch, R->patch, r8, "patch");
+  h2d(L.separation, R->separation, 4 * r8, "separation"); h2d(L.point, R->point, 12 * r8, "point");
+  h2d(L.shift, R->shift, 12 * r8, "shift"); h2d(L.ni, R->normal_impulse, 4 * r8, "normal_impulse");
+  h2d(L.ti1, R->tangent_impulse1, r8, "tangent_impulse1"); h2d(L.ti2, R->tangent_impulse2, r8, "tangent_impulse2");
+  h2d(L.ri1, R->roll_impulse1, r8, "roll_impulse1"); h2d(L.ri2, R->roll_impulse2, r8, "roll_impulse2");
+  h2d(L.si, R->spin_impulse, r8, "spin_impulse"); h2d(L.drift1, R->drift1, r8, "drift1"); h2d(L.drift2, R->drift2, r8, "drift2");
+  h2d(L.maxni, R->max_normal_impulse, 4 * r8, "max_normal_impulse");
+  h2d(L.relvel, R->relative_velocity, 4 * r8, "relative_velocity"); h2d(L.gap, R->gap, r8, "gap");
+  h2d(A.bp, bs->position, 3 * b8, "seed position"); h2d(A.bq, bs->rotation, 4 * b8, "seed rotation");
+  h2d(A.bv, bs->velocity, 3 * b8, "seed velocity"); h2d(A.bw, bs->angular, 3 * b8, "seed angular");
+  h2d(A.btum, bs->tumbled, 3 * b8, "seed tumbled"); h2d(A.bceil, bs->ceiling, b8, "seed ceiling");
+  h2d(L.seed_ni, rs->normal_impulse, 4 * r8, "seed normal_impulse");
+  h2d(L.seed_ti1, rs->tangent_impulse1, r8, "seed tangent_impulse1");
+  h2d(L.seed_ti2, rs->tangent_impulse2, r8, "seed tangent_impulse2");
+  h2d(L.seed_ri1, rs->roll_impulse1, r8, "seed roll_impulse1"); h2d(L.seed_ri2, rs->roll_impulse2, r8, "seed roll_impulse2");
+  h2d(L.seed_si, rs->spin_impulse, r8, "seed spin_impulse");
+  h2d(A.bdrift1, rs->drift1, r8, "seed drift1"); h2d(A.bdrift2, rs->drift2, r8, "seed drift2");
+  h2d(L.worlds, aw.data(), sizeof(bgadj::AdjWorld) * static_cast<size_t>(nw), "worlds");
+  ok = ok && cuda_ok(c, cudaMemsetAsync(d.status, 0, sizeof(int32_t), st), "status");
+  if (!ok) {
+    cudaStreamSynchronize(st);
+    return BG_EINVAL;
+  }
+  if (d.begin == nullptr) {
+    cudaEventCreate(&d.begin);
+    cudaEventCreate(&d.end);
+  }
+  cudaEventRecord(d.begin, st);
+  const int blocks = static_cast<int>(threads / kAdjointThreads);
+  adjoint_step<<<blocks, kAdjointThreads, 0, st>>>(A, d.tapes);
+  if (!cuda_ok(c, cudaGetLastError(), "adjoint_step launch")) return BG_ECUDA;
+  cudaEventRecord(d.end, st);
+  d.timed = true;
+  const int pblocks = std::max(1, std::min(4 * c->sms, (nr + 255) / 256));
+  adjoint_pack<<<pblocks, 256, 0, st>>>(A.st, A.bst, A.pr, L.out, nr);
+  if (!cuda_ok(c, cudaGetLastError(), "adjoint_pack launch")) return BG_ECUDA;
+  auto d2h = [&](void* dst, const void* src, size_t bytes, const char* what) {
+    if (!ok || bytes == 0 || dst == nullptr) return;
+    ok = cuda_ok(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st), what);
+  };
+  // the recomputed step's results, as bg_solve_step leaves them
+  d2h(B->position, A.p, 3 * b8, "position"); d2h(B->rotation, A.q, 4 * b8, "rotation");
+  d2h(B->velocity, A.v, 3 * b8, "velocity"); d2h(B->angular, A.w, 3 * b8, "angular");
+  d2h(B->tumbled, A.tum, 3 * b8, "tumbled"); d2h(B->ceiling, A.ceil, b8, "ceiling");
+  d2h(R->normal_impulse, L.out.ni, 4 * r8, "normal_impulse"); d2h(R->tangent_impulse1, L.out.ti1, r8, "tangent_impulse1");
+  d2h(R->tangent_impulse2, L.out.ti2, r8, "tangent_impulse2"); d2h(R->roll_impulse1, L.out.ri1, r8, "roll_impulse1");
+  d2h(R->roll_impulse2, L.out.ri2, r8, "roll_impulse2"); d2h(R->spin_impulse, L.out.si, r8, "spin_impulse");
+  d2h(R->drift1, A.drift1, r8, "drift1"); d2h(R->drift2, A.drift2, r8, "drift2"); d2h(R->gap, L.out.gap, r8, "gap");
+  d2h(R->max_normal_impulse, L.out.maxni, 4 * r8, "max_normal_impulse");
+  d2h(R->relative_velocity, L.out.relvel, 4 * r8, "relative_velocity");
+  d2h(R->sliding, L.out.sliding, static_cast<size_t>(nr), "sliding");
+  d2h(R->anchor_a, L.out.anchor_a, 3 * r8, "anchor_a"); d2h(R->anchor_b, L.out.anchor_b, 3 * r8, "anchor_b");
+  // the adjoints of the step's input
+  d2h(bg->position, A.bp, 3 * b8, "grad position"); d2h(bg->rotation, A.bq, 4 * b8, "grad rotation");
+  d2h(bg->velocity, A.bv, 3 * b8, "grad velocity"); d2h(bg->angular, A.bw, 3 * b8, "grad angular");
+  d2h(bg->tumbled, A.btum, 3 * b8, "grad tumbled"); d2h(bg->ceiling, A.bceil, b8, "grad ceiling");
+  d2h(rg->normal_impulse, L.out.g_ni, 4 * r8, "grad normal_impulse");
+  d2h(rg->tangent_impulse1, L.out.g_ti1, r8, "grad tangent_impulse1");
+  d2h(rg->tangent_impulse2, L.out.g_ti2, r8, "grad tangent_impulse2");
+  d2h(rg->roll_impulse1, L.out.g_ri1, r8, "grad roll_impulse1"); d2h(rg->roll_impulse2, L.out.g_ri2, r8, "grad roll_impulse2");
+  d2h(rg->spin_impulse, L.out.g_si, r8, "grad spin_impulse");
+  d2h(rg->drift1, A.bdrift1, r8, "grad drift1"); d2h(rg->drift2, A.bdrift2, r8, "grad drift2");
+  d2h(rg->normal, A.bnormal, 3 * r8, "grad normal"); d2h(rg->t1, A.bt1, 3 * r8, "grad t1"); d2h(rg->t2, A.bt2, 3 * r8, "grad t2");
+  d2h(rg->friction, A.bfriction, r8, "grad friction"); d2h(rg->restitution, A.brestitution, r8, "grad restitution");
+  d2h(rg->separation, A.bseparation, 4 * r8, "grad separation"); d2h(rg->point, A.bpoint, 12 * r8, "grad point");
+  int32_t status = 0;
+  std::vector<bgad::Tape> tapes(threads);
+  d2h(&status, d.status, sizeof status, "status");
+  d2h(tapes.data(), d.tapes, sizeof(bgad::Tape) * threads, "tapes");
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(st), "bg_backward");
+  if (!ok) return BG_ECUDA;
+  d.peak = 0;
+  for (const bgad::Tape& t : tapes) d.peak = std::max(d.peak, std::max(t.peak, t.n));
+  if (status != 0) {
+    set_error(c, "bg_backward: a replay needed more than %d tape nodes", BG_TAPE_NODES);
+    return BG_ENOMEM;
+  }
+  return BG_OK;
+}
+
+int32_t bg_backward_tape_peak(const bg_ctx* c) { return c == nullptr ? BG_EINVAL : c->adj.peak; }
+
+double bg_backward_ms(bg_ctx* c) {
+  if (c == nullptr || !c->adj.timed) return -1.0;
+  cudaSetDevice(c->device);
+  if (cudaEventSynchronize(c->adj.end) != cudaSuccess) return -1.0;
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, c->adj.begin, c->adj.end) != cudaSuccess) return -1.0;
+  return static_cast<double>(ms);
 }
 
 }  // extern "C"

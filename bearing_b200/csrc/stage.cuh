@@ -68,7 +68,7 @@ __device__ __forceinline__ void axes_of(const double* q, double* ax) {
 
 // The reference's own arctangent (src/core/math.js:127-200, fdlibm's method and constants as it
 // states them), so slipped() turns angles to the same bits.
-__device__ __forceinline__ double ref_atan(double x) {
+__host__ __device__ __forceinline__ double ref_atan(double x) {
   const double ATAN_HI[4] = {4.63647609000806093515e-01, 7.85398163397448278999e-01,
                              9.82793723247329054082e-01, 1.57079632679489655800e+00};
   const double ATAN_LO[4] = {2.26987774529616870924e-17, 3.06161699786838301793e-17,
@@ -104,7 +104,7 @@ __device__ __forceinline__ double ref_atan(double x) {
   return x < 0 ? -r : r;
 }
 
-__device__ __forceinline__ double ref_atan2(double y, double x) {
+__host__ __device__ __forceinline__ double ref_atan2(double y, double x) {
   const double PI_ = 3.1415926535897931160e+00, PI_LO = 1.2246467991473531772e-16;
   const double PI_O_2 = 1.5707963267948965580e+00, PI_O_4 = 7.8539816339744827900e-01;
   if (x != x || y != y) return x + y;

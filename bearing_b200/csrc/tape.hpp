@@ -37,6 +37,7 @@ struct Tape {
   double* db;
   double* adj;
   int32_t overflow;   // a node did not fit: the replay's adjoints are not to be used
+  int32_t peak;       // the most nodes any replay on this tape has recorded
 };
 
 // The calling thread's tape (defined once, where the tapes are set up: device and host side).
@@ -108,10 +109,10 @@ BGAD_HD TV fabs(const TV& a) { return unary(a.v < 0 ? -a.v : a.v, a, a.v < 0 ? -
 BGAD_HD double val(const TV& a) { return a.v; }
 BGAD_HD double val(double a) { return a; }
 
-// Clears the tape for a new replay.
+// Clears the tape for a new replay (an overflow stays flagged until the caller reads it).
 BGAD_HD void reset(Tape* t) {
+  if (t->n > t->peak) t->peak = t->n;
   t->n = 0;
-  t->overflow = 0;
 }
 
 // Adds g to the adjoint of x's node (nothing for a constant).

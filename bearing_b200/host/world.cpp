@@ -25,7 +25,8 @@
 #include <unordered_map>
 #include <vector>
 
-#include "collide.hpp"
+#include "collide_impl.hpp"
+#include "../csrc/tape.hpp"
 
 namespace {
 
@@ -862,6 +863,15 @@ int32_t bw_row_memory_get(const bw_world* w, bw_row_memory* out) {
   return BG_OK;
 }
 
+int32_t bw_materials(const bw_world* w, double* friction, double* restitution) {
+  if (w == nullptr || friction == nullptr || restitution == nullptr) return BG_EINVAL;
+  for (int s = 0; s < w->n; s++) {
+    friction[s] = w->friction[static_cast<size_t>(s)];
+    restitution[s] = w->restitution[static_cast<size_t>(s)];
+  }
+  return BG_OK;
+}
+
 bw_world* bw_clone(const bw_world* w) {
   if (w == nullptr) return nullptr;
   try {
@@ -1151,6 +1161,252 @@ int32_t bw_batch_end_step(bw_batch* b, int32_t threads) {
     take(b->relativeVelocity, 4 * r, c.relativeVelocity.data(), 4 * m); take(b->sliding, r, c.sliding.data(), m);
     take(b->anchorA, 3 * r, c.anchorA.data(), 3 * m); take(b->anchorB, 3 * r, c.anchorB.data(), 3 * m);
     rcs[static_cast<size_t>(i)] = bw_end_step(w);
+  });
+  for (int32_t rc : rcs)
+    if (rc != BG_OK) return rc;
+  return BG_OK;
+}
+
+}  // extern "C"
+
+// ---- the host side's share of a step's adjoint ----
+
+namespace bgad {
+namespace {
+thread_local Tape* t_tape = nullptr;
+}
+Tape* thread_tape() { return t_tape; }
+}  // namespace bgad
+
+namespace {
+
+using bgad::TV;
+
+// A tape of the calling host thread's own, for the life of one object.
+struct HostTape {
+  std::vector<int32_t> pa, pb;
+  std::vector<double> da, db, adj;
+  bgad::Tape t{};
+  explicit HostTape(int cap) : pa(static_cast<size_t>(cap)), pb(static_cast<size_t>(cap)), da(static_cast<size_t>(cap)),
+                               db(static_cast<size_t>(cap)), adj(static_cast<size_t>(cap)) {
+    t = bgad::Tape{0, cap, pa.data(), pb.data(), da.data(), db.data(), adj.data(), 0, 0};
+    bgad::t_tape = &t;
+  }
+  ~HostTape() { bgad::t_tape = nullptr; }
+};
+
+// Math.max with JavaScript's NaN and signed-zero rules, for recorded values.
+TV jmax_tv(const TV& a, const TV& b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  if (a > b) return a;
+  if (b > a) return b;
+  if (a == 0 && b == 0) return std::signbit(a.v) ? b : a;
+  return a;
+}
+
+// axesOf: src/core/math.js:222-227.
+void axes_tv(const TV* q, TV* ax) {
+  const TV x = q[0], y = q[1], z = q[2], w = q[3];
+  ax[0] = 1 - 2 * (y * y + z * z); ax[1] = 2 * (x * y + z * w); ax[2] = 2 * (x * z - y * w);
+  ax[3] = 2 * (x * y - z * w); ax[4] = 1 - 2 * (x * x + z * z); ax[5] = 2 * (y * z + x * w);
+  ax[6] = 2 * (x * z + y * w); ax[7] = 2 * (y * z - x * w); ax[8] = 1 - 2 * (x * x + y * y);
+}
+
+// World w of a batch (or the one world): its first slot, first row and row count.
+struct Part {
+  int body0, row0, nrows, solved;
+};
+
+std::vector<Part> parts_of(const bg_rows* R, const bg_worlds* W) {
+  std::vector<Part> out;
+  if (W == nullptr) {
+    out.push_back(Part{0, 0, R->count, R->solved});
+    return out;
+  }
+  for (int i = 0; i < W->count; i++)
+    out.push_back(Part{W->body_offset[i], W->row_offset[i], W->row_offset[i + 1] - W->row_offset[i],
+                       W->starts[BG_STARTS * i + RESTING]});
+  return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t bw_keep_backward(const bg_rows* R, const bg_worlds* W, const double* g, bg_row_grads* o) {
+  if (R == nullptr || g == nullptr || o == nullptr) return BG_EINVAL;
+  for (const Part& part : parts_of(R, W)) {
+    for (int j = 0; j < part.nrows; j++) {
+      const int m = part.row0 + j, m3 = 3 * m;
+      const double* gm = g + BW_MEMORY * static_cast<size_t>(m);
+      for (int k = 0; k < P; k++) o->normal_impulse[P * m + k] = 0;
+      o->tangent_impulse1[m] = 0; o->tangent_impulse2[m] = 0; o->roll_impulse1[m] = 0; o->roll_impulse2[m] = 0;
+      o->spin_impulse[m] = 0; o->drift1[m] = 0; o->drift2[m] = 0;
+      if (j >= part.solved) continue;   // a resting row: its pair keeps what it had
+      const double* t1 = R->t1 + m3;
+      const double* t2 = R->t2 + m3;
+      const double* n = R->normal + m3;
+      const double r1 = R->roll_impulse1[m], r2 = R->roll_impulse2[m], sp = R->spin_impulse[m];
+      const double l1 = R->tangent_impulse1[m], l2 = R->tangent_impulse2[m];
+      const double d1 = R->drift1[m], d2 = R->drift2[m];
+      const double* gt = gm + 7;   // twist = t1 r1 + t2 r2 + n sp
+      const double* gf = gm + 4;   // friction = t1 l1 + t2 l2
+      const double* gs = gm + 10;  // slip = t1 d1 + t2 d2
+      for (int c = 0; c < 3; c++) {
+        o->roll_impulse1[m] += t1[c] * gt[c];
+        o->roll_impulse2[m] += t2[c] * gt[c];
+        o->spin_impulse[m] += n[c] * gt[c];
+        o->tangent_impulse1[m] += t1[c] * gf[c];
+        o->tangent_impulse2[m] += t2[c] * gf[c];
+        o->drift1[m] += t1[c] * gs[c];
+        o->drift2[m] += t2[c] * gs[c];
+        o->t1[m3 + c] += r1 * gt[c] + l1 * gf[c] + d1 * gs[c];
+        o->t2[m3 + c] += r2 * gt[c] + l2 * gf[c] + d2 * gs[c];
+        o->normal[m3 + c] += sp * gt[c];
+      }
+      for (int k = 0; k < R->points[m]; k++) o->normal_impulse[P * m + k] = gm[k];
+    }
+  }
+  return BG_OK;
+}
+
+int32_t bw_narrow_backward(const bg_bodies* B, const bg_rows* R, const bg_worlds* W, const bw_row_memory* M,
+                           const double* gravity, const double* friction, const double* restitution,
+                           const bg_row_grads* g, double* gp, double* gq, double* gfr, double* gre, double* gmem,
+                           int32_t threads) {
+  if (B == nullptr || R == nullptr || M == nullptr || gravity == nullptr || friction == nullptr || restitution == nullptr ||
+      g == nullptr || gp == nullptr || gq == nullptr || gfr == nullptr || gre == nullptr || gmem == nullptr)
+    return BG_EINVAL;
+  const std::vector<Part> parts = parts_of(R, W);
+  std::vector<int32_t> rcs(parts.size(), BG_OK);
+  parallel(static_cast<int>(parts.size()), threads, [&](int wi) {
+    const Part& part = parts[static_cast<size_t>(wi)];
+    HostTape tape(1 << 16);
+    bgad::Tape* t = &tape.t;
+    for (int j = 0; j < part.nrows; j++) {
+      const int m = part.row0 + j, m3 = 3 * m;
+      double* gm = gmem + BW_MEMORY * static_cast<size_t>(m);
+      for (int k = 0; k < BW_MEMORY; k++) gm[k] = 0;
+      const int a = part.body0 + R->a[m], b = part.body0 + R->b[m];
+      bgad::reset(t);
+      TV pose[2][7];
+      bearing::ShapeT<TV> sh[2];
+      for (int e = 0; e < 2; e++) {
+        const int s = e == 0 ? a : b;
+        for (int k = 0; k < 3; k++) pose[e][k] = bgad::leaf(B->position[3 * s + k]);
+        for (int k = 0; k < 4; k++) pose[e][3 + k] = bgad::leaf(B->rotation[4 * s + k]);
+        const double* d = B->dims + 3 * s;
+        bearing::ShapeT<TV>& x = sh[e];
+        if (B->shape[s] == BG_BOX) {
+          x.kind = bearing::K_BOX;
+          x.half[0] = d[0] * 0.5; x.half[1] = d[1] * 0.5; x.half[2] = d[2] * 0.5;
+        } else if (B->shape[s] == BG_SPHERE) {
+          x.kind = bearing::K_SPHERE;
+          x.half[0] = d[0];
+        } else {
+          x.kind = bearing::K_CAPSULE;
+          x.half[0] = d[0];
+          x.half[1] = (d[1] - 2 * d[0]) * 0.5;
+        }
+        for (int k = 0; k < 3; k++) x.center[k] = pose[e][k];
+        const double scale = B->type[s] == BG_DYNAMIC ? B->gravity_scale[s] : 0;
+        for (int k = 0; k < 3; k++) x.weight[k] = gravity[k] * scale;
+        axes_tv(pose[e] + 3, x.axes);
+      }
+      const TV fa = bgad::leaf(friction[a]), fb = bgad::leaf(friction[b]);
+      const TV ea = bgad::leaf(restitution[a]), eb = bgad::leaf(restitution[b]);
+      // narrowphase: src/collide.js:204-218
+      bearing::ManifoldT<TV> mf;
+      bearing::collideT<TV>(sh[0], sh[1], M->margin[m], R->tolerance[m], mf);
+      const int count = R->points[m];
+      bool same_points = mf.count == count;
+      for (int k = 0; k < count && same_points; k++) same_points = mf.ids[k] == M->pid[P * m + k];
+      if (!same_points || t->overflow) {
+        rcs[static_cast<size_t>(wi)] = BG_EFAULT;
+        return;
+      }
+      // emit: src/contact.js:901-921, basis: 1283-1292
+      const TV fr = sqrt(fa * fb);
+      const TV re = jmax_tv(ea, eb);
+      const TV nx = mf.normal[0], ny = mf.normal[1], nz = mf.normal[2];
+      const TV ax = fabs(nx), ay = fabs(ny), az = fabs(nz);
+      TV tx, ty, tz;
+      if (ax <= ay && ax <= az) { tx = 0; ty = nz; tz = -ny; } else if (ay <= az) { tx = -nz; ty = 0; tz = nx; } else { tx = ny; ty = -nx; tz = 0; }
+      const TV l = 1 / sqrt(tx * tx + ty * ty + tz * tz);
+      tx *= l; ty *= l; tz *= l;
+      const TV T1[3] = {tx, ty, tz};
+      const TV T2[3] = {ny * tz - nz * ty, nz * tx - nx * tz, nx * ty - ny * tx};
+      const TV N[3] = {nx, ny, nz};
+      // carry: src/contact.js:999-1036
+      const int remembered = M->remembered[m];
+      TV mem[13];
+      TV ni[P], ti1, ti2, ri1, ri2, si, dr1, dr2;
+      if (remembered > 0) {
+        const double* src = M->memory + BW_MEMORY * static_cast<size_t>(m);
+        for (int k = 0; k < 13; k++) mem[k] = bgad::leaf(src[k]);
+        const TV* twist = mem + 7;
+        const TV* fric = mem + 4;
+        const TV* slip = mem + 10;
+        if (count <= 2) {
+          ri1 = twist[0] * T1[0] + twist[1] * T1[1] + twist[2] * T1[2];
+          ri2 = twist[0] * T2[0] + twist[1] * T2[1] + twist[2] * T2[2];
+        }
+        si = twist[0] * N[0] + twist[1] * N[1] + twist[2] * N[2];
+        ti1 = fric[0] * T1[0] + fric[1] * T1[1] + fric[2] * T1[2];
+        ti2 = fric[0] * T2[0] + fric[1] * T2[1] + fric[2] * T2[2];
+        bool same = false;
+        for (int k = 0; k < count; k++) {
+          for (int q = 0; q < remembered; q++) {
+            if (M->memory_pid[P * m + q] != M->pid[P * m + k]) continue;
+            ni[k] = mem[q];
+            same = true;
+            break;
+          }
+        }
+        if (same) {
+          dr1 = slip[0] * T1[0] + slip[1] * T1[1] + slip[2] * T1[2];
+          dr2 = slip[0] * T2[0] + slip[1] * T2[1] + slip[2] * T2[2];
+        }
+      }
+      if (t->overflow) {
+        rcs[static_cast<size_t>(wi)] = BG_ENOMEM;
+        return;
+      }
+      bgad::clear_adjoints(t);
+      for (int c = 0; c < 3; c++) {
+        bgad::seed(t, N[c], g->normal[m3 + c]);
+        bgad::seed(t, T1[c], g->t1[m3 + c]);
+        bgad::seed(t, T2[c], g->t2[m3 + c]);
+      }
+      bgad::seed(t, fr, g->friction[m]);
+      bgad::seed(t, re, g->restitution[m]);
+      for (int k = 0; k < count; k++) {
+        bgad::seed(t, mf.separations[k], g->separation[P * m + k]);
+        for (int c = 0; c < 3; c++) bgad::seed(t, mf.points[3 * k + c], g->point[12 * m + 3 * k + c]);
+        bgad::seed(t, ni[k], g->normal_impulse[P * m + k]);
+      }
+      bgad::seed(t, ti1, g->tangent_impulse1[m]);
+      bgad::seed(t, ti2, g->tangent_impulse2[m]);
+      bgad::seed(t, ri1, g->roll_impulse1[m]);
+      bgad::seed(t, ri2, g->roll_impulse2[m]);
+      bgad::seed(t, si, g->spin_impulse[m]);
+      bgad::seed(t, dr1, g->drift1[m]);
+      bgad::seed(t, dr2, g->drift2[m]);
+      bgad::sweep(t);
+      for (int e = 0; e < 2; e++) {
+        const int s = e == 0 ? a : b;
+        if (B->type[s] != BG_DYNAMIC || B->inv_mass[s] == 0) continue;
+        for (int k = 0; k < 3; k++) gp[3 * s + k] += bgad::adjoint(t, pose[e][k]);
+        for (int k = 0; k < 4; k++) gq[4 * s + k] += bgad::adjoint(t, pose[e][3 + k]);
+      }
+      gfr[a] += bgad::adjoint(t, fa);
+      gfr[b] += bgad::adjoint(t, fb);
+      gre[a] += bgad::adjoint(t, ea);
+      gre[b] += bgad::adjoint(t, eb);
+      if (remembered > 0)
+        for (int k = 0; k < 13; k++) gm[k] = bgad::adjoint(t, mem[k]);
+    }
   });
   for (int32_t rc : rcs)
     if (rc != BG_OK) return rc;

@@ -17,7 +17,9 @@ name; every random draw comes from numpy's PCG64 with the seed given.
             +-0.2 m; friction 0.6, restitution 0.1; dropped on a walled 100 x 1 x 100 ground.
   batch     worlds of log-uniform 8..512 bodies, each a pyramid, a box stack or a sphere
             pile, friction U(0.3, 0.8), restitution U(0, 0.4).
-  tower     a 3 x 10 tower of 0.5 m cubes struck by a 0.5 m, 50 kg sphere at 5..15 m/s.
+  tower     a 3 x 10 tower of 0.5 m cubes struck by a 0.5 m, 50 kg sphere at 5..15 m/s, with
+            friction U(0.2, 0.9) and restitution U(0, 0.5) for every body; the loss is the
+            squared distance of the cubes' final centres from seeded targets.
 """
 from __future__ import annotations
 
@@ -171,18 +173,41 @@ def batch_world(world, rng):
     return kind, slots
 
 
-def tower(world, rng, targets=None):
-    """The differentiable scene: a 3 x 10 tower of 0.5 m cubes and a 50 kg ball thrown at it."""
+def tower_targets(rng, centres):
+    """The loss's targets for the tower's cubes: each cube's starting centre moved by N(0, 0.1) m
+    on every axis, drawn after the scene's own draws."""
+    centres = np.asarray(centres, dtype=np.float64)
+    return centres + rng.normal(0.0, 0.1, centres.shape)
+
+
+def tower(world, rng):
+    """The differentiable scene: a 3 x 10 tower of 0.5 m cubes and a 50 kg ball thrown at it.
+    Returns the slots and the draws: friction, restitution, speed, the cubes' and the ball's slots,
+    and the loss's targets for the cubes (tower_targets)."""
     mu = float(rng.uniform(0.2, 0.9))
     e = float(rng.uniform(0.0, 0.5))
     speed = float(rng.uniform(5.0, 15.0))
     slots = [world.addBody({"type": "static", "size": (40.0, 1.0, 40.0), "position": (0.0, -0.5, 0.0),
                             "friction": mu, "restitution": e})]
-    cubes = []
+    cubes, centres = [], []
     for layer in range(10):
         for k in range(3):
-            cubes.append(world.addBody({"size": (0.5, 0.5, 0.5), "position": (0.5 * k - 0.5, 0.25 + 0.5 * layer, 0.0),
+            centres.append((0.5 * k - 0.5, 0.25 + 0.5 * layer, 0.0))
+            cubes.append(world.addBody({"size": (0.5, 0.5, 0.5), "position": centres[-1],
                                         "friction": mu, "restitution": e}))
     ball = world.addBody({"shape": "sphere", "radius": 0.5, "mass": 50.0, "friction": mu, "restitution": e,
                           "position": (-0.5, 0.5, -4.0), "velocity": (0.0, 0.0, speed)})
-    return slots + cubes + [ball], dict(friction=mu, restitution=e, speed=speed, cubes=cubes, ball=ball)
+    return slots + cubes + [ball], dict(friction=mu, restitution=e, speed=speed, cubes=cubes, ball=ball,
+                                        targets=tower_targets(rng, centres))
+
+
+def tower_loss(position, info, body0=0):
+    """The tower's loss, the sum over its cubes of the squared distance from each cube's centre to
+    its target, and the loss's adjoint of every position (3 per slot, from slot body0)."""
+    cubes = np.asarray(info["cubes"], dtype=np.int64) + body0
+    idx = (3 * cubes[:, None] + np.arange(3)[None, :])
+    d = position[idx] - info["targets"]
+    seed = np.zeros_like(position)
+    seed[idx] = 2 * d
+    return float(np.sum(d * d)), seed
+

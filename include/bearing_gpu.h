@@ -242,6 +242,63 @@ int32_t bg_block_threads(const bg_ctx* ctx);
 int32_t bg_set_batch_groups(bg_ctx* ctx, int32_t groups);
 
 /*
+ * The adjoint of the solve stage: Bearing itself has no derivatives; this is the backward pass a
+ * differentiable World takes through src/world.js:962-1032.  Given a step's input (the same
+ * structures bg_solve_step takes, for one world or, with `worlds`, a batch) and the adjoints of a
+ * loss with respect to the step's results, it computes the adjoints with respect to the step's
+ * input.  It recomputes the step on the device, recording what each pass read, then sweeps the
+ * passes in reverse, replaying each row and body from its record: the derivative is the one of the
+ * step's own active set (the points each block LCP pushed, the friction cone's Newton rounds, the
+ * clamps that held, the branches of tumble and untwist), so it equals a finite difference wherever
+ * no decision of the step changes.  The recomputed results are written into the step's written
+ * columns as bg_solve_step writes them.
+ *
+ * Results (adjoints of a loss) have the layout of the columns they belong to.  Body seeds and
+ * results: position 3, rotation 4, velocity 3, angular 3, tumbled 3, ceiling 1 per slot; bodies
+ * that do not move (inverse mass 0) are constants of the step, and their results are 0.  Row seeds
+ * (the step's results): normal_impulse 4, tangent_impulse1/2, roll_impulse1/2, spin_impulse,
+ * drift1/2 per row.  Row results (the step's input): the same impulses and drift as carried in,
+ * and normal 3, t1 3, t2 3, friction 1, restitution 1, separation 4, point 12 per row.
+ * Scope: dynamic and static boxes, spheres and capsules, without locks, freezing or joints; other
+ * worlds return BG_EUNSUPPORTED.  Synchronous.
+ */
+typedef struct bg_body_grads {
+  double* position;
+  double* rotation;
+  double* velocity;
+  double* angular;
+  double* tumbled;
+  double* ceiling;
+} bg_body_grads;
+
+typedef struct bg_row_grads {
+  double* normal_impulse;
+  double* tangent_impulse1;
+  double* tangent_impulse2;
+  double* roll_impulse1;
+  double* roll_impulse2;
+  double* spin_impulse;
+  double* drift1;
+  double* drift2;
+  double* normal;              /* results only */
+  double* t1;
+  double* t2;
+  double* friction;
+  double* restitution;
+  double* separation;
+  double* point;
+} bg_row_grads;
+
+int32_t bg_backward(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows, const bg_worlds* worlds,
+                    const bg_step* step, const bg_body_grads* body_seed, const bg_row_grads* row_seed,
+                    bg_body_grads* body_grad, bg_row_grads* row_grad);
+/* The most tape nodes one replay of the last bg_backward recorded (each thread's tape holds
+ * BG_TAPE_NODES), and the device time in milliseconds of its kernel. */
+#define BG_TAPE_NODES 8192
+int32_t bg_backward_tape_peak(const bg_ctx* ctx);
+double bg_backward_ms(bg_ctx* ctx);
+
+/*
  * The solve stage without allocating: no counterpart in the reference.
  *
  * For callers that may not allocate device memory themselves: a host runtime (a game engine's,

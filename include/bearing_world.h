@@ -128,6 +128,37 @@ int32_t bw_batch_row_memory(const bw_batch* batch, bw_row_memory* out);
 bw_world* bw_clone(const bw_world* world);
 int32_t bw_copy(bw_world* dst, const bw_world* src);
 
+/*
+ * The host side's share of a step's adjoint (bg_backward, bearing_gpu.h, is the solve stage's),
+ * for one world or, with `worlds`, a batch laid out as bw_batch_views lays it.  Both run after the
+ * step's bw_begin_step state is known again (the rows, and the bw_row_memory of that step).
+ *
+ * bw_keep_backward: the reverse of keep() (src/contact.js:1091-1115).  From the adjoints of what
+ * each solved row left in its pair's memory (memory_grad, BW_MEMORY per row: normalImpulse[4],
+ * friction[3], twist[3], slip[3]) to those of the row's results: it writes row_grad's impulses
+ * and drift (the seeds bg_backward takes) and adds to row_grad's normal, t1 and t2.
+ *
+ * bw_narrow_backward: the reverse of each row's narrowphase (src/collide.js, for spheres, capsules
+ * and boxes), emit (src/contact.js:889-921), basis (1283-1292) and carry (999-1036).  From the
+ * adjoints of the rows' input (row_grad, as bg_backward leaves them) it adds those of each body's
+ * position (3) and rotation (4) into position_grad / rotation_grad (moving bodies only), those of
+ * each body's friction and restitution (World._friction / _restitution, given per slot in
+ * `friction` / `restitution`) into friction_grad / restitution_grad, and writes those of the
+ * memory each row carried in into memory_grad (BW_MEMORY per row; 0 where nothing was carried).
+ * Returns BG_EFAULT if a row's replayed narrowphase does not find the rows' own points (the step
+ * is not the one the rows came from).  `threads`: host threads over whole worlds.
+ */
+int32_t bw_keep_backward(const bg_rows* rows, const bg_worlds* worlds, const double* memory_grad, bg_row_grads* row_grad);
+int32_t bw_narrow_backward(const bg_bodies* bodies, const bg_rows* rows, const bg_worlds* worlds,
+                           const bw_row_memory* memory, const double* gravity, const double* friction,
+                           const double* restitution, const bg_row_grads* row_grad, double* position_grad,
+                           double* rotation_grad, double* friction_grad, double* restitution_grad, double* memory_grad,
+                           int32_t threads);
+
+/* Each slot's friction and restitution (World._friction, _restitution: what emit() mixes per
+ * pair), copied into arrays of bw_stats.bodies entries. */
+int32_t bw_materials(const bw_world* world, double* friction, double* restitution);
+
 /* World.transforms: 7 floats per slot (position, rotation x y z w). */
 const float* bw_transforms(const bw_world* world);
 int32_t bw_stats_get(const bw_world* world, bw_stats* out);

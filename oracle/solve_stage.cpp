@@ -1535,4 +1535,84 @@ int32_t oracle_dual_pose(const void* h, int32_t slot, double* value, double* tan
   return BG_OK;
 }
 
+// One solve stage in dual numbers along one direction: `B`, `R` and `S` are its input as
+// oracle_solve_step takes it; `dB` and `dR` give, in the same layout, the input's tangent (the
+// columns the stage reads: bodies' position, rotation, velocity, angular, tumbled, ceiling; rows'
+// normal, t1, t2, friction, restitution, separation, point, and the impulses and drift carried
+// in), and receive the tangent of everything the stage writes.  The real parts go into B and R as
+// oracle_solve_step leaves them.  Used to check the adjoint by dot products: for any seed y and
+// direction x, y . (J x) here equals (J^T y) . x from the reverse sweep.
+int32_t oracle_stage_jvp(const bg_bodies* B, const bg_rows* R, const bg_step* S, const bg_bodies* dB, const bg_rows* dR) {
+  const size_t n = static_cast<size_t>(B->capacity), c = static_cast<size_t>(R->count);
+  auto lift = [](const double* v, const double* d, size_t k) {
+    std::vector<D> out(k > 0 ? k : 1);
+    for (size_t i = 0; i < k; i++) {
+      out[i] = D(v[i]);
+      out[i].d[0] = d != nullptr ? d[i] : 0.0;
+    }
+    return out;
+  };
+  std::vector<D> position = lift(B->position, dB->position, 3 * n), rotation = lift(B->rotation, dB->rotation, 4 * n),
+                 velocity = lift(B->velocity, dB->velocity, 3 * n), angular = lift(B->angular, dB->angular, 3 * n),
+                 tumbled = lift(B->tumbled, dB->tumbled, 3 * n), ceiling = lift(B->ceiling, dB->ceiling, n),
+                 start = lift(B->start, nullptr, 3 * n), start_q = lift(B->start_q, nullptr, 4 * n),
+                 inv_i = lift(B->inv_i, nullptr, 6 * n);
+  std::vector<D> normal = lift(R->normal, dR->normal, 3 * c), t1 = lift(R->t1, dR->t1, 3 * c),
+                 t2 = lift(R->t2, dR->t2, 3 * c), friction = lift(R->friction, dR->friction, c),
+                 restitution = lift(R->restitution, dR->restitution, c),
+                 separation = lift(R->separation, dR->separation, P * c), point = lift(R->point, dR->point, 3 * P * c),
+                 ni = lift(R->normal_impulse, dR->normal_impulse, P * c),
+                 ti1 = lift(R->tangent_impulse1, dR->tangent_impulse1, c),
+                 ti2 = lift(R->tangent_impulse2, dR->tangent_impulse2, c),
+                 ri1 = lift(R->roll_impulse1, dR->roll_impulse1, c), ri2 = lift(R->roll_impulse2, dR->roll_impulse2, c),
+                 si = lift(R->spin_impulse, dR->spin_impulse, c), drift1 = lift(R->drift1, dR->drift1, c),
+                 drift2 = lift(R->drift2, dR->drift2, c), gap = lift(R->gap, nullptr, c),
+                 maxni = lift(R->max_normal_impulse, nullptr, P * c), relvel = lift(R->relative_velocity, nullptr, P * c),
+                 anchor_a = lift(R->anchor_a, nullptr, 3 * c), anchor_b = lift(R->anchor_b, nullptr, 3 * c);
+  BodiesT<D> DB;
+  DB.capacity = B->capacity; DB.awake_count = B->awake_count; DB.awake_list = B->awake_list; DB.awake = B->awake;
+  DB.position = position.data(); DB.rotation = rotation.data(); DB.velocity = velocity.data();
+  DB.angular = angular.data(); DB.tumbled = tumbled.data(); DB.ceiling = ceiling.data();
+  DB.start = start.data(); DB.start_q = start_q.data(); DB.inv_i = inv_i.data();
+  DB.inv_mass = B->inv_mass; DB.inertia = B->inertia; DB.inv_inertia = B->inv_inertia; DB.dims = B->dims;
+  DB.damping = B->damping; DB.angular_damping = B->angular_damping; DB.gravity_scale = B->gravity_scale;
+  DB.type = B->type; DB.shape = B->shape; DB.frozen = B->frozen; DB.framed = B->framed; DB.lock = B->lock;
+  DB.joint_head = B->joint_head;
+  RowsT<D> DR;
+  DR.count = R->count; DR.solved = R->solved;
+  for (int k = 0; k < BG_STARTS; k++) DR.starts[k] = R->starts[k];
+  DR.row = R->row; DR.a = R->a; DR.b = R->b; DR.points = R->points;
+  DR.normal = normal.data(); DR.t1 = t1.data(); DR.t2 = t2.data(); DR.friction = friction.data();
+  DR.restitution = restitution.data(); DR.tolerance = R->tolerance; DR.patch = R->patch;
+  DR.separation = separation.data(); DR.point = point.data(); DR.shift = R->shift;
+  DR.normal_impulse = ni.data(); DR.tangent_impulse1 = ti1.data(); DR.tangent_impulse2 = ti2.data();
+  DR.roll_impulse1 = ri1.data(); DR.roll_impulse2 = ri2.data(); DR.spin_impulse = si.data();
+  DR.drift1 = drift1.data(); DR.drift2 = drift2.data(); DR.gap = gap.data(); DR.max_normal_impulse = maxni.data();
+  DR.relative_velocity = relvel.data(); DR.sliding = R->sliding; DR.anchor_a = anchor_a.data();
+  DR.anchor_b = anchor_b.data();
+  {
+    Stage<D> stage(DB, DR, nullptr);
+    stage.run(*S);
+  }
+  auto drop = [](double* v, double* d, const std::vector<D>& src, size_t k) {
+    for (size_t i = 0; i < k; i++) {
+      if (v != nullptr) v[i] = src[i].v;
+      if (d != nullptr) d[i] = src[i].d[0];
+    }
+  };
+  drop(B->position, dB->position, position, 3 * n); drop(B->rotation, dB->rotation, rotation, 4 * n);
+  drop(B->velocity, dB->velocity, velocity, 3 * n); drop(B->angular, dB->angular, angular, 3 * n);
+  drop(B->tumbled, dB->tumbled, tumbled, 3 * n); drop(B->ceiling, dB->ceiling, ceiling, n);
+  drop(B->start, dB->start, start, 3 * n); drop(B->start_q, dB->start_q, start_q, 4 * n);
+  drop(B->inv_i, dB->inv_i, inv_i, 6 * n);
+  drop(R->normal_impulse, dR->normal_impulse, ni, P * c); drop(R->tangent_impulse1, dR->tangent_impulse1, ti1, c);
+  drop(R->tangent_impulse2, dR->tangent_impulse2, ti2, c); drop(R->roll_impulse1, dR->roll_impulse1, ri1, c);
+  drop(R->roll_impulse2, dR->roll_impulse2, ri2, c); drop(R->spin_impulse, dR->spin_impulse, si, c);
+  drop(R->drift1, dR->drift1, drift1, c); drop(R->drift2, dR->drift2, drift2, c); drop(R->gap, dR->gap, gap, c);
+  drop(R->max_normal_impulse, dR->max_normal_impulse, maxni, P * c);
+  drop(R->relative_velocity, dR->relative_velocity, relvel, P * c);
+  drop(R->anchor_a, dR->anchor_a, anchor_a, 3 * c); drop(R->anchor_b, dR->anchor_b, anchor_b, 3 * c);
+  return BG_OK;
+}
+
 }  // extern "C"
