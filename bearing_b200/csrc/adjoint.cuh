@@ -1066,8 +1066,11 @@ AHD void replay_pass_row(const AdjParams& A, const AdjWorld& W, int m, int pass,
   leaves(L.normal, r.normal, 3); leaves(L.t1, r.t1, 3); leaves(L.t2, r.t2, 3);
   L.friction = bgad::leaf(r.friction[0]);
   L.drift1 = bgad::leaf(A.in_drift1[m]); L.drift2 = bgad::leaf(A.in_drift2[m]);
-  RowLeaves O = L;   // the row works on O: its results replace O's entries, L keeps the leaves
-  const RowIO<TV> o = leaf_io(O, r);
+  // The row overwrites its bodies' velocities and its state in L: keep the leaves it reads there.
+  TV in_v[12], in_st[RSTATE];
+  for (int c = 0; c < 3; c++) { in_v[c] = L.va[c]; in_v[3 + c] = L.wa[c]; in_v[6 + c] = L.vb[c]; in_v[9 + c] = L.wb[c]; }
+  for (int k = 0; k < RSTATE; k++) in_st[k] = L.st[k];
+  const RowIO<TV> o = leaf_io(L, r);
   if (kind == WARM) warm_row(o);
   else solve_row(o, h, kind == SOLVE, kind == SOLVE && sub > 0, A.soft);
   if (t->overflow) {
@@ -1077,17 +1080,17 @@ AHD void replay_pass_row(const AdjParams& A, const AdjWorld& W, int m, int pass,
   bgad::clear_adjoints(t);
   const bool ma = moving(A, a), mb = moving(A, b);
   for (int c = 0; c < 3; c++) {
-    if (ma) { bgad::seed(t, O.va[c], A.bv[3 * a + c]); bgad::seed(t, O.wa[c], A.bw[3 * a + c]); }
-    if (mb) { bgad::seed(t, O.vb[c], A.bv[3 * b + c]); bgad::seed(t, O.wb[c], A.bw[3 * b + c]); }
+    if (ma) { bgad::seed(t, L.va[c], A.bv[3 * a + c]); bgad::seed(t, L.wa[c], A.bw[3 * a + c]); }
+    if (mb) { bgad::seed(t, L.vb[c], A.bv[3 * b + c]); bgad::seed(t, L.wb[c], A.bw[3 * b + c]); }
   }
   double* bst = A.bst + RSTATE * static_cast<int64_t>(m);
-  for (int k = 0; k < RSTATE; k++) bgad::seed(t, O.st[k], bst[k]);
+  for (int k = 0; k < RSTATE; k++) bgad::seed(t, L.st[k], bst[k]);
   bgad::sweep(t);
   // results: the state and velocities it read replace the adjoints of what it wrote; everything
   // else it read adds to its adjoint
-  set_adjoints(bst, t, L.st, RSTATE);
-  if (ma) { set_adjoints(A.bv + 3 * a, t, L.va, 3); set_adjoints(A.bw + 3 * a, t, L.wa, 3); }
-  if (mb) { set_adjoints(A.bv + 3 * b, t, L.vb, 3); set_adjoints(A.bw + 3 * b, t, L.wb, 3); }
+  set_adjoints(bst, t, in_st, RSTATE);
+  if (ma) { set_adjoints(A.bv + 3 * a, t, in_v, 3); set_adjoints(A.bw + 3 * a, t, in_v + 3, 3); }
+  if (mb) { set_adjoints(A.bv + 3 * b, t, in_v + 6, 3); set_adjoints(A.bw + 3 * b, t, in_v + 9, 3); }
   if (reads_pose) {
     if (ma) {
       add_adjoints(A.bp + 3 * a, t, L.pa, 3); add_adjoints(A.bq + 4 * a, t, L.qa, 4);
@@ -1170,19 +1173,19 @@ AHD void reverse(const AdjParams& A, const AdjWorld& W, const Lane& lane) {
       leaves(L.pr + PR_ANA, r.pr + PR_ANA, 6);
       leaves(L.t1, r.t1, 3); leaves(L.t2, r.t2, 3);
       L.drift1 = bgad::leaf(A.in_drift1[m]); L.drift2 = bgad::leaf(A.in_drift2[m]);
-      RowLeaves O = L;
-      const RowIO<TV> o = leaf_io(O, r);
-      slipped_row(o, O.qa0, O.qb0, A.awake[a] != 0, A.awake[b] != 0);
+      const TV in_d1 = L.drift1, in_d2 = L.drift2;   // slipped() overwrites them in L
+      const RowIO<TV> o = leaf_io(L, r);
+      slipped_row(o, L.qa0, L.qb0, A.awake[a] != 0, A.awake[b] != 0);
       if (t->overflow) {
         *A.status = 1;
         return;
       }
       bgad::clear_adjoints(t);
-      bgad::seed(t, O.drift1, A.bdrift1[m]);
-      bgad::seed(t, O.drift2, A.bdrift2[m]);
+      bgad::seed(t, L.drift1, A.bdrift1[m]);
+      bgad::seed(t, L.drift2, A.bdrift2[m]);
       bgad::sweep(t);
-      A.bdrift1[m] = bgad::adjoint(t, L.drift1);
-      A.bdrift2[m] = bgad::adjoint(t, L.drift2);
+      A.bdrift1[m] = bgad::adjoint(t, in_d1);
+      A.bdrift2[m] = bgad::adjoint(t, in_d2);
       if (moving(A, a)) {
         add_adjoints(A.bp + 3 * a, t, L.pa, 3); add_adjoints(A.bq + 4 * a, t, L.qa, 4);
         add_adjoints(A.bstart + 3 * a, t, L.sa, 3); add_adjoints(A.bstartq + 4 * a, t, L.qa0, 4);
@@ -1223,8 +1226,10 @@ AHD void reverse(const AdjParams& A, const AdjWorld& W, const Lane& lane) {
         leaves(L.pr, r.pr, PREP);
         leaves(L.normal, r.normal, 3);
         L.restitution = bgad::leaf(r.restitution[0]);
-        RowLeaves O = L;
-        const RowIO<TV> o = leaf_io(O, r);
+        TV in_v[12], in_ni[P];   // bounce_row() overwrites these in L
+        for (int c = 0; c < 3; c++) { in_v[c] = L.va[c]; in_v[3 + c] = L.wa[c]; in_v[6 + c] = L.vb[c]; in_v[9 + c] = L.wb[c]; }
+        for (int k = 0; k < P; k++) in_ni[k] = L.st[RS_NI + k];
+        const RowIO<TV> o = leaf_io(L, r);
         bounce_row(o, gravity);
         if (t->overflow) {
           *A.status = 1;
@@ -1233,15 +1238,15 @@ AHD void reverse(const AdjParams& A, const AdjWorld& W, const Lane& lane) {
         bgad::clear_adjoints(t);
         const bool ma = moving(A, a), mb = moving(A, b);
         for (int c = 0; c < 3; c++) {
-          if (ma) { bgad::seed(t, O.va[c], A.bv[3 * a + c]); bgad::seed(t, O.wa[c], A.bw[3 * a + c]); }
-          if (mb) { bgad::seed(t, O.vb[c], A.bv[3 * b + c]); bgad::seed(t, O.wb[c], A.bw[3 * b + c]); }
+          if (ma) { bgad::seed(t, L.va[c], A.bv[3 * a + c]); bgad::seed(t, L.wa[c], A.bw[3 * a + c]); }
+          if (mb) { bgad::seed(t, L.vb[c], A.bv[3 * b + c]); bgad::seed(t, L.wb[c], A.bw[3 * b + c]); }
         }
         double* bst = A.bst + RSTATE * static_cast<int64_t>(m);
-        for (int k = 0; k < P; k++) bgad::seed(t, O.st[RS_NI + k], bst[RS_NI + k]);
+        for (int k = 0; k < P; k++) bgad::seed(t, L.st[RS_NI + k], bst[RS_NI + k]);
         bgad::sweep(t);
-        if (ma) { set_adjoints(A.bv + 3 * a, t, L.va, 3); set_adjoints(A.bw + 3 * a, t, L.wa, 3); }
-        if (mb) { set_adjoints(A.bv + 3 * b, t, L.vb, 3); set_adjoints(A.bw + 3 * b, t, L.wb, 3); }
-        set_adjoints(bst + RS_NI, t, L.st + RS_NI, P);
+        if (ma) { set_adjoints(A.bv + 3 * a, t, in_v, 3); set_adjoints(A.bw + 3 * a, t, in_v + 3, 3); }
+        if (mb) { set_adjoints(A.bv + 3 * b, t, in_v + 6, 3); set_adjoints(A.bw + 3 * b, t, in_v + 9, 3); }
+        set_adjoints(bst + RS_NI, t, in_ni, P);
         add_adjoints(bst + RS_RELVEL, t, L.st + RS_RELVEL, P);
         add_adjoints(A.bpr + PREP * static_cast<int64_t>(m), t, L.pr, PREP);
         add_adjoints(A.bnormal + 3 * m, t, L.normal, 3);
@@ -1321,8 +1326,7 @@ AHD void reverse(const AdjParams& A, const AdjWorld& W, const Lane& lane) {
       leaves(L.ia, r.ia, 6); leaves(L.ib, r.ib, 6);
       leaves(L.normal, r.normal, 3); leaves(L.t1, r.t1, 3); leaves(L.t2, r.t2, 3);
       leaves(L.separation, r.separation, P); leaves(L.point, r.point, 3 * P);
-      RowLeaves O = L;
-      const RowIO<TV> o = leaf_io(O, r);
+      const RowIO<TV> o = leaf_io(L, r);   // it writes only pr and st, which it does not read
       prepare_row(o);
       if (t->overflow) {
         *A.status = 1;
@@ -1330,9 +1334,9 @@ AHD void reverse(const AdjParams& A, const AdjWorld& W, const Lane& lane) {
       }
       bgad::clear_adjoints(t);
       const double* bpr = A.bpr + PREP * static_cast<int64_t>(m);
-      for (int k = 0; k < PREP; k++) bgad::seed(t, O.pr[k], bpr[k]);
+      for (int k = 0; k < PREP; k++) bgad::seed(t, L.pr[k], bpr[k]);
       const double* bst = A.bst + RSTATE * static_cast<int64_t>(m);
-      for (int k = 0; k < P; k++) bgad::seed(t, O.st[RS_RELVEL + k], bst[RS_RELVEL + k]);
+      for (int k = 0; k < P; k++) bgad::seed(t, L.st[RS_RELVEL + k], bst[RS_RELVEL + k]);
       bgad::sweep(t);
       if (moving(A, a)) {
         add_adjoints(A.bp + 3 * a, t, L.pa, 3); add_adjoints(A.bq + 4 * a, t, L.qa, 4);

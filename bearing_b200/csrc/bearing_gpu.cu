@@ -1963,7 +1963,8 @@ int32_t bg_backward(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_wo
       set_error(c, "bg_backward: slot %d is kinematic, locked, frozen, jointed or not a box, sphere or capsule", s);
       return BG_EUNSUPPORTED;
     }
-  const size_t threads = static_cast<size_t>(std::min(nw, 4 * c->sms)) * kAdjointThreads;
+  // One warp a world, every world at once up to 16 a streaming multiprocessor (more loop).
+  const size_t threads = static_cast<size_t>(std::min(nw, 16 * c->sms)) * kAdjointThreads;
   if (!adj_ensure(c, static_cast<size_t>(nb), static_cast<size_t>(nr), static_cast<size_t>(na), static_cast<size_t>(nw),
                   S->substeps, threads))
     return BG_ENOMEM;

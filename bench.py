@@ -51,8 +51,11 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--resident-only", action="store_true", help="time the resident solve only (for profiling)")
     p.add_argument("--batch-worlds", type=int, default=4096, help="worlds in the batched-worlds measurement")
-    p.add_argument("--batch-at", type=int, default=60, help="steps the batch takes before its timed solve stage")
+    p.add_argument("--batch-at", type=int, default=300, help="steps the batch takes before its timed solve stage")
     p.add_argument("--no-batch", action="store_true", help="skip the batched-worlds measurement")
+    p.add_argument("--adjoint-worlds", type=int, default=1024, help="towers in the backward-pass measurement")
+    p.add_argument("--adjoint-steps", type=int, default=120)
+    p.add_argument("--no-adjoint", action="store_true", help="skip the backward-pass measurement")
     return p.parse_args()
 
 
@@ -196,12 +199,12 @@ def time_resident(lib, ctx, copy, steps, warmup, torch):
     return times, stage, launches, out
 
 
-def time_e2e(lib, ctx, copy, steps, warmup, torch):
+def time_e2e(lib, ctx, copy, steps, warmup, torch, pinned=True):
     """bg_solve_step with host arrays in page-locked memory (as a World that keeps its columns
-    pinned passes them): uploads, solve and downloads inside the timed region.  The arrays are
-    refilled with the step's input, untimed, before every call."""
+    pinned passes them), or in ordinary pageable memory: uploads, solve and downloads inside the
+    timed region.  The arrays are refilled with the step's input, untimed, before every call."""
     stream = torch.cuda.ExternalStream(lib.bg_stream(ctx))
-    work = copy.pinned()
+    work = copy.pinned() if pinned else copy.copy()
     times = []
     for i in range(warmup + steps):
         work.fill(copy)
@@ -330,9 +333,21 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
     batched_locked = batched_e2e(base.pinned())
     work = base.copy()
     batched = batched_e2e(work)
-    # the plain path, world by world
+    # the plain path, world by world: each world's solve stage with its input resident (uploaded
+    # untimed, events around bg_solve), summed over the worlds
     parts = [base.world(i) for i in range(base.worlds)]
     one = lib.bg_create(device, 0)
+    one_stream = torch.cuda.ExternalStream(lib.bg_stream(one))
+    loop_resident = 0.0
+    for p in parts:
+        Bw, Rw, Sw = p.views()
+        assert lib.bg_upload(one, C.byref(Bw), C.byref(Rw)) == 0, lib.bg_last_error(one)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(one_stream)
+        assert lib.bg_solve(one, C.byref(Sw)) == 0, lib.bg_last_error(one)
+        e1.record(one_stream)
+        e1.synchronize()
+        loop_resident += e0.elapsed_time(e1)
     loop = []
     for i in range(2):
         outs = [p.copy() for p in parts]
@@ -349,13 +364,14 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
     batch.destroy()
     ms_res, ms_bat, ms_loop = statistics.mean(resident), statistics.mean(batched), min(loop)
     ms_lock = statistics.mean(batched_locked)
+    ms_loop_res = loop_resident
     algo = batch_algorithmic_bytes(base)   # this rank's worlds
     slots, rows = int(base.stage.capacity), int(base.stage.count)
     solved = int(sum(int(base.starts[k * 35 + 33]) for k in range(base.worlds)))
     if dist:
-        t = torch.tensor([ms_res, ms_bat, ms_loop, ms_lock], device="cuda", dtype=torch.float64)
+        t = torch.tensor([ms_res, ms_bat, ms_loop, ms_lock, ms_loop_res], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_res, ms_bat, ms_loop, ms_lock = (float(x) for x in t.tolist())
+        ms_res, ms_bat, ms_loop, ms_lock, ms_loop_res = (float(x) for x in t.tolist())
         t = torch.tensor([slots, rows, solved, 0 if same else 1], device="cuda", dtype=torch.int64)
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         slots, rows, solved, unequal = (int(x) for x in t.tolist())
@@ -369,8 +385,60 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
             "batched_e2e": {"value": n / (ms_bat / 1000), "ms_per_step": ms_bat, "host_memory": "pageable"},
             "batched_e2e_page_locked": {"value": n / (ms_lock / 1000), "ms_per_step": ms_lock},
             "per_world_loop_e2e": {"value": n / (ms_loop / 1000), "ms_per_step": ms_loop},
-            "speedup_e2e": ms_loop / ms_bat, "bit_identical": same, "cta_threads": cta_threads,
+            "per_world_loop_resident": {"value": n / (ms_loop_res / 1000), "ms_per_step": ms_loop_res,
+                                        "how": "sum over the worlds of bg_solve with that world's input resident"},
+            "speedup_e2e": ms_loop / ms_bat, "speedup_resident": ms_loop_res / ms_res,
+            "bit_identical": same, "cta_threads": cta_threads,
             "roofline": batch_roofline(algo, ms_res, cta_threads)}
+
+
+def measure_adjoint(args, device, log):
+    """The differentiable workload: `adjoint_worlds` towers struck by a ball (scenes.tower), stepped
+    `adjoint_steps` times as one batch with a checkpoint every 20 steps, then the backward pass: the
+    gradient of each tower's loss with respect to its friction, restitution and launch velocity
+    (bearing_b200.adjoint.tower_gradients).  Timed end to end on the host clock (the forward steps,
+    then the backward pass: recomputing each 20-step segment, the host's reverse and bg_backward);
+    the adjoint kernels' own device time beside it.  CPU baseline: the oracle's dual-number run of
+    a sample of the same towers (five directions at once: one forward pass gives the same five
+    derivatives), on one thread."""
+    from bearing_b200 import adjoint, scenes
+    from bearing_b200.world import World
+    import numpy as np
+    import oracle_io
+    n, steps = args.adjoint_worlds, args.adjoint_steps
+    t0 = time.perf_counter()
+    out = adjoint.tower_gradients(n, seed=5000, steps=steps, checkpoint=20, device=device)
+    wall = time.perf_counter() - t0
+    if log:
+        log(f"adjoint: {n} towers x {steps} steps: forward {out['forward_s']:.1f} s, backward "
+            f"{out['backward_s']:.1f} s ({out['device_ms'] / 1000:.1f} s in the adjoint kernels)")
+    sample = 2
+    tc = time.perf_counter()
+    worst = 0.0
+    for i in range(sample):
+        w = World({}, solver=oracle_io.solver(0))
+        _, info = scenes.tower(w, scenes.batch_rng(5000, i))
+        dual = oracle_io.DualWorld(w, info["friction"], info["restitution"], info["ball"])
+        for _ in range(steps):
+            dual.step(DT)
+        g = np.zeros(5)
+        for s, t in zip(info["cubes"], info["targets"]):
+            v, tan = dual.pose(s)
+            g += 2 * (v[:3] - t) @ tan[:3]
+        dual.close()
+        w.destroy()
+        worst = max(worst, float(np.max(np.abs(out["gradients"][i] - g)) / np.max(np.abs(g))))
+    cpu_s = (time.perf_counter() - tc) / sample
+    return {"workload": f"{n} towers (3 x 10 cubes of 0.5 m) struck by a 50 kg ball, {steps} steps, "
+                        f"checkpoint every 20 steps; gradients of each tower's loss w.r.t. friction, "
+                        f"restitution and the launch velocity",
+            "unit": "tower-gradients/s", "value": n / (out["forward_s"] + out["backward_s"]),
+            "forward_s": out["forward_s"], "backward_s": out["backward_s"], "wall_s": wall,
+            "adjoint_kernel_s": out["device_ms"] / 1000, "tape_peak_nodes": out["tape_peak"],
+            "check": {"worlds": sample, "max_rel_err_vs_dual_numbers": worst},
+            "cpu_baseline": {"value": 1 / cpu_s, "unit": "tower-gradients/s", "cores": 1, "kind": "port",
+                             "sample": f"{sample} towers' dual-number runs (the oracle, 5 directions) on one "
+                                       f"thread"}}
 
 
 def batch_roofline(algo, ms, cta_threads):
@@ -489,14 +557,17 @@ def main():
     times, stage, launches, out = time_resident(lib, ctx, copy, args.steps, args.warmup, torch)
     clock = clocks.stop()
     e2e_times = times if args.resident_only else time_e2e(lib, ctx, copy, args.steps, args.warmup, torch)
+    pageable_times = times if args.resident_only else time_e2e(lib, ctx, copy, args.steps, args.warmup, torch,
+                                                                pinned=False)
     torch.cuda.synchronize()
     ms = statistics.mean(times)
     ms_e2e = statistics.mean(e2e_times)
+    ms_pageable = statistics.mean(pageable_times)
     ms_stage = statistics.mean(stage)
     if dist:
-        t = torch.tensor([ms, ms_e2e, ms_stage], device="cuda", dtype=torch.float64)
+        t = torch.tensor([ms, ms_e2e, ms_stage, ms_pageable], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e, ms_stage = (float(x) for x in t.tolist())
+        ms, ms_e2e, ms_stage, ms_pageable = (float(x) for x in t.tolist())
     rows_per_stage = copy.solved * SUBSTEPS * 3
     value = world_size * rows_per_stage / (ms / 1000)
     e2e = world_size * rows_per_stage / (ms_e2e / 1000)
@@ -516,6 +587,9 @@ def main():
     batch = None
     if not args.no_batch and not args.resident_only:   # every rank, or none: it holds collectives
         batch = measure_batch(args, lib, torch, local, log, rank, world_size, dist)
+    adj = None
+    if not args.no_adjoint and not args.resident_only and rank == 0 and world_size == 1:
+        adj = measure_adjoint(args, local, log)
     if rank == 0:
         line = {"metric": "contact rows/s", "value": value, "unit": "rows/s", "n_gpus": world_size,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -525,11 +599,13 @@ def main():
                                overflow=int(copy.starts[33] - copy.starts[32]), awake=copy.awake_count),
                 "e2e": {"value": e2e, "unit": "rows/s", "ms_per_step": ms_e2e, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "host_memory": "page-locked"},
+                "e2e_pageable": {"value": world_size * rows_per_stage / (ms_pageable / 1000), "unit": "rows/s",
+                                 "ms_per_step": ms_pageable, "host_memory": "pageable (ordinary numpy arrays)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": measured_traffic(args.bodies, algo),
                              "traffic_source": "ncu capture at step 101, scaled by algorithmic bytes", "kernel_ms": ms_stage,
                              "algorithmic_bytes": algo, "peak_source": peak_source},
-                "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches, "batch": batch}
+                "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches, "batch": batch, "adjoint": adj}
         print(json.dumps(line), flush=True)
     lib.bg_destroy(ctx)
     solver.close()

@@ -294,7 +294,7 @@ int32_t bg_backward(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows, c
                     bg_body_grads* body_grad, bg_row_grads* row_grad);
 /* The most tape nodes one replay of the last bg_backward recorded (each thread's tape holds
  * BG_TAPE_NODES), and the device time in milliseconds of its kernel. */
-#define BG_TAPE_NODES 8192
+#define BG_TAPE_NODES 4096
 int32_t bg_backward_tape_peak(const bg_ctx* ctx);
 double bg_backward_ms(bg_ctx* ctx);
 
