@@ -154,6 +154,19 @@ class RowMemory(C.Structure):
 BW_MEMORY = 16
 
 
+class Pairs(C.Structure):
+    """bg_pairs: the pairs narrow() hands to collide(), with their margins and tolerances."""
+
+    _fields_ = [("count", C.c_int32), ("a", _i32), ("b", _i32), ("margin", _d), ("tolerance", _d)]
+
+
+class Manifolds(C.Structure):
+    """bg_manifolds: one manifold a pair (points 0..BG_POINTS)."""
+
+    _fields_ = [("points", _u8), ("normal", _d), ("point", _d), ("separation", _d),
+                ("pid", C.POINTER(C.c_uint32))]
+
+
 class Options(C.Structure):
     _fields_ = [("gravity", C.c_double * 3), ("substeps", C.c_int32)]
 
@@ -242,10 +255,12 @@ def host() -> C.CDLL:
         lib.bw_clone.restype = C.c_void_p
         lib.bw_clone.argtypes = [C.c_void_p]
         lib.bw_copy.argtypes = [C.c_void_p, C.c_void_p]
+        lib.bw_narrow_pairs.argtypes = [C.c_void_p, C.POINTER(Pairs)]
+        lib.bw_collide_pairs.argtypes = [C.POINTER(Bodies), _d, C.POINTER(Pairs), C.POINTER(Manifolds), C.c_int32]
         for f in ("bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step", "bw_end_step",
                   "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_stats_get", "bw_batch_begin_step",
                   "bw_batch_views", "bw_batch_end_step", "bw_row_memory_get", "bw_batch_row_memory", "bw_copy",
-                  "bw_keep_backward", "bw_narrow_backward", "bw_materials"):
+                  "bw_keep_backward", "bw_narrow_backward", "bw_materials", "bw_narrow_pairs", "bw_collide_pairs"):
             getattr(lib, f).restype = C.c_int32
         _host = lib
     return _host
@@ -278,6 +293,16 @@ def gpu() -> C.CDLL:
         lib.bg_batch_download.argtypes = three
         lib.bg_stream.restype = C.c_void_p
         lib.bg_stream.argtypes = [C.c_void_p]
+        lib.bg_register_host.argtypes = three + [C.c_int32]
+        lib.bg_register_host.restype = C.c_int32
+        lib.bg_unregister_host.argtypes = [C.c_void_p]
+        lib.bg_unregister_host.restype = C.c_int32
+        lib.bg_registered_bytes.argtypes = [C.c_void_p]
+        lib.bg_registered_bytes.restype = C.c_int64
+        lib.bg_collide.argtypes = [C.c_void_p, C.POINTER(Bodies), _d, C.POINTER(Pairs), C.POINTER(Manifolds)]
+        lib.bg_collide.restype = C.c_int32
+        lib.bg_last_collide_ms.argtypes = [C.c_void_p]
+        lib.bg_last_collide_ms.restype = C.c_double
         lib.bg_last_launches.argtypes = [C.c_void_p]
         lib.bg_set_wait_budget.argtypes = [C.c_void_p, C.c_int64]
         lib.bg_last_stage_ms.argtypes = [C.c_void_p]
@@ -311,12 +336,13 @@ GPU_SYMBOLS = [
     "bg_solve", "bg_download", "bg_batch_solve_step", "bg_batch_upload", "bg_batch_solve",
     "bg_batch_download", "bg_stream", "bg_last_launches", "bg_last_stage_ms", "bg_set_wait_budget", "bg_set_block_threads",
     "bg_block_threads", "bg_set_batch_groups", "bg_backward", "bg_backward_tape_peak", "bg_backward_ms",
-    "bg_solve_step_static",
+    "bg_solve_step_static", "bg_register_host", "bg_unregister_host", "bg_registered_bytes", "bg_collide",
+    "bg_last_collide_ms",
 ]
 HOST_SYMBOLS = [
     "bw_create", "bw_destroy", "bw_last_error", "bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step",
     "bw_end_step", "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_transforms", "bw_stats_get",
     "bw_batch_create", "bw_batch_destroy", "bw_batch_begin_step", "bw_batch_views", "bw_batch_end_step",
     "bw_row_memory_get", "bw_batch_row_memory", "bw_clone", "bw_copy", "bw_keep_backward", "bw_narrow_backward",
-    "bw_materials",
+    "bw_materials", "bw_narrow_pairs", "bw_collide_pairs",
 ]

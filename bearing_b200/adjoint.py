@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import time
 
 import numpy as np
 
@@ -98,14 +99,19 @@ class _Record:
         self.out = {f: np.ctypeslib.as_array(getattr(R, f), shape=(k[f] * self.nr,)).copy() if self.nr else
                     np.zeros(1) for f in self.KEPT}
 
-    def views(self, results=False):
-        """bg_bodies / bg_rows / bg_worlds / bg_step over copies of the record's arrays (the solve
-        stage's reverse writes its recomputed results into them); with `results`, the rows carry
-        the step's results where keep() reads them."""
-        body = {f: v.copy() for f, v in self.body.items()}
-        rows = {f: v.copy() for f, v in self.rows.items()}
+    # What the solve stage's reverse writes (the recomputed step's results), per bg_bodies / bg_rows.
+    WRITTEN_BODY = ("position", "rotation", "velocity", "angular", "tumbled", "ceiling", "start", "start_q", "inv_i")
+    WRITTEN_ROW = KEPT + ("gap", "max_normal_impulse", "relative_velocity", "sliding", "anchor_a", "anchor_b")
+
+    def views(self, results=False, writable=False):
+        """bg_bodies / bg_rows / bg_worlds / bg_step over the record's arrays: with `writable`, over
+        copies of the columns the solve stage's reverse writes its recomputed results into (the
+        rest are only read, and shared); with `results`, the rows carry the step's results where
+        keep() reads them."""
+        body = {f: v.copy() if writable and f in self.WRITTEN_BODY else v for f, v in self.body.items()}
+        rows = {f: v.copy() if writable and f in self.WRITTEN_ROW else v for f, v in self.rows.items()}
         if results:
-            rows.update({f: v.copy() for f, v in self.out.items()})
+            rows.update(self.out)
         keep = [body, rows]
         B, R, W = _ffi.Bodies(), _ffi.Rows(), _ffi.Worlds()
         B.capacity, B.awake_count = self.nb, self.na
@@ -177,6 +183,8 @@ class BatchBackward:
         self.gravity = np.zeros(3)
         self.device_ms = 0.0
         self.tape_peak = 0
+        # host seconds of the backward pass, by part (bg_backward's is its wall time, kernel included)
+        self.times = {"recompute": 0.0, "keep_backward": 0.0, "stage_backward": 0.0, "narrow_backward": 0.0}
 
     def close(self):
         if self.batch:
@@ -218,6 +226,7 @@ class BatchBackward:
             self._step()
 
     def _reverse_step(self, rec, bar, mem_next, grad_fr, grad_re):
+        t0 = time.perf_counter()
         nr = rec.nr
         mem_after = np.zeros(_ffi.BW_MEMORY * max(nr, 1))
         keys = rec.keys()
@@ -235,7 +244,8 @@ class BatchBackward:
         seed = Grads("row", nr)
         if self.host.bw_keep_backward(C.byref(R), C.byref(W), mem_after.ctypes.data_as(_PD), C.byref(seed.s)) != 0:
             raise RuntimeError("bw_keep_backward failed")
-        B, R, W, S, keep = rec.views()
+        t1 = time.perf_counter()
+        B, R, W, S, keep = rec.views(writable=True)
         body_grad, row_grad = Grads("body", self.nb), Grads("row", nr)
         rc = self.gpu.bg_backward(self.ctx, C.byref(B), C.byref(R), C.byref(W), C.byref(S), C.byref(bar.s),
                                   C.byref(seed.s), C.byref(body_grad.s), C.byref(row_grad.s))
@@ -245,6 +255,7 @@ class BatchBackward:
         self.tape_peak = max(self.tape_peak, self.gpu.bg_backward_tape_peak(self.ctx))
         for f in ("normal", "t1", "t2"):   # keep() read these too
             row_grad[f][: 3 * nr] += seed[f][: 3 * nr]
+        t2 = time.perf_counter()
         B, R, W, S, keep = rec.views()   # the step's input, untouched
         mem_before = np.zeros(_ffi.BW_MEMORY * max(nr, 1))
         rc = self.host.bw_narrow_backward(C.byref(B), C.byref(R), C.byref(W), C.byref(rec.mem.s),
@@ -255,6 +266,10 @@ class BatchBackward:
                                           grad_re.ctypes.data_as(_PD), mem_before.ctypes.data_as(_PD), self.threads)
         if rc != 0:
             raise RuntimeError(f"bw_narrow_backward: {rc}")
+        t3 = time.perf_counter()
+        self.times["keep_backward"] += t1 - t0
+        self.times["stage_backward"] += t2 - t1
+        self.times["narrow_backward"] += t3 - t2
         return body_grad, (keys, mem_before[: _ffi.BW_MEMORY * nr])
 
     def backward(self, seed):
@@ -273,7 +288,9 @@ class BatchBackward:
             for c0 in sorted(self.checkpoints, reverse=True):
                 for w, snap in zip(self.worlds, self.checkpoints[c0]):
                     self.host.bw_copy(w._w, snap)
+                t0 = time.perf_counter()
                 recs = [self._step(record=True) for _ in range(c0, min(c0 + self.checkpoint, self.steps))]
+                self.times["recompute"] += time.perf_counter() - t0
                 for rec in reversed(recs):
                     bar, mem_next = self._reverse_step(rec, bar, mem_next, grad_fr, grad_re)
         finally:
@@ -293,8 +310,6 @@ def tower_gradients(count, seed=5000, steps=120, dt=1 / 60, checkpoint=20, first
     of each tower's loss (scenes.tower_loss) with respect to its friction, its restitution and the
     ball's launch velocity (3).  Returns a dict: gradients (count x 5), losses, the final positions,
     and timings (forward and backward seconds, the adjoint kernels' device milliseconds)."""
-    import time
-
     from . import scenes
     from .world import World
 
@@ -325,7 +340,8 @@ def tower_gradients(count, seed=5000, steps=120, dt=1 / 60, checkpoint=20, first
             ball = o + info["ball"]
             grads[i, 2:] = bar["velocity"][3 * ball: 3 * ball + 3]
         return dict(gradients=grads, losses=np.array(losses), position=position, forward_s=t1 - t0,
-                    backward_s=t2 - t1, device_ms=bb.device_ms, tape_peak=bb.tape_peak, infos=infos)
+                    backward_s=t2 - t1, device_ms=bb.device_ms, tape_peak=bb.tape_peak, infos=infos,
+                    backward_parts=dict(bb.times))
     finally:
         bb.close()
         for w in worlds:

@@ -19,16 +19,20 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
 
+#include <unistd.h>
+
 #include "../../include/bearing_gpu.h"
 #include "layout.cuh"
 #include "stage.cuh"
 #include "adjoint.cuh"
+#include "../host/collide_impl.hpp"
 
 namespace {
 
@@ -374,9 +378,25 @@ std::vector<std::pair<size_t, size_t>> piece_groups(const Plan& plan, int groups
   return out;
 }
 
-// Whether host memory is page-locked (cudaHostAlloc'd or registered): the device can copy it
-// directly, with no gather through the library's own pinned block.
-bool host_pinned(const void* p) {
+// The ranges bg_register_host page-locked, every context's together (a registration belongs to
+// the process, not to one context): base -> bytes.
+std::mutex g_registry_mu;
+std::map<uintptr_t, size_t> g_registered;
+
+// Whether the host memory [p, p + bytes) is page-locked, so that the device can copy it directly
+// with no gather through the library's own pinned block: inside one range bg_register_host locked,
+// or (memory locked some other way, cudaHostAlloc'd say) page-locked as CUDA reports it.  A column
+// that starts inside a registered range but runs past its end is staged.
+bool host_pinned(const void* p, size_t bytes) {
+  const uintptr_t at = reinterpret_cast<uintptr_t>(p);
+  {
+    std::lock_guard<std::mutex> lock(g_registry_mu);
+    auto it = g_registered.upper_bound(at);
+    if (it != g_registered.begin()) {
+      --it;
+      if (at < it->first + it->second) return at + bytes <= it->first + it->second;
+    }
+  }
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
@@ -485,6 +505,15 @@ struct bg_ctx {
   int nbodies = 0, nrows = 0, nawake = 0, nworlds = 0;
   bool uploaded = false;
   bool batch = false;
+  // the host ranges bg_register_host page-locked for this context: (base, bytes)
+  std::vector<std::pair<uintptr_t, size_t>> registered;
+  // bg_collide's device block (grown by doubling, freed with the context) and its kernel's events
+  struct Narrow {
+    unsigned char* block = nullptr;
+    size_t bodies = 0, pairs = 0;
+    cudaEvent_t begin = nullptr, end = nullptr;
+    bool timed = false;
+  } nw;
   // bg_backward's own device memory (grown by doubling, freed with the context)
   struct Adjoint {
     std::vector<void*> allocs;
@@ -821,7 +850,7 @@ int upload_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R, int nb, int 
   staged.end = plan.end;
   for (const Piece& pc : plan.pieces) {
     if (pc.bytes == 0) continue;
-    if (host_pinned(pc.from)) {
+    if (host_pinned(pc.from, pc.bytes)) {
       if (!cuda_ok(c, cudaMemcpyAsync(c->d_in + pc.off, pc.from, pc.bytes, cudaMemcpyHostToDevice, c->stream), "upload"))
         return BG_ECUDA;
     } else {
@@ -840,11 +869,22 @@ int upload_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R, int nb, int 
       add_slices(slices, static_cast<const unsigned char*>(pc.from), c->h_in + pc.off, pc.bytes);
     }
     copy_slices(pool, slices);
-    const size_t lo = staged.pieces[g.first].off;
-    const size_t hi = staged.pieces[g.second - 1].off + staged.pieces[g.second - 1].bytes;
-    if (hi > lo &&
-        !cuda_ok(c, cudaMemcpyAsync(c->d_in + lo, c->h_in + lo, hi - lo, cudaMemcpyHostToDevice, c->stream), "upload"))
-      return BG_ECUDA;
+    // One copy per run of staged pieces that lie next to each other in the block: a column copied
+    // straight from the caller's memory between two of them must not be overwritten with whatever
+    // the staging block holds at its place.
+    for (size_t k = g.first; k < g.second;) {
+      const size_t lo = staged.pieces[k].off;
+      size_t hi = lo + staged.pieces[k].bytes;
+      size_t e = k + 1;
+      while (e < g.second && staged.pieces[e].off <= ((hi + 255) & ~static_cast<size_t>(255))) {
+        hi = staged.pieces[e].off + staged.pieces[e].bytes;
+        e++;
+      }
+      if (hi > lo &&
+          !cuda_ok(c, cudaMemcpyAsync(c->d_in + lo, c->h_in + lo, hi - lo, cudaMemcpyHostToDevice, c->stream), "upload"))
+        return BG_ECUDA;
+      k = e;
+    }
   }
   if (!cuda_ok(c, cudaEventRecord(c->in_free, c->stream), "upload")) return BG_ECUDA;
   c->in_pending = true;
@@ -1143,7 +1183,7 @@ int download_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
   bool ok = true;
   for (const Piece& pc : all.pieces) {
     if (pc.bytes == 0 || pc.to == nullptr) continue;
-    if (host_pinned(pc.to))
+    if (host_pinned(pc.to, pc.bytes))
       ok = ok && cuda_ok(c, cudaMemcpyAsync(pc.to, c->d_out + pc.off, pc.bytes, cudaMemcpyDeviceToHost, c->stream),
                          "download");
     else
@@ -1178,6 +1218,60 @@ int download_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R) {
     return BG_ETIMEOUT;
   }
   return BG_OK;
+}
+
+// Waits for every copy this context (and its groups' contexts) may have in flight, then releases
+// the ranges it registered.
+void release_registered(bg_ctx* c) {
+  if (c->registered.empty()) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (bg_ctx* k : c->kids)
+    if (k->stream) cudaStreamSynchronize(k->stream);
+  std::lock_guard<std::mutex> lock(g_registry_mu);
+  for (const auto& r : c->registered) {
+    cudaHostUnregister(reinterpret_cast<void*>(r.first));
+    g_registered.erase(r.first);
+  }
+  cudaGetLastError();
+  c->registered.clear();
+}
+
+// Every non-NULL column of B and R, in and out, for nb slots and nr rows, as page-aligned
+// ranges, sorted, with ranges that overlap or touch merged (two columns on one page are one range).
+std::vector<std::pair<uintptr_t, uintptr_t>> column_pages(bg_ctx* c, const bg_bodies* B, const bg_rows* R, size_t nb,
+                                                          size_t nr) {
+  // plan_in and plan_out set the context's staging pointers as they go: keep the uploaded ones
+  const BodyStage bin = c->bin;
+  const RowStage rin = c->rin;
+  const BodyOut bout = c->bout;
+  const RowOut rout = c->rout;
+  int32_t* const awake_in = c->awake_in;
+  double* const maxni_in = c->maxni_in;
+  double* const relvel_in = c->relvel_in;
+  double* const gap_in = c->gap_in;
+  const Plan in = plan_in(c, B, R, nb, nr, nb, nullptr);
+  const Plan out = plan_out(c, B, R, nb, nr, nullptr);
+  c->bin = bin; c->rin = rin; c->bout = bout; c->rout = rout; c->awake_in = awake_in;
+  c->maxni_in = maxni_in; c->relvel_in = relvel_in; c->gap_in = gap_in;
+  const uintptr_t page = static_cast<uintptr_t>(sysconf(_SC_PAGESIZE) > 0 ? sysconf(_SC_PAGESIZE) : 4096);
+  std::vector<std::pair<uintptr_t, uintptr_t>> spans;
+  auto add = [&](const void* p, size_t bytes) {
+    if (p == nullptr || bytes == 0) return;
+    const uintptr_t lo = reinterpret_cast<uintptr_t>(p) / page * page;
+    const uintptr_t hi = (reinterpret_cast<uintptr_t>(p) + bytes + page - 1) / page * page;
+    spans.emplace_back(lo, hi);
+  };
+  for (const Piece& pc : in.pieces) add(pc.from, pc.bytes);
+  for (const Piece& pc : out.pieces) add(pc.to, pc.bytes);
+  std::sort(spans.begin(), spans.end());
+  std::vector<std::pair<uintptr_t, uintptr_t>> merged;
+  for (const auto& s : spans) {
+    if (!merged.empty() && s.first <= merged.back().second)
+      merged.back().second = std::max(merged.back().second, s.second);
+    else
+      merged.push_back(s);
+  }
+  return merged;
 }
 
 }  // namespace
@@ -1217,11 +1311,15 @@ void bg_destroy(bg_ctx* c) {
   if (c == nullptr) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  release_registered(c);
   for (bg_ctx* k : c->kids) bg_destroy(k);
   c->kids.clear();
   free_all(c);
   for (void* p : c->adj.allocs) cudaFree(p);
   c->adj.allocs.clear();
+  if (c->nw.block) cudaFree(c->nw.block);
+  if (c->nw.begin) cudaEventDestroy(c->nw.begin);
+  if (c->nw.end) cudaEventDestroy(c->nw.end);
   if (c->adj.begin) cudaEventDestroy(c->adj.begin);
   if (c->adj.end) cudaEventDestroy(c->adj.end);
   c->pool.reset();
@@ -1237,6 +1335,52 @@ void bg_destroy(bg_ctx* c) {
 const char* bg_last_error(const bg_ctx* c) { return c == nullptr ? "no context" : c->error.c_str(); }
 
 void* bg_stream(bg_ctx* c) { return c == nullptr ? nullptr : static_cast<void*>(c->stream); }
+
+int32_t bg_register_host(bg_ctx* c, const bg_bodies* B, const bg_rows* R, int32_t row_capacity) {
+  if (c == nullptr) return BG_EINVAL;
+  if (B == nullptr || R == nullptr) {
+    set_error(c, "bg_register_host: bodies or rows is NULL");
+    return BG_EINVAL;
+  }
+  if (B->capacity < 0 || R->count < 0 || row_capacity < R->count) {
+    set_error(c, "bg_register_host: capacity %d, row count %d, row capacity %d", B->capacity, R->count, row_capacity);
+    return BG_EINVAL;
+  }
+  cudaSetDevice(c->device);
+  const auto spans = column_pages(c, B, R, static_cast<size_t>(B->capacity), static_cast<size_t>(row_capacity));
+  release_registered(c);
+  std::lock_guard<std::mutex> lock(g_registry_mu);
+  for (const auto& s : spans) {
+    const size_t bytes = s.second - s.first;
+    const cudaError_t e = cudaHostRegister(reinterpret_cast<void*>(s.first), bytes, cudaHostRegisterPortable);
+    if (e == cudaErrorHostMemoryAlreadyRegistered) {   // someone else's: theirs to keep or release
+      cudaGetLastError();
+      continue;
+    }
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_error(c, "bg_register_host: cudaHostRegister of %zu bytes: %s", bytes, cudaGetErrorString(e));
+      return BG_ECUDA;   // the ranges registered so far stay listed, released as usual
+    }
+    c->registered.emplace_back(s.first, bytes);
+    g_registered[s.first] = bytes;
+  }
+  return BG_OK;
+}
+
+int32_t bg_unregister_host(bg_ctx* c) {
+  if (c == nullptr) return BG_EINVAL;
+  cudaSetDevice(c->device);
+  release_registered(c);
+  return BG_OK;
+}
+
+int64_t bg_registered_bytes(const bg_ctx* c) {
+  if (c == nullptr) return 0;
+  int64_t n = 0;
+  for (const auto& r : c->registered) n += static_cast<int64_t>(r.second);
+  return n;
+}
 
 int32_t bg_last_launches(const bg_ctx* c) { return c == nullptr ? 0 : c->last_launches; }
 
@@ -1579,7 +1723,7 @@ int groups_for(const bg_ctx* c, const bg_rows* R, const bg_worlds* W) {
   // memory bandwidth (4,096 worlds, 845,037 rows: page-locked 36 ms in one piece, 24 ms in 4-6
   // groups; pageable 42 ms, 35 ms in 2-3 groups, 43 ms in 8).
   if (g == 0) {
-    const int64_t per = host_pinned(R->normal) ? kRowsPerGroup : 2 * static_cast<int64_t>(kRowsPerGroup);
+    const int64_t per = host_pinned(R->normal, 3 * sizeof(double) * static_cast<size_t>(R->count)) ? kRowsPerGroup : 2 * static_cast<int64_t>(kRowsPerGroup);
     g = static_cast<int>(std::min<int64_t>(BG_MAX_BATCH_GROUPS, R->count / per));
   }
   return std::max(1, std::min(g, W->count));
@@ -2389,3 +2533,248 @@ extern "C" int32_t bg_solve_step_static(const bg_bodies* bodies, const bg_rows* 
   if (cudaStreamSynchronize(s) != cudaSuccess) return BG_ECUDA;
   return status == 0 ? BG_OK : status == kStaticRefused ? BG_EINVAL : BG_ETIMEOUT;
 }
+
+// ---- the narrowphase on the device (bg_collide) -------------------------------------------
+//
+// One thread a pair, running the same narrowphase source the host side of the step runs
+// (host/collide_impl.hpp, the reference's src/collide.js restated, compiled here for sm_100a with
+// -fmad=false, so the manifolds match the host's bit for bit).  The pairs are first put in order of
+// their two shapes' kinds (a counting sort on the device), so each warp runs one of the six pair
+// functions: box-box's face clipping, capsule-box's and the rest diverge only where their own
+// branches do.
+
+namespace {
+
+constexpr int kCollideThreads = 128;
+constexpr int kPairClasses = 6;   // sphere-sphere, sphere-capsule, sphere-box, capsule-capsule, capsule-box, box-box
+
+struct CollideParams {
+  const double *p, *q, *dims, *gscale;
+  const uint8_t *shape, *type;
+  const int32_t *a, *b;
+  const double *margin, *tol;
+  int32_t n;
+  double gravity[3];
+  int32_t* counts;   // kPairClasses pairs per class, then kPairClasses cursors
+  int32_t* order;    // pairs in class order
+  uint8_t* points;
+  double *normal, *point, *separation;
+  uint32_t* pid;
+};
+
+__device__ __forceinline__ int kind_of(uint8_t shape) {
+  return shape == BG_SPHERE ? bearing::K_SPHERE : shape == BG_CAPSULE ? bearing::K_CAPSULE : bearing::K_BOX;
+}
+
+// The pair's class: its two kinds, lower first, as collide() dispatches them (src/collide.js:225-242).
+__device__ __forceinline__ int pair_class(const CollideParams& c, int i) {
+  int x = kind_of(c.shape[c.a[i]]), y = kind_of(c.shape[c.b[i]]);
+  if (x > y) { const int t = x; x = y; y = t; }
+  return x == 0 ? y : x == 1 ? 2 + y : 5;
+}
+
+__global__ void collide_count(CollideParams c) {
+  __shared__ int local[kPairClasses];
+  if (threadIdx.x < kPairClasses) local[threadIdx.x] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x)
+    atomicAdd(&local[pair_class(c, i)], 1);
+  __syncthreads();
+  if (threadIdx.x < kPairClasses && local[threadIdx.x] > 0) atomicAdd(&c.counts[threadIdx.x], local[threadIdx.x]);
+}
+
+// Each class's first place in `order` (the cursors the scatter moves on).
+__global__ void collide_starts(CollideParams c) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int at = 0;
+  for (int k = 0; k < kPairClasses; k++) {
+    c.counts[kPairClasses + k] = at;
+    at += c.counts[k];
+  }
+}
+
+__global__ void collide_scatter(CollideParams c) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x)
+    c.order[atomicAdd(&c.counts[kPairClasses + pair_class(c, i)], 1)] = i;
+}
+
+// load(): src/contact.js:1244-1276, for boxes, spheres and capsules, with the axes of
+// src/core/math.js:222-227.
+__device__ void load_shape(const CollideParams& c, int slot, bearing::Shape& s) {
+  const double* d = c.dims + 3 * slot;
+  const uint8_t shape = c.shape[slot];
+  if (shape == BG_SPHERE) {
+    s.kind = bearing::K_SPHERE;
+    s.half[0] = d[0]; s.half[1] = 0; s.half[2] = 0;
+  } else if (shape == BG_CAPSULE) {
+    s.kind = bearing::K_CAPSULE;
+    s.half[0] = d[0]; s.half[1] = (d[1] - 2 * d[0]) * 0.5; s.half[2] = 0;
+  } else {
+    s.kind = bearing::K_BOX;
+    s.half[0] = d[0] * 0.5; s.half[1] = d[1] * 0.5; s.half[2] = d[2] * 0.5;
+  }
+  for (int k = 0; k < 3; k++) s.center[k] = c.p[3 * slot + k];
+  const double scale = c.type[slot] == BG_DYNAMIC ? c.gscale[slot] : 0;
+  for (int k = 0; k < 3; k++) s.weight[k] = c.gravity[k] * scale;
+  const double* q = c.q + 4 * slot;
+  const double x = q[0], y = q[1], z = q[2], w = q[3];
+  double* ax = s.axes;
+  ax[0] = 1 - 2 * (y * y + z * z); ax[1] = 2 * (x * y + z * w); ax[2] = 2 * (x * z - y * w);
+  ax[3] = 2 * (x * y - z * w); ax[4] = 1 - 2 * (x * x + z * z); ax[5] = 2 * (y * z + x * w);
+  ax[6] = 2 * (x * z + y * w); ax[7] = 2 * (y * z - x * w); ax[8] = 1 - 2 * (x * x + y * y);
+}
+
+__global__ void __launch_bounds__(kCollideThreads) collide_pairs(CollideParams c) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < c.n; j += gridDim.x * blockDim.x) {
+    const int i = c.order[j];
+    bearing::Shape sa, sb;
+    bearing::Manifold mf;
+    load_shape(c, c.a[i], sa);
+    load_shape(c, c.b[i], sb);
+    const int count = bearing::collideT<double>(sa, sb, c.margin[i], c.tol[i], mf);
+    c.points[i] = static_cast<uint8_t>(count);
+    for (int k = 0; k < 3; k++) c.normal[3 * i + k] = count > 0 ? mf.normal[k] : 0.0;
+    for (int k = 0; k < bg::P; k++) {
+      const bool used = k < count;
+      for (int e = 0; e < 3; e++) c.point[3 * (bg::P * i + k) + e] = used ? mf.points[3 * k + e] : 0.0;
+      c.separation[bg::P * i + k] = used ? mf.separations[k] : 0.0;
+      c.pid[bg::P * i + k] = used ? mf.ids[k] : 0u;
+    }
+  }
+}
+
+// bg_collide's arrays for nb slots and np pairs, carved from `base` (NULL: only measures).
+struct CollideLayout {
+  double *p, *q, *dims, *gscale;
+  uint8_t *shape, *type;
+  int32_t *a, *b, *counts, *order;
+  double *margin, *tol;
+  uint8_t* points;
+  double *normal, *point, *separation;
+  uint32_t* pid;
+  size_t bytes;
+};
+
+CollideLayout collide_layout(unsigned char* base, size_t nb, size_t np) {
+  Carve k{base};
+  CollideLayout L;
+  L.p = k.take<double>(3 * nb); L.q = k.take<double>(4 * nb); L.dims = k.take<double>(3 * nb);
+  L.gscale = k.take<double>(nb); L.shape = k.take<uint8_t>(nb); L.type = k.take<uint8_t>(nb);
+  L.a = k.take<int32_t>(np); L.b = k.take<int32_t>(np); L.margin = k.take<double>(np); L.tol = k.take<double>(np);
+  L.counts = k.take<int32_t>(2 * kPairClasses); L.order = k.take<int32_t>(np);
+  L.points = k.take<uint8_t>(np); L.normal = k.take<double>(3 * np); L.point = k.take<double>(3 * bg::P * np);
+  L.separation = k.take<double>(bg::P * np); L.pid = k.take<uint32_t>(bg::P * np);
+  L.bytes = k.end;
+  return L;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t bg_collide(bg_ctx* c, const bg_bodies* B, const double* gravity, const bg_pairs* P, bg_manifolds* out) {
+  if (c == nullptr) return BG_EINVAL;
+  if (B == nullptr || gravity == nullptr || P == nullptr || out == nullptr) {
+    set_error(c, "bg_collide: bodies, gravity, pairs or out is NULL");
+    return BG_EINVAL;
+  }
+  const int64_t nb = B->capacity, np = P->count;
+  if (nb < 0 || np < 0) {
+    set_error(c, "bg_collide: capacity %d, pairs %d", B->capacity, P->count);
+    return BG_EINVAL;
+  }
+  if (np == 0) return BG_OK;
+  if (P->a == nullptr || P->b == nullptr || P->margin == nullptr || P->tolerance == nullptr || out->points == nullptr ||
+      out->normal == nullptr || out->point == nullptr || out->separation == nullptr || out->pid == nullptr ||
+      B->position == nullptr || B->rotation == nullptr || B->dims == nullptr || B->shape == nullptr ||
+      B->type == nullptr || B->gravity_scale == nullptr) {
+    set_error(c, "bg_collide: a column is NULL");
+    return BG_EINVAL;
+  }
+  // every index is checked before anything is copied: a pair's slots among the bodies', and the
+  // shapes it reads boxes, spheres or capsules
+  for (int64_t i = 0; i < np; i++) {
+    const int32_t a = P->a[i], b = P->b[i];
+    if (a < 0 || a >= nb || b < 0 || b >= nb) {
+      set_error(c, "bg_collide: pair %lld has slots %d, %d of %lld", static_cast<long long>(i), a, b,
+                static_cast<long long>(nb));
+      return BG_EINVAL;
+    }
+    for (const int32_t s : {a, b})
+      if (B->shape[s] != BG_BOX && B->shape[s] != BG_SPHERE && B->shape[s] != BG_CAPSULE) {
+        set_error(c, "bg_collide: slot %d is not a box, sphere or capsule", s);
+        return BG_EUNSUPPORTED;
+      }
+  }
+  cudaSetDevice(c->device);
+  bg_ctx::Narrow& d = c->nw;
+  if (d.block == nullptr || static_cast<size_t>(nb) > d.bodies || static_cast<size_t>(np) > d.pairs) {
+    cudaStreamSynchronize(c->stream);
+    if (d.block) cudaFree(d.block);
+    d.block = nullptr;
+    d.bodies = grown(d.bodies, static_cast<size_t>(nb));
+    d.pairs = grown(d.pairs, static_cast<size_t>(np));
+    void* block = nullptr;
+    if (cudaMalloc(&block, collide_layout(nullptr, d.bodies, d.pairs).bytes) != cudaSuccess) {
+      cudaGetLastError();
+      d.bodies = d.pairs = 0;
+      set_error(c, "bg_collide: cudaMalloc failed");
+      return BG_ENOMEM;
+    }
+    d.block = static_cast<unsigned char*>(block);
+  }
+  if (d.begin == nullptr) {
+    cudaEventCreate(&d.begin);
+    cudaEventCreate(&d.end);
+  }
+  const CollideLayout L = collide_layout(d.block, d.bodies, d.pairs);
+  const size_t b8 = static_cast<size_t>(nb) * sizeof(double), p8 = static_cast<size_t>(np) * sizeof(double);
+  const size_t p4 = static_cast<size_t>(np) * sizeof(int32_t);
+  cudaStream_t st = c->stream;
+  bool ok = true;
+  auto h2d = [&](void* dst, const void* src, size_t bytes) {
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st), "bg_collide upload");
+  };
+  h2d(L.p, B->position, 3 * b8); h2d(L.q, B->rotation, 4 * b8); h2d(L.dims, B->dims, 3 * b8);
+  h2d(L.gscale, B->gravity_scale, b8); h2d(L.shape, B->shape, static_cast<size_t>(nb)); h2d(L.type, B->type, static_cast<size_t>(nb));
+  h2d(L.a, P->a, p4); h2d(L.b, P->b, p4); h2d(L.margin, P->margin, p8); h2d(L.tol, P->tolerance, p8);
+  ok = ok && cuda_ok(c, cudaMemsetAsync(L.counts, 0, 2 * kPairClasses * sizeof(int32_t), st), "bg_collide");
+  if (!ok) return BG_ECUDA;
+  CollideParams k;
+  k.p = L.p; k.q = L.q; k.dims = L.dims; k.gscale = L.gscale; k.shape = L.shape; k.type = L.type;
+  k.a = L.a; k.b = L.b; k.margin = L.margin; k.tol = L.tol; k.n = static_cast<int32_t>(np);
+  for (int e = 0; e < 3; e++) k.gravity[e] = gravity[e];
+  k.counts = L.counts; k.order = L.order; k.points = L.points; k.normal = L.normal; k.point = L.point;
+  k.separation = L.separation; k.pid = L.pid;
+  const int sweep = std::max(1, std::min(static_cast<int>((np + 255) / 256), 4 * c->sms));
+  collide_count<<<sweep, 256, 0, st>>>(k);
+  collide_starts<<<1, 32, 0, st>>>(k);
+  collide_scatter<<<sweep, 256, 0, st>>>(k);
+  const int blocks = static_cast<int>(std::min<int64_t>((np + kCollideThreads - 1) / kCollideThreads, 64 * c->sms));
+  cudaEventRecord(d.begin, st);
+  collide_pairs<<<blocks, kCollideThreads, 0, st>>>(k);
+  cudaEventRecord(d.end, st);
+  d.timed = true;
+  c->last_launches += 4;
+  if (!cuda_ok(c, cudaGetLastError(), "bg_collide launch")) return BG_ECUDA;
+  auto d2h = [&](void* dst, const void* src, size_t bytes) {
+    ok = ok && cuda_ok(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st), "bg_collide download");
+  };
+  d2h(out->points, L.points, static_cast<size_t>(np)); d2h(out->normal, L.normal, 3 * p8);
+  d2h(out->point, L.point, 3 * bg::P * p8); d2h(out->separation, L.separation, bg::P * p8);
+  d2h(out->pid, L.pid, bg::P * p4);
+  ok = ok && cuda_ok(c, cudaStreamSynchronize(st), "bg_collide");
+  return ok ? BG_OK : BG_ECUDA;
+}
+
+double bg_last_collide_ms(bg_ctx* c) {
+  if (c == nullptr || !c->nw.timed) return -1;
+  float ms = 0;
+  if (cudaEventSynchronize(c->nw.end) != cudaSuccess || cudaEventElapsedTime(&ms, c->nw.begin, c->nw.end) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return ms;
+}
+
+}  // extern "C"

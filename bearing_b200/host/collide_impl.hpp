@@ -16,38 +16,53 @@
 
 #include "collide.hpp"
 
+// The same source serves the host side of the step (g++) and the device narrowphase (nvcc, one
+// thread a pair): every function is callable from both.
+#if defined(__CUDACC__)
+#define NW_HD __host__ __device__
+#else
+#define NW_HD
+#endif
+
 namespace bearing {
 namespace narrow_detail {
 
 using std::fabs;
 using std::sqrt;
-inline double val(double x) { return x; }
+NW_HD inline double val(double x) { return x; }
+// The sign bit of x (Math.max / Math.min tell +0 from -0 by it).
+NW_HD inline bool sign_bit(double x) {
+#if defined(__CUDA_ARCH__)
+  return __double_as_longlong(x) < 0;
+#else
+  return std::signbit(x);
+#endif
+}
 
 constexpr double INF = std::numeric_limits<double>::infinity();
 constexpr double PARALLEL = 7.450580596923828e-9;   // 2^-27, src/collide.js:686
 
-const int CORNER_P[4] = {-1, 1, 1, -1}, CORNER_Q[4] = {-1, -1, 1, 1};   // src/collide.js:703
-const int EDGE_FROM[12] = {0, 2, 4, 6, 0, 1, 4, 5, 0, 1, 2, 3};        // src/collide.js:791
-const int EDGE_TO[12] = {1, 3, 5, 7, 2, 3, 6, 7, 4, 5, 6, 7};
-const int EDGE_PLANE[4] = {3, 0, 2, 1}, PLANE_EDGE[4] = {1, 3, 2, 0};  // src/collide.js:869
+// The reference's small tables, as functions (device code reads no host arrays).
+// CORNER_P, CORNER_Q: src/collide.js:703.
+NW_HD inline int corner_p(int v) { return v == 1 || v == 2 ? 1 : -1; }
+NW_HD inline int corner_q(int v) { return v >= 2 ? 1 : -1; }
+// EDGE_FROM, EDGE_TO: src/collide.js:791 (edges along x: corners 2i, 2i+1; along y: 0 1 4 5 to
+// +2; along z: 0 1 2 3 to +4).
+NW_HD inline int edge_from(int i) { return i < 4 ? 2 * i : i < 8 ? (i - 4) + ((i - 4) >= 2 ? 2 : 0) : i - 8; }
+NW_HD inline int edge_to(int i) { return edge_from(i) + (i < 4 ? 1 : i < 8 ? 2 : 4); }
+// EDGE_PLANE {3, 0, 2, 1}, PLANE_EDGE {1, 3, 2, 0}: src/collide.js:869.
+NW_HD inline int edge_plane(int e) { return e == 0 ? 3 : e == 1 ? 0 : e == 2 ? 2 : 1; }
+NW_HD inline int plane_edge(int k) { return k == 0 ? 1 : k == 1 ? 3 : k == 2 ? 2 : 0; }
 
-// SWAPPED: src/collide.js:870-877.
-struct Swapped {
-  uint8_t f[32];
-  Swapped() {
-    for (int i = 0; i < 32; i++) f[i] = static_cast<uint8_t>(i);
-    for (int v = 0; v < 4; v++) {
-      const int j = CORNER_P[v] > 0 ? 0 : 1, k = CORNER_Q[v] > 0 ? 2 : 3;
-      f[v] = static_cast<uint8_t>(20 + 4 * j + k);
-      f[20 + 4 * j + k] = static_cast<uint8_t>(v);
-    }
-    for (int e = 0; e < 4; e++)
-      for (int k = 0; k < 4; k++) f[4 + 4 * e + k] = static_cast<uint8_t>(4 + 4 * PLANE_EDGE[k] + EDGE_PLANE[e]);
-  }
-};
-inline const Swapped& swapped() {
-  static const Swapped s;
-  return s;
+// SWAPPED[f]: src/collide.js:870-877, entry by entry: a corner v of the incident face and the
+// crossing of its two reference planes trade places, an edge-plane crossing is renumbered from
+// the other box's side, and every other feature keeps its number.
+NW_HD inline int swapped_feature(int f) {
+  if (f < 4) return 20 + 4 * (corner_p(f) > 0 ? 0 : 1) + (corner_q(f) > 0 ? 2 : 3);
+  if (f < 20) return 4 + 4 * plane_edge((f - 4) % 4) + edge_plane((f - 4) / 4);
+  for (int v = 0; v < 4; v++)
+    if (f == 20 + 4 * (corner_p(v) > 0 ? 0 : 1) + (corner_q(v) > 0 ? 2 : 3)) return v;
+  return f;
 }
 
 template <class T>
@@ -55,23 +70,23 @@ struct NarrowT {
   using Shape = ShapeT<T>;
   using Manifold = ManifoldT<T>;
   // sgn, clamp01: src/collide.js:246-247.
-  static T sgn(const T& x) { return x < 0 ? T(-1) : T(1); }
-  static T clamp01(const T& x) { return x < 0 ? T(0) : x > 1 ? T(1) : x; }
+  NW_HD static T sgn(const T& x) { return x < 0 ? T(-1) : T(1); }
+  NW_HD static T clamp01(const T& x) { return x < 0 ? T(0) : x > 1 ? T(1) : x; }
   // Math.max / Math.min with JavaScript's NaN and signed-zero rules.
-  static T jmax(const T& a, const T& b) {
+  NW_HD static T jmax(const T& a, const T& b) {
     if (a != a) return a;
     if (b != b) return b;
     if (a > b) return a;
     if (b > a) return b;
-    if (a == 0 && b == 0) return std::signbit(val(a)) ? b : a;
+    if (a == 0 && b == 0) return sign_bit(val(a)) ? b : a;
     return a;
   }
-  static T jmin(const T& a, const T& b) {
+  NW_HD static T jmin(const T& a, const T& b) {
     if (a != a) return a;
     if (b != b) return b;
     if (a < b) return a;
     if (b < a) return b;
-    if (a == 0 && b == 0) return std::signbit(val(a)) ? a : b;
+    if (a == 0 && b == 0) return sign_bit(val(a)) ? a : b;
     return a;
   }
 
@@ -90,7 +105,7 @@ struct NarrowT {
   T FOOT[3];
 
   // normalize: src/collide.js:257-264.
-  T normalize(T x, T y, T z) {
+  NW_HD T normalize(T x, T y, T z) {
     const T m = jmax(jmax(fabs(x), fabs(y)), fabs(z));
     if (m == 0) return 0;
     const T sx = x / m, sy = y / m, sz = z / m;
@@ -99,23 +114,23 @@ struct NarrowT {
     return l * m;
   }
   // perpendicular: src/collide.js:272-277.
-  void perpendicular(T vx, T vy, T vz) {
+  NW_HD void perpendicular(T vx, T vy, T vz) {
     const T ax = fabs(vx), ay = fabs(vy), az = fabs(vz);
     if (ax <= ay && ax <= az) normalize(0, vz, -vy);
     else if (ay <= az) normalize(-vz, 0, vx);
     else normalize(vy, -vx, 0);
   }
-  static void setNormal(Manifold& out, T x, T y, T z) {
+  NW_HD static void setNormal(Manifold& out, T x, T y, T z) {
     out.normal[0] = x; out.normal[1] = y; out.normal[2] = z;
   }
-  static void addPoint(Manifold& out, T x, T y, T z, T separation, uint32_t id) {
+  NW_HD static void addPoint(Manifold& out, T x, T y, T z, T separation, uint32_t id) {
     const int k = out.count++;
     out.points[3 * k] = x; out.points[3 * k + 1] = y; out.points[3 * k + 2] = z;
     out.separations[k] = separation;
     out.ids[k] = id;
   }
   // balls: src/collide.js:296-306.
-  bool balls(T ax, T ay, T az, T ra, T bx, T by, T bz, T rb,
+  NW_HD bool balls(T ax, T ay, T az, T ra, T bx, T by, T bz, T rb,
              T fx, T fy, T fz, T margin, Manifold& out, uint32_t id) {
     const T dist = normalize(bx - ax, by - ay, bz - az);
     const T separation = dist - ra - rb;
@@ -127,21 +142,21 @@ struct NarrowT {
     return true;
   }
   // segment: src/collide.js:309-313.
-  static void segment(const Shape& c, T* out) {
+  NW_HD static void segment(const Shape& c, T* out) {
     const T h = c.half[1];
     const T* y = c.axes;
     out[0] = c.center[0] - y[3] * h; out[1] = c.center[1] - y[4] * h; out[2] = c.center[2] - y[5] * h;
     out[3] = c.center[0] + y[3] * h; out[4] = c.center[1] + y[4] * h; out[5] = c.center[2] + y[5] * h;
   }
   // nearestOnSegment: src/collide.js:316-321.
-  static T nearestOnSegment(const T* s, T x, T y, T z) {
+  NW_HD static T nearestOnSegment(const T* s, T x, T y, T z) {
     const T dx = s[3] - s[0], dy = s[4] - s[1], dz = s[5] - s[2];
     const T dd = dx * dx + dy * dy + dz * dz;
     if (dd == 0) return 0;
     return clamp01(((x - s[0]) * dx + (y - s[1]) * dy + (z - s[2]) * dz) / dd);
   }
   // closestSegments: src/collide.js:332-349.
-  void closestSegments(const T* p, const T* q) {
+  NW_HD void closestSegments(const T* p, const T* q) {
     const T d1x = p[3] - p[0], d1y = p[4] - p[1], d1z = p[5] - p[2];
     const T d2x = q[3] - q[0], d2y = q[4] - q[1], d2z = q[5] - q[2];
     const T rx = p[0] - q[0], ry = p[1] - q[1], rz = p[2] - q[2];
@@ -161,12 +176,12 @@ struct NarrowT {
   }
 
   // sphereSphere: src/collide.js:353-357.
-  void sphereSphere(const Shape& a, const Shape& b, T margin, Manifold& out) {
+  NW_HD void sphereSphere(const Shape& a, const Shape& b, T margin, Manifold& out) {
     balls(a.center[0], a.center[1], a.center[2], a.half[0], b.center[0], b.center[1], b.center[2], b.half[0],
           0, 1, 0, margin, out, 0);
   }
   // sphereCapsule: src/collide.js:361-369.
-  void sphereCapsule(const Shape& a, const Shape& b, T margin, Manifold& out) {
+  NW_HD void sphereCapsule(const Shape& a, const Shape& b, T margin, Manifold& out) {
     const T* c = a.center;
     segment(b, segB);
     const T t = nearestOnSegment(segB, c[0], c[1], c[2]);
@@ -176,7 +191,7 @@ struct NarrowT {
     balls(c[0], c[1], c[2], a.half[0], qx, qy, qz, b.half[0], unit[0], unit[1], unit[2], margin, out, 0);
   }
   // sphereBox: src/collide.js:371-403.
-  void sphereBox(const Shape& a, const Shape& b, T margin, Manifold& out) {
+  NW_HD void sphereBox(const Shape& a, const Shape& b, T margin, Manifold& out) {
     const T* ax = b.axes;
     const T* h = b.half;
     const T r = a.half[0];
@@ -209,7 +224,7 @@ struct NarrowT {
   }
 
   // capsuleCapsule: src/collide.js:424-482.
-  void capsuleCapsule(const Shape& a, const Shape& b, T margin, T tolerance, Manifold& out) {
+  NW_HD void capsuleCapsule(const Shape& a, const Shape& b, T margin, T tolerance, Manifold& out) {
     segment(a, segA);
     segment(b, segB);
     closestSegments(segA, segB);
@@ -268,14 +283,14 @@ struct NarrowT {
   }
 
   // toWorld: src/collide.js:552-557.
-  void toWorld(const Shape& b, T x, T y, T z) {
+  NW_HD void toWorld(const Shape& b, T x, T y, T z) {
     const T* ax = b.axes;
     world[0] = b.center[0] + ax[0] * x + ax[3] * y + ax[6] * z;
     world[1] = b.center[1] + ax[1] * x + ax[4] * y + ax[7] * z;
     world[2] = b.center[2] + ax[2] * x + ax[5] * y + ax[8] * z;
   }
   // segmentHitsBox: src/collide.js:560-575.
-  static bool segmentHitsBox(const T* s, const T* h) {
+  NW_HD static bool segmentHitsBox(const T* s, const T* h) {
     T t0 = 0, t1 = 1;
     for (int i = 0; i < 3; i++) {
       const T p = s[i], d = s[3 + i] - s[i];
@@ -292,7 +307,7 @@ struct NarrowT {
     return true;
   }
   // clipToFace: src/collide.js:583-615.
-  bool clipToFace(const Shape& b, int axis, T facing, T r, T margin, Manifold& out, uint32_t idBase) {
+  NW_HD bool clipToFace(const Shape& b, int axis, T facing, T r, T margin, Manifold& out, uint32_t idBase) {
     const T* h = b.half;
     const int j = (axis + 1) % 3, k = (axis + 2) % 3;
     T u0 = 0, u1 = 1;
@@ -326,7 +341,7 @@ struct NarrowT {
     return out.count > 0;
   }
   // capsuleBoxDeep: src/collide.js:626-676.
-  void capsuleBoxDeep(const Shape& a, const Shape& b, T margin, T tolerance, Manifold& out) {
+  NW_HD void capsuleBoxDeep(const Shape& a, const Shape& b, T margin, T tolerance, Manifold& out) {
     const T* h = b.half;
     const T r = a.half[0];
     const T dx = local[3] - local[0], dy = local[4] - local[1], dz = local[5] - local[2];
@@ -377,7 +392,7 @@ struct NarrowT {
     addPoint(out, world[0], world[1], world[2], separation, static_cast<uint32_t>(32 + i));
   }
   // capsuleBox: src/collide.js:497-547.
-  void capsuleBox(const Shape& a, const Shape& b, T margin, T tolerance, Manifold& out) {
+  NW_HD void capsuleBox(const Shape& a, const Shape& b, T margin, T tolerance, Manifold& out) {
     segment(a, segA);
     const T* bx = b.axes;
     const T* h = b.half;
@@ -429,13 +444,13 @@ struct NarrowT {
   }
 
   // support: src/collide.js:840-844.
-  static T support(const T* X, const T* h, T nx, T ny, T nz) {
+  NW_HD static T support(const T* X, const T* h, T nx, T ny, T nz) {
     return h[0] * fabs(X[0] * nx + X[1] * ny + X[2] * nz)
       + h[1] * fabs(X[3] * nx + X[4] * ny + X[5] * nz)
       + h[2] * fabs(X[6] * nx + X[7] * ny + X[8] * nz);
   }
   // corners: src/collide.js:780-788.
-  static void corners(const Shape& x, T* c) {
+  NW_HD static void corners(const Shape& x, T* c) {
     const T* X = x.axes;
     const T* h = x.half;
     for (int k = 0; k < 8; k++) {
@@ -446,7 +461,7 @@ struct NarrowT {
     }
   }
   // boxBoxClosest: src/collide.js:800-837.
-  void boxBoxClosest(const Shape& a, const Shape& b, T margin, Manifold& out) {
+  NW_HD void boxBoxClosest(const Shape& a, const Shape& b, T margin, Manifold& out) {
     corners(a, cornerA);
     corners(b, cornerB);
     T best = INF, ax = 0, ay = 0, az = 0, bx = 0, by = 0, bz = 0;
@@ -471,9 +486,9 @@ struct NarrowT {
       }
     }
     for (int i = 0; i < 12; i++) {
-      for (int k = 0; k < 3; k++) { segA[k] = cornerA[3 * EDGE_FROM[i] + k]; segA[3 + k] = cornerA[3 * EDGE_TO[i] + k]; }
+      for (int k = 0; k < 3; k++) { segA[k] = cornerA[3 * edge_from(i) + k]; segA[3 + k] = cornerA[3 * edge_to(i) + k]; }
       for (int j = 0; j < 12; j++) {
-        for (int k = 0; k < 3; k++) { segB[k] = cornerB[3 * EDGE_FROM[j] + k]; segB[3 + k] = cornerB[3 * EDGE_TO[j] + k]; }
+        for (int k = 0; k < 3; k++) { segB[k] = cornerB[3 * edge_from(j) + k]; segB[3 + k] = cornerB[3 * edge_to(j) + k]; }
         closestSegments(segA, segB);
         const T px = segA[0] + (segA[3] - segA[0]) * segS, py = segA[1] + (segA[4] - segA[1]) * segS,
                      pz = segA[2] + (segA[5] - segA[2]) * segS;
@@ -490,7 +505,7 @@ struct NarrowT {
   }
 
   // clipPolygon: src/collide.js:966-999.
-  static int clipPolygon(const T* src, const int* sf, const int* sl, int count, T* dst, int* df, int* dl,
+  NW_HD static int clipPolygon(const T* src, const int* sf, const int* sl, int count, T* dst, int* df, int* dl,
                          T px, T py, T pz, T offset, int plane, T slack) {
     int n = 0;
     for (int v = 0; v < count; v++) {
@@ -522,7 +537,7 @@ struct NarrowT {
   }
 
   // four: src/collide.js:1116-1141.
-  void four(int n, int a, T nx, T ny, T nz, T pressed, T touching) {
+  NW_HD void four(int n, int a, T nx, T ny, T nz, T pressed, T touching) {
     int b = -1;
     T far = -1;
     for (int pass = 0; pass < 3 && b < 0; pass++) {
@@ -551,7 +566,7 @@ struct NarrowT {
     FOUR[0] = a; FOUR[1] = d; FOUR[2] = b; FOUR[3] = c;
   }
   // foot: src/collide.js:1171-1178.
-  bool foot(const Shape& s, T nx, T ny, T nz) {
+  NW_HD bool foot(const Shape& s, T nx, T ny, T nz) {
     const T* w = s.weight;
     const T* c = s.center;
     const T alongN = w[0] * nx + w[1] * ny + w[2] * nz;
@@ -563,7 +578,7 @@ struct NarrowT {
     return true;
   }
   // rests: src/collide.js:1151-1164.
-  bool rests(const Shape& s, T nx, T ny, T nz) {
+  NW_HD bool rests(const Shape& s, T nx, T ny, T nz) {
     if (!foot(s, nx, ny, nz)) return false;
     const T px = FOOT[0], py = FOOT[1], pz = FOOT[2];
     int from = FOUR[0];
@@ -578,7 +593,7 @@ struct NarrowT {
     return true;
   }
   // under: src/collide.js:1185-1194.
-  int under(int n, T nx, T ny, T nz, T pressed) {
+  NW_HD int under(int n, T nx, T ny, T nz, T pressed) {
     int start = -1;
     T nearest = INF;
     for (int k = 0; k < n; k++) {
@@ -591,7 +606,7 @@ struct NarrowT {
     return start;
   }
   // reducePoints: src/collide.js:1077-1104.
-  void reducePoints(int n, T nx, T ny, T nz, T tolerance, Manifold& out) {
+  NW_HD void reducePoints(int n, T nx, T ny, T nz, T tolerance, Manifold& out) {
     if (n <= MAX_POINTS) {
       for (int k = 0; k < n; k++) addPoint(out, kept[3 * k], kept[3 * k + 1], kept[3 * k + 2], keptSep[k], keptId[k]);
       return;
@@ -618,7 +633,7 @@ struct NarrowT {
     if (d >= 0) addPoint(out, kept[3 * d], kept[3 * d + 1], kept[3 * d + 2], keptSep[d], keptId[d]);
   }
   // faceContact: src/collide.js:884-945.
-  void faceContact(const Shape& ref, const Shape& inc, int axis, bool flipped, T margin, T tolerance,
+  NW_HD void faceContact(const Shape& ref, const Shape& inc, int axis, bool flipped, T margin, T tolerance,
                    Manifold& out) {
     const T* R = ref.axes;
     const T* I = inc.axes;
@@ -641,7 +656,7 @@ struct NarrowT {
     const T cy = inc.center[1] + I[3 * incAxis + 1] * incSign * hi[incAxis];
     const T cz = inc.center[2] + I[3 * incAxis + 2] * incSign * hi[incAxis];
     for (int v = 0; v < 4; v++) {
-      const T sp = CORNER_P[v], sq = CORNER_Q[v];
+      const T sp = corner_p(v), sq = corner_q(v);
       polyA[3 * v] = cx + I[3 * p] * sp * hi[p] + I[3 * q] * sq * hi[q];
       polyA[3 * v + 1] = cy + I[3 * p + 1] * sp * hi[p] + I[3 * q + 1] * sq * hi[q];
       polyA[3 * v + 2] = cz + I[3 * p + 2] * sp * hi[p] + I[3 * q + 2] * sq * hi[q];
@@ -671,7 +686,7 @@ struct NarrowT {
       const T m = separation * 0.5;
       kept[3 * n] = vx - nx * m; kept[3 * n + 1] = vy - ny * m; kept[3 * n + 2] = vz - nz * m;
       keptSep[n] = separation;
-      keptId[n] = flipped ? (static_cast<uint32_t>(incFace) << 9) | (static_cast<uint32_t>(refFace) << 6) | swapped().f[feat[v]]
+      keptId[n] = flipped ? (static_cast<uint32_t>(incFace) << 9) | (static_cast<uint32_t>(refFace) << 6) | static_cast<uint32_t>(swapped_feature(feat[v]))
                           : (static_cast<uint32_t>(refFace) << 9) | (static_cast<uint32_t>(incFace) << 6) | static_cast<uint32_t>(feat[v]);
       n++;
     }
@@ -681,7 +696,7 @@ struct NarrowT {
     reducePoints(n, nx, ny, nz, tolerance, out);
   }
   // boxEdge: src/collide.js:1218-1229.
-  static void boxEdge(const Shape& x, int i, T nx, T ny, T nz, T* s) {
+  NW_HD static void boxEdge(const Shape& x, int i, T nx, T ny, T nz, T* s) {
     const T* X = x.axes;
     const T* h = x.half;
     T cx = x.center[0], cy = x.center[1], cz = x.center[2];
@@ -695,7 +710,7 @@ struct NarrowT {
     s[3] = cx + ex; s[4] = cy + ey; s[5] = cz + ez;
   }
   // edgeContact: src/collide.js:1201-1215.
-  void edgeContact(const Shape& a, const Shape& b, int i, int j, T nx, T ny, T nz, T margin,
+  NW_HD void edgeContact(const Shape& a, const Shape& b, int i, int j, T nx, T ny, T nz, T margin,
                    Manifold& out) {
     boxEdge(a, i, nx, ny, nz, segA);
     boxEdge(b, j, -nx, -ny, -nz, segB);
@@ -712,7 +727,7 @@ struct NarrowT {
              (1u << 13) | static_cast<uint32_t>(3 * i + j));
   }
   // boxBox: src/collide.js:713-775.
-  void boxBox(const Shape& a, const Shape& b, T margin, T tolerance, Manifold& out) {
+  NW_HD void boxBox(const Shape& a, const Shape& b, T margin, T tolerance, Manifold& out) {
     const T* A = a.axes;
     const T* B = b.axes;
     const T* ha = a.half;
@@ -766,7 +781,7 @@ struct NarrowT {
   }
 
   // pair: src/collide.js:225-242 (spheres, capsules and boxes).
-  void pair(const Shape& a, const Shape& b, T margin, T tolerance, Manifold& out) {
+  NW_HD void pair(const Shape& a, const Shape& b, T margin, T tolerance, Manifold& out) {
     if (a.kind == K_SPHERE) {
       if (b.kind == K_SPHERE) sphereSphere(a, b, margin, out);
       else if (b.kind == K_CAPSULE) sphereCapsule(a, b, margin, out);
@@ -785,7 +800,7 @@ struct NarrowT {
 
 // collide(a, b, margin, tolerance, out): src/collide.js:204-218.  Returns the point count.
 template <class T>
-int collideT(const ShapeT<T>& a, const ShapeT<T>& b, double margin, double tolerance, ManifoldT<T>& out) {
+NW_HD int collideT(const ShapeT<T>& a, const ShapeT<T>& b, double margin, double tolerance, ManifoldT<T>& out) {
   narrow_detail::NarrowT<T> nw;
   out.count = 0;
   out.loss = 0;

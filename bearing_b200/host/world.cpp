@@ -466,10 +466,15 @@ struct bw_world {
     }
   }
 
+  // The pairs narrow() handed to collide() this step, with the margin and tolerance it passed.
+  std::vector<int32_t> narrowA, narrowB;
+  std::vector<double> narrowMargin, narrowTol;
+
   // narrow(): src/contact.js:296-327 with find() 334-368 (no reuse cache, no time of impact).
   void narrow() {
     Shape sa, sb;
     Manifold mf;
+    narrowA.clear(); narrowB.clear(); narrowMargin.clear(); narrowTol.clear();
     for (int p = 0; p < pairs.active;) {
       const int a = pairs.a[p], b = pairs.b[p];
       if (!fatOverlap(a, b)) {
@@ -485,6 +490,7 @@ struct bw_world {
         met = false;
       } else {
         const double margin = motion[a] + motion[b] + tol;
+        narrowA.push_back(a); narrowB.push_back(b); narrowMargin.push_back(margin); narrowTol.push_back(tol);
         load(a, sa);
         load(b, sb);
         if (bearing::collide(sa, sb, margin, tol, mf) == 0) {
@@ -889,6 +895,70 @@ int32_t bw_copy(bw_world* dst, const bw_world* src) {
   } catch (const std::exception&) {
     return BG_ENOMEM;
   }
+  return BG_OK;
+}
+
+int32_t bw_narrow_pairs(const bw_world* w, bg_pairs* out) {
+  if (w == nullptr || out == nullptr) return BG_EINVAL;
+  out->count = static_cast<int32_t>(w->narrowA.size());
+  out->a = w->narrowA.data();
+  out->b = w->narrowB.data();
+  out->margin = w->narrowMargin.data();
+  out->tolerance = w->narrowTol.data();
+  return BG_OK;
+}
+
+int32_t bw_collide_pairs(const bg_bodies* B, const double* gravity, const bg_pairs* pairs, bg_manifolds* out,
+                         int32_t threads) {
+  if (B == nullptr || gravity == nullptr || pairs == nullptr || out == nullptr || pairs->count < 0) return BG_EINVAL;
+  const int n = pairs->count;
+  if (n > 0 && (pairs->a == nullptr || pairs->b == nullptr || pairs->margin == nullptr || pairs->tolerance == nullptr ||
+                out->points == nullptr || out->normal == nullptr || out->point == nullptr ||
+                out->separation == nullptr || out->pid == nullptr || B->position == nullptr ||
+                B->rotation == nullptr || B->dims == nullptr || B->shape == nullptr || B->type == nullptr ||
+                B->gravity_scale == nullptr))
+    return BG_EINVAL;
+  for (int i = 0; i < n; i++)
+    if (pairs->a[i] < 0 || pairs->a[i] >= B->capacity || pairs->b[i] < 0 || pairs->b[i] >= B->capacity) return BG_EINVAL;
+  // load(), from the columns: the same shapes the step's narrowphase builds
+  auto shape_of = [&](int slot, Shape& s) {
+    const double* d = B->dims + 3 * slot;
+    if (B->shape[slot] == BG_BOX) {
+      s.kind = bearing::K_BOX;
+      s.half[0] = d[0] * 0.5; s.half[1] = d[1] * 0.5; s.half[2] = d[2] * 0.5;
+    } else if (B->shape[slot] == BG_SPHERE) {
+      s.kind = bearing::K_SPHERE;
+      s.half[0] = d[0]; s.half[1] = 0; s.half[2] = 0;
+    } else {
+      s.kind = bearing::K_CAPSULE;
+      s.half[0] = d[0]; s.half[1] = (d[1] - 2 * d[0]) * 0.5; s.half[2] = 0;
+    }
+    for (int k = 0; k < 3; k++) s.center[k] = B->position[3 * slot + k];
+    const double scale = B->type[slot] == BG_DYNAMIC ? B->gravity_scale[slot] : 0;
+    for (int k = 0; k < 3; k++) s.weight[k] = gravity[k] * scale;
+    axesOf(B->rotation + 4 * slot, s.axes);
+  };
+  const int nt = std::max(1, std::min<int>(threads, 64));
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; t++)
+    pool.emplace_back([&, t]() {
+      Shape sa, sb;
+      Manifold mf;
+      for (int i = static_cast<int>(static_cast<int64_t>(n) * t / nt); i < static_cast<int64_t>(n) * (t + 1) / nt; i++) {
+        shape_of(pairs->a[i], sa);
+        shape_of(pairs->b[i], sb);
+        const int count = bearing::collide(sa, sb, pairs->margin[i], pairs->tolerance[i], mf);
+        out->points[i] = static_cast<uint8_t>(count);
+        for (int k = 0; k < 3; k++) out->normal[3 * i + k] = count > 0 ? mf.normal[k] : 0;
+        for (int k = 0; k < P; k++) {
+          const bool used = k < count;
+          for (int q = 0; q < 3; q++) out->point[3 * (P * i + k) + q] = used ? mf.points[3 * k + q] : 0;
+          out->separation[P * i + k] = used ? mf.separations[k] : 0;
+          out->pid[P * i + k] = used ? mf.ids[k] : 0;
+        }
+      }
+    });
+  for (auto& th : pool) th.join();
   return BG_OK;
 }
 

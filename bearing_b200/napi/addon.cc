@@ -64,16 +64,10 @@ napi_value Create(napi_env env, napi_callback_info info) {
   return out;
 }
 
-// solveStep(ctx, world, contacts, dt, substeps) -> 0 or a BG_E* code: src/world.js:962-1032.
-napi_value SolveStep(napi_env env, napi_callback_info info) {
-  size_t argc = 5;
-  napi_value argv[5];
-  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
-  if (argc < 5) return fail(env, "solveStep(ctx, world, contacts, dt, substeps)");
-  bg_ctx* ctx = nullptr;
-  napi_get_value_external(env, argv[0], reinterpret_cast<void**>(&ctx));
-  napi_value w = argv[1], c = argv[2];
-  bg_bodies B;
+// World's and Contacts' own typed arrays as bg_bodies / bg_rows; false (with an exception
+// pending) if one is missing or of the wrong type.  sliding, anchorA and anchorB stay NULL: after
+// the stage only slipped() reads them, and the device runs it (src/contact.js:1122-1182).
+bool views(napi_env env, napi_value w, napi_value c, bg_bodies& B, bg_rows& R) {
   std::memset(&B, 0, sizeof B);
   B.capacity = number(env, w, "_capacity");
   B.awake_count = number(env, w, "_awakeCount");
@@ -101,7 +95,6 @@ napi_value SolveStep(napi_env env, napi_callback_info info) {
   B.framed = static_cast<const uint8_t*>(column(env, w, "_framed", napi_uint8_array));
   B.lock = static_cast<const uint8_t*>(column(env, w, "_lock", napi_uint8_array));
   B.joint_head = static_cast<const int32_t*>(column(env, w, "_jointHead", napi_int32_array));
-  bg_rows R;
   std::memset(&R, 0, sizeof R);
   R.count = number(env, c, "count");
   R.solved = number(env, c, "solved");
@@ -132,12 +125,23 @@ napi_value SolveStep(napi_env env, napi_callback_info info) {
   R.gap = static_cast<double*>(column(env, c, "gap", napi_float64_array));
   R.max_normal_impulse = static_cast<double*>(column(env, c, "maxNormalImpulse", napi_float64_array));
   R.relative_velocity = static_cast<double*>(column(env, c, "relativeVelocity", napi_float64_array));
-  R.sliding = static_cast<uint8_t*>(column(env, c, "sliding", napi_uint8_array));
-  R.anchor_a = static_cast<double*>(column(env, c, "anchorA", napi_float64_array));
-  R.anchor_b = static_cast<double*>(column(env, c, "anchorB", napi_float64_array));
   bool pending = false;
   napi_is_exception_pending(env, &pending);
-  if (pending) return nullptr;
+  return !pending;
+}
+
+// solveStep(ctx, world, contacts, dt, substeps) -> 0 or a BG_E* code: src/world.js:962-1032.
+napi_value SolveStep(napi_env env, napi_callback_info info) {
+  size_t argc = 5;
+  napi_value argv[5];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  if (argc < 5) return fail(env, "solveStep(ctx, world, contacts, dt, substeps)");
+  bg_ctx* ctx = nullptr;
+  napi_get_value_external(env, argv[0], reinterpret_cast<void**>(&ctx));
+  napi_value w = argv[1], c = argv[2];
+  bg_bodies B;
+  bg_rows R;
+  if (!views(env, w, c, B, R)) return nullptr;
   bg_step S;
   napi_get_value_double(env, argv[3], &S.dt);
   napi_get_value_int32(env, argv[4], &S.substeps);
@@ -150,6 +154,25 @@ napi_value SolveStep(napi_env env, napi_callback_info info) {
   }
   napi_value out;
   napi_create_int32(env, bg_solve_step(ctx, &B, &R, &S), &out);
+  return out;
+}
+
+// registerHost(ctx, world, contacts) -> 0 or a BG_E* code: page-locks the World's and Contacts'
+// typed arrays in place (bg_register_host), for contacts.capacity rows.  Called once, and again
+// whenever either has grown (Contacts._alloc, src/contact.js:184-255), so that solveStep copies
+// them straight to and from the device.
+napi_value RegisterHost(napi_env env, napi_callback_info info) {
+  size_t argc = 3;
+  napi_value argv[3];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  if (argc < 3) return fail(env, "registerHost(ctx, world, contacts)");
+  bg_ctx* ctx = nullptr;
+  napi_get_value_external(env, argv[0], reinterpret_cast<void**>(&ctx));
+  bg_bodies B;
+  bg_rows R;
+  if (!views(env, argv[1], argv[2], B, R)) return nullptr;
+  napi_value out;
+  napi_create_int32(env, bg_register_host(ctx, &B, &R, number(env, argv[2], "capacity")), &out);
   return out;
 }
 
@@ -168,9 +191,10 @@ napi_value Init(napi_env env, napi_value exports) {
   napi_property_descriptor props[] = {
       {"create", nullptr, Create, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"solveStep", nullptr, SolveStep, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"registerHost", nullptr, RegisterHost, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"lastError", nullptr, LastError, nullptr, nullptr, nullptr, napi_default, nullptr},
   };
-  napi_define_properties(env, exports, 3, props);
+  napi_define_properties(env, exports, sizeof props / sizeof props[0], props);
   return exports;
 }
 

@@ -199,16 +199,33 @@ def time_resident(lib, ctx, copy, steps, warmup, torch):
     return times, stage, launches, out
 
 
-def time_e2e(lib, ctx, copy, steps, warmup, torch, pinned=True):
-    """bg_solve_step with host arrays in page-locked memory (as a World that keeps its columns
-    pinned passes them), or in ordinary pageable memory: uploads, solve and downloads inside the
-    timed region.  The arrays are refilled with the step's input, untimed, before every call."""
+def host_views(work):
+    """The views bg_solve_step gets from a World: every column, except the three written columns
+    only slipped() reads after the stage (sliding, anchor_a, anchor_b), which it runs on the device
+    itself; those are NULL and not copied back."""
+    B, R, S = work.views()
+    R.sliding = None
+    R.anchor_a = None
+    R.anchor_b = None
+    return B, R, S
+
+
+def time_e2e(lib, ctx, copy, steps, warmup, torch, host="page-locked"):
+    """bg_solve_step end to end: uploads, solve and downloads inside the timed region.  `host` is
+    where the caller's columns live: "page-locked" (allocated pinned, as a World that keeps its
+    columns pinned passes them), "registered" (ordinary arrays, page-locked in place once by
+    bg_register_host, as a World does when its columns are made or grow) or "pageable" (ordinary
+    arrays).  The arrays are refilled with the step's input, untimed, before every call."""
     stream = torch.cuda.ExternalStream(lib.bg_stream(ctx))
-    work = copy.pinned() if pinned else copy.copy()
+    work = copy.pinned() if host == "page-locked" else copy.copy()
+    if host == "registered":
+        B, R, _ = host_views(work)
+        rc = lib.bg_register_host(ctx, C.byref(B), C.byref(R), work.count)
+        assert rc == 0, lib.bg_last_error(ctx)
     times = []
     for i in range(warmup + steps):
         work.fill(copy)
-        B, R, S = work.views()
+        B, R, S = host_views(work)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         rc = lib.bg_solve_step(ctx, C.byref(B), C.byref(R), C.byref(S))
@@ -217,18 +234,20 @@ def time_e2e(lib, ctx, copy, steps, warmup, torch, pinned=True):
         e1.synchronize()
         if i >= warmup:
             times.append(e0.elapsed_time(e1))
+    if host == "registered":
+        assert lib.bg_unregister_host(ctx) == 0
     return times
 
 
 def io_bytes(copy):
-    """Bytes bg_solve_step copies in and out per step, from the columns it moves."""
-    from stage_io import BODY_COLUMNS, ROW_COLUMNS, BODY_OUT, ROW_OUT, ROW_OUT_SOLVED
-    import numpy as np
-    h2d_body = [f for f, _, _ in BODY_COLUMNS if f not in ("start_q",)]
+    """Bytes bg_solve_step copies in and out per step, from the columns it moves: every body and row
+    column in (the output-only sliding and anchors excepted), and every written column out but the
+    three host_views leaves NULL."""
+    from stage_io import BODY_COLUMNS, ROW_COLUMNS, BODY_OUT, ROW_OUT
     h2d_row = [f for f, _, _ in ROW_COLUMNS if f not in ("sliding", "anchor_a", "anchor_b")]
-    h2d = sum(copy.body[f].nbytes for f in h2d_body) + copy.awake_list.nbytes + sum(copy.rows[f].nbytes for f in h2d_row)
-    d2h_body = BODY_OUT + ["start_q"]
-    d2h = sum(copy.body[f].nbytes for f in d2h_body) + sum(copy.rows[f].nbytes for f in ROW_OUT + ROW_OUT_SOLVED)
+    h2d = sum(copy.body[f].nbytes for f, _, _ in BODY_COLUMNS) + copy.awake_list.nbytes + \
+        sum(copy.rows[f].nbytes for f in h2d_row)
+    d2h = sum(copy.body[f].nbytes for f in BODY_OUT) + sum(copy.rows[f].nbytes for f in ROW_OUT)
     return int(h2d), int(d2h)
 
 
@@ -435,6 +454,7 @@ def measure_adjoint(args, device, log):
             "unit": "tower-gradients/s", "value": n / (out["forward_s"] + out["backward_s"]),
             "forward_s": out["forward_s"], "backward_s": out["backward_s"], "wall_s": wall,
             "adjoint_kernel_s": out["device_ms"] / 1000, "tape_peak_nodes": out["tape_peak"],
+            "backward_parts_s": out["backward_parts"],
             "check": {"worlds": sample, "max_rel_err_vs_dual_numbers": worst},
             "cpu_baseline": {"value": 1 / cpu_s, "unit": "tower-gradients/s", "cores": 1, "kind": "port",
                              "sample": f"{sample} towers' dual-number runs (the oracle, 5 directions) on one "
@@ -558,16 +578,19 @@ def main():
     clock = clocks.stop()
     e2e_times = times if args.resident_only else time_e2e(lib, ctx, copy, args.steps, args.warmup, torch)
     pageable_times = times if args.resident_only else time_e2e(lib, ctx, copy, args.steps, args.warmup, torch,
-                                                                pinned=False)
+                                                                host="pageable")
+    registered_times = times if args.resident_only else time_e2e(lib, ctx, copy, args.steps, args.warmup, torch,
+                                                                  host="registered")
     torch.cuda.synchronize()
     ms = statistics.mean(times)
     ms_e2e = statistics.mean(e2e_times)
     ms_pageable = statistics.mean(pageable_times)
+    ms_registered = statistics.mean(registered_times)
     ms_stage = statistics.mean(stage)
     if dist:
-        t = torch.tensor([ms, ms_e2e, ms_stage, ms_pageable], device="cuda", dtype=torch.float64)
+        t = torch.tensor([ms, ms_e2e, ms_stage, ms_pageable, ms_registered], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e, ms_stage, ms_pageable = (float(x) for x in t.tolist())
+        ms, ms_e2e, ms_stage, ms_pageable, ms_registered = (float(x) for x in t.tolist())
     rows_per_stage = copy.solved * SUBSTEPS * 3
     value = world_size * rows_per_stage / (ms / 1000)
     e2e = world_size * rows_per_stage / (ms_e2e / 1000)
@@ -601,6 +624,9 @@ def main():
                         "d2h_bytes_per_step": d2h, "host_memory": "page-locked"},
                 "e2e_pageable": {"value": world_size * rows_per_stage / (ms_pageable / 1000), "unit": "rows/s",
                                  "ms_per_step": ms_pageable, "host_memory": "pageable (ordinary numpy arrays)"},
+                "e2e_registered": {"value": world_size * rows_per_stage / (ms_registered / 1000), "unit": "rows/s",
+                                   "ms_per_step": ms_registered,
+                                   "host_memory": "ordinary numpy arrays page-locked in place once by bg_register_host"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": measured_traffic(args.bodies, algo),
                              "traffic_source": "ncu capture at step 101, scaled by algorithmic bytes", "kernel_ms": ms_stage,

@@ -63,7 +63,8 @@ extern "C" {
 /* bg_create flags */
 #define BG_FLAG_NONE 0u
 /* Reserved (accepted, no effect).  Every transfer already takes the fastest route by itself: a
- * column in page-locked host memory (cudaHostAlloc'd or registered by the caller) is copied to and
+ * column in page-locked host memory (cudaHostAlloc'd, or registered by the caller or through
+ * bg_register_host) is copied to and
  * from directly; any other column goes through the library's own pinned staging, gathered and
  * scattered by a pool of host threads. */
 #define BG_FLAG_PIN_HOST 1u
@@ -155,9 +156,11 @@ typedef struct bg_rows {
   double* gap;                 /* least separation as the last pass saw it */
   double* max_normal_impulse;  /* 4 per row */
   double* relative_velocity;   /* 4 per row */
+  /* written, and read after the stage by nothing but slipped() (src/contact.js:1125-1160), which
+   * runs on the device: each may be NULL, and is then not copied back */
   uint8_t* sliding;
-  double* anchor_a;            /* 3 per row, may be NULL */
-  double* anchor_b;            /* 3 per row, may be NULL */
+  double* anchor_a;            /* 3 per row */
+  double* anchor_b;            /* 3 per row */
 } bg_rows;
 
 typedef struct bg_step {
@@ -214,6 +217,26 @@ int32_t bg_batch_solve_step(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows*
 int32_t bg_batch_upload(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows, const bg_worlds* worlds);
 int32_t bg_batch_solve(bg_ctx* ctx, const bg_step* step);
 int32_t bg_batch_download(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows);
+
+/*
+ * Page-locks the caller's own long-lived columns (cudaHostRegister), so that the copies of every
+ * later call go straight between them and the device, with no gather through the library's
+ * staging block.  A Bearing World keeps its columns in typed arrays that live until they grow
+ * (src/world.js:228-311, src/contact.js:196-248); this is the call a World makes once, and again
+ * after either grows.  Every non-NULL column of `bodies` is registered for bodies->capacity slots
+ * (awake_list: capacity entries) and of `rows` for `row_capacity` rows (>= rows->count: the
+ * columns' allocated length).  Columns that share pages are registered as one range.  A call
+ * replaces the ranges this context registered before (waiting for its stream first); a range
+ * that CUDA reports as registered already (by another context, say) is left to its owner.
+ * bg_unregister_host releases them, as does bg_destroy.  Until then the memory must stay
+ * allocated: free or move it only after either.  A column that a call's copy would read or write
+ * past its registered range (rows grew past row_capacity) is staged as if never registered.
+ * Results never depend on it.
+ */
+int32_t bg_register_host(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows, int32_t row_capacity);
+int32_t bg_unregister_host(bg_ctx* ctx);
+/* Bytes this context holds page-locked by bg_register_host (0 if none). */
+int64_t bg_registered_bytes(const bg_ctx* ctx);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
 void* bg_stream(bg_ctx* ctx);
@@ -327,6 +350,38 @@ double bg_backward_ms(bg_ctx* ctx);
 #define BG_STATIC_MAX_BODIES 512
 #define BG_STATIC_MAX_ROWS 2048
 int32_t bg_solve_step_static(const bg_bodies* bodies, const bg_rows* rows, const bg_step* step, void* stream);
+
+/*
+ * The narrowphase on the device, for spheres, capsules and boxes: what src/contact.js narrow()
+ * asks of src/collide.js collide(a, b, margin, tolerance) for each pair whose boxes meet
+ * (src/contact.js:296-368, src/collide.js:204-1229), one pair a thread.  Each pair's manifold has
+ * the reference's normal (from a to b), points, separations and feature ids, bit for bit; a pair
+ * that does not touch has 0 points.  Entries past a pair's point count are 0.
+ * Reads bodies' capacity, position, rotation, dims, shape, type and gravity_scale (the rest may be
+ * NULL); a body's axes are worked out from its rotation as src/core/math.js:222-227 does, and its
+ * weight (the direction reducePoints() leans on, src/collide.js:1151-1178) is gravity times its
+ * gravity scale for a dynamic body, 0 otherwise.  Synchronous.
+ */
+typedef struct bg_pairs {
+  int32_t count;
+  const int32_t* a;            /* each pair's slots, as narrow() hands them to collide() */
+  const int32_t* b;
+  const double* margin;        /* motion[a] + motion[b] + tolerance (src/contact.js:351) */
+  const double* tolerance;     /* min(size[a], size[b]) * PIXEL (src/contact.js:316) */
+} bg_pairs;
+
+typedef struct bg_manifolds {
+  uint8_t* points;             /* 0..BG_POINTS per pair */
+  double* normal;              /* 3 per pair */
+  double* point;               /* 3 * BG_POINTS per pair */
+  double* separation;          /* BG_POINTS per pair */
+  uint32_t* pid;               /* BG_POINTS per pair */
+} bg_manifolds;
+
+int32_t bg_collide(bg_ctx* ctx, const bg_bodies* bodies, const double* gravity, const bg_pairs* pairs,
+                   bg_manifolds* out);
+/* Device time in milliseconds of the last bg_collide's kernel (synchronises; negative if none). */
+double bg_last_collide_ms(bg_ctx* ctx);
 
 #ifdef __cplusplus
 }

@@ -123,6 +123,15 @@ int32_t bw_row_memory_get(const bw_world* world, bw_row_memory* out);
 /* The same for a batch after bw_batch_begin_step, rows end to end as bw_batch_views lays them. */
 int32_t bw_batch_row_memory(const bw_batch* batch, bw_row_memory* out);
 
+/* The pairs the last bw_begin_step's narrowphase handed to collide() (src/contact.js:351-356:
+ * those whose boxes met), in the order it took them, with the margin and tolerance it passed:
+ * views into the world's own arrays, valid until its next step.  bw_collide_pairs runs the host's
+ * narrowphase (the one the step itself uses) over any such list, with the bodies' current poses:
+ * what bg_collide does on the device. */
+int32_t bw_narrow_pairs(const bw_world* world, bg_pairs* out);
+int32_t bw_collide_pairs(const bg_bodies* bodies, const double* gravity, const bg_pairs* pairs, bg_manifolds* out,
+                         int32_t threads);
+
 /* A deep copy of a world (its bodies, pairs with their memory, broadphase and step count), for
  * checkpoints; bw_destroy frees it.  NULL if out of memory.  bw_copy makes dst a copy of src. */
 bw_world* bw_clone(const bw_world* world);

@@ -46,6 +46,9 @@ def test_calls_on_a_null_context_are_refused():
     assert g.bg_solve(None, None) == _ffi.BG_EINVAL
     assert g.bg_restore(None) == _ffi.BG_EINVAL
     assert g.bg_upload(None, None, None) == _ffi.BG_EINVAL
+    assert g.bg_register_host(None, None, None, 0) == _ffi.BG_EINVAL
+    assert g.bg_unregister_host(None) == _ffi.BG_EINVAL
+    assert g.bg_registered_bytes(None) == 0
     assert g.bg_last_error(None) == b"no context"
     g.bg_destroy(None)
 

@@ -1,0 +1,75 @@
+"""The pair list a step's narrowphase worked on (bw_narrow_pairs) and the host's narrowphase over
+such a list (bw_collide_pairs), on the CPU: run over the list the world recorded, the narrowphase
+finds exactly the manifolds the world emitted as rows (their count, normal, points and
+separations, in found order), so the list is the narrowphase's whole input and the device
+narrowphase (bg_collide) can be checked against it pair by pair."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import narrow_io
+import oracle_io
+from stage_io import StageCopy
+from bearing_b200 import _ffi, scenes
+from bearing_b200.world import World
+
+DT = 1 / 60
+P = _ffi.BG_POINTS
+
+
+def boxes_and_balls(w):
+    scenes.pile(w, count=600, seed=7, extent=10.0)
+
+
+def raining(w):
+    scenes.rain(w, count=150, seed=3)
+
+
+@pytest.mark.parametrize("build,steps", [(scenes.pyramid, 10), (boxes_and_balls, 40), (raining, 90)],
+                         ids=["pyramid", "pile600", "rain150"])
+def test_the_recorded_pairs_give_the_worlds_rows(build, steps):
+    w = World({}, solver=oracle_io.solver(0))
+    build(w)
+    for _ in range(steps):
+        w.step(DT)
+    w.begin_step(DT)
+    pairs = narrow_io.world_pairs(w)
+    assert pairs.count > 0
+    B, R, S = w.views()
+    got = narrow_io.host_collide(B, tuple(S.gravity), pairs)
+    rows = StageCopy(w)
+    met = np.flatnonzero(got.points[: pairs.count] > 0)
+    assert met.size == rows.count   # every met pair is a row, in found order
+    for f, i in enumerate(met):
+        m = int(rows.rows["row"][f])
+        n = int(got.points[i])
+        assert rows.rows["points"][m] == n
+        assert rows.rows["a"][m] == pairs.a[i] and rows.rows["b"][m] == pairs.b[i]
+        assert got.normal[3 * i: 3 * i + 3].tobytes() == rows.rows["normal"][3 * m: 3 * m + 3].tobytes()
+        assert got.separation[P * i: P * i + n].tobytes() == rows.rows["separation"][P * m: P * m + n].tobytes()
+        assert got.point[3 * P * i: 3 * P * i + 3 * n].tobytes() == \
+            rows.rows["point"][3 * P * m: 3 * P * m + 3 * n].tobytes()
+    # a pair with no contact leaves zeros, as do the entries past a manifold's points
+    empty = got.points[: pairs.count] == 0
+    assert not got.normal[: 3 * pairs.count].reshape(-1, 3)[empty].any()
+    counts = got.points[: pairs.count].astype(np.int64)
+    unused = np.arange(P)[None, :] >= counts[:, None]
+    assert not got.separation[: P * pairs.count].reshape(-1, P)[unused].any()
+    assert not got.pid[: P * pairs.count].reshape(-1, P)[unused].any()
+    w.destroy()
+
+
+def test_bad_slots_are_refused():
+    w = World({}, solver=oracle_io.solver(0))
+    scenes.pyramid(w, rows=3)
+    w.begin_step(DT)
+    pairs = narrow_io.world_pairs(w)
+    B, _, S = w.views()
+    pairs.b[0] = B.capacity
+    out = narrow_io.ManifoldSet(pairs.count)
+    g = np.zeros(3)
+    rc = _ffi.host().bw_collide_pairs(C.byref(B), g.ctypes.data_as(C.POINTER(C.c_double)), C.byref(pairs.view()),
+                                      C.byref(out.s), 1)
+    assert rc == _ffi.BG_EINVAL
+    w.destroy()
