@@ -299,6 +299,8 @@ def gpu() -> C.CDLL:
         lib.bg_unregister_host.restype = C.c_int32
         lib.bg_registered_bytes.argtypes = [C.c_void_p]
         lib.bg_registered_bytes.restype = C.c_int64
+        lib.bg_backward_bytes.argtypes = [C.c_void_p]
+        lib.bg_backward_bytes.restype = C.c_int64
         lib.bg_collide.argtypes = [C.c_void_p, C.POINTER(Bodies), _d, C.POINTER(Pairs), C.POINTER(Manifolds)]
         lib.bg_collide.restype = C.c_int32
         lib.bg_last_collide_ms.argtypes = [C.c_void_p]
@@ -337,7 +339,7 @@ GPU_SYMBOLS = [
     "bg_batch_download", "bg_stream", "bg_last_launches", "bg_last_stage_ms", "bg_set_wait_budget", "bg_set_block_threads",
     "bg_block_threads", "bg_set_batch_groups", "bg_backward", "bg_backward_tape_peak", "bg_backward_ms",
     "bg_solve_step_static", "bg_register_host", "bg_unregister_host", "bg_registered_bytes", "bg_collide",
-    "bg_last_collide_ms",
+    "bg_last_collide_ms", "bg_backward_bytes",
 ]
 HOST_SYMBOLS = [
     "bw_create", "bw_destroy", "bw_last_error", "bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step",

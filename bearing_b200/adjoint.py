@@ -182,6 +182,7 @@ class BatchBackward:
             self.restitution[o: o + w._count] = re
         self.gravity = np.zeros(3)
         self.device_ms = 0.0
+        self.device_bytes = 0
         self.tape_peak = 0
         # host seconds of the backward pass, by part (bg_backward's is its wall time, kernel included)
         self.times = {"recompute": 0.0, "keep_backward": 0.0, "stage_backward": 0.0, "narrow_backward": 0.0}
@@ -252,6 +253,7 @@ class BatchBackward:
         if rc != 0:
             raise RuntimeError(f"bg_backward: {rc} {self.gpu.bg_last_error(self.ctx).decode()}")
         self.device_ms += self.gpu.bg_backward_ms(self.ctx)
+        self.device_bytes += self.gpu.bg_backward_bytes(self.ctx)
         self.tape_peak = max(self.tape_peak, self.gpu.bg_backward_tape_peak(self.ctx))
         for f in ("normal", "t1", "t2"):   # keep() read these too
             row_grad[f][: 3 * nr] += seed[f][: 3 * nr]
@@ -340,7 +342,8 @@ def tower_gradients(count, seed=5000, steps=120, dt=1 / 60, checkpoint=20, first
             ball = o + info["ball"]
             grads[i, 2:] = bar["velocity"][3 * ball: 3 * ball + 3]
         return dict(gradients=grads, losses=np.array(losses), position=position, forward_s=t1 - t0,
-                    backward_s=t2 - t1, device_ms=bb.device_ms, tape_peak=bb.tape_peak, infos=infos,
+                    backward_s=t2 - t1, device_ms=bb.device_ms, device_bytes=bb.device_bytes, tape_peak=bb.tape_peak,
+                    infos=infos,
                     backward_parts=dict(bb.times))
     finally:
         bb.close()

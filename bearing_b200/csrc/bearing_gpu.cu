@@ -526,6 +526,7 @@ struct bg_ctx {
     cudaEvent_t begin = nullptr, end = nullptr;
     int peak = 0;
     bool timed = false;
+    int64_t bytes = 0;   // what the last kernel moves by design (see bg_backward_bytes)
   } adj;
 };
 
@@ -2185,6 +2186,21 @@ int32_t bg_backward(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_wo
     cudaEventCreate(&d.begin);
     cudaEventCreate(&d.end);
   }
+  // The bytes the kernel moves by design, its roofline's numerator: each solved row, each pass, its
+  // record written by the recompute and read back by its replay, its prepared terms read and their
+  // adjoints read and written by the replay, and its state's adjoints read and written; each awake
+  // body, each substep, its record both ways and its 16 adjoints read and written.
+  {
+    int64_t solved = 0, awake = 0;
+    for (const bg::WorldDesc& w : worlds) {
+      solved += w.solved;
+      awake += w.nawake;
+    }
+    const int64_t passes = 3 * static_cast<int64_t>(S->substeps);
+    d.bytes = static_cast<int64_t>(sizeof(double)) *
+              (solved * passes * (2 * bgadj::REC_ROW + 3 * bgadj::PREP + 2 * bgadj::RSTATE) +
+               awake * S->substeps * (2 * bgadj::REC_BODY + 2 * 16));
+  }
   cudaEventRecord(d.begin, st);
   const int blocks = static_cast<int>(threads / kAdjointThreads);
   adjoint_step<<<blocks, kAdjointThreads, 0, st>>>(A, d.tapes);
@@ -2239,6 +2255,8 @@ int32_t bg_backward(bg_ctx* c, const bg_bodies* B, const bg_rows* R, const bg_wo
 }
 
 int32_t bg_backward_tape_peak(const bg_ctx* c) { return c == nullptr ? BG_EINVAL : c->adj.peak; }
+
+int64_t bg_backward_bytes(const bg_ctx* c) { return c == nullptr ? 0 : c->adj.bytes; }
 
 double bg_backward_ms(bg_ctx* c) {
   if (c == nullptr || !c->adj.timed) return -1.0;

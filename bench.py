@@ -455,10 +455,63 @@ def measure_adjoint(args, device, log):
             "forward_s": out["forward_s"], "backward_s": out["backward_s"], "wall_s": wall,
             "adjoint_kernel_s": out["device_ms"] / 1000, "tape_peak_nodes": out["tape_peak"],
             "backward_parts_s": out["backward_parts"],
+            "roofline": {"bound": "hbm", "kernel": "adjoint_step",
+                         "achieved": out["device_bytes"] / (out["device_ms"] / 1000) / 1e9, "peak": hbm_peak()[0],
+                         "unit": "GB/s", "frac": out["device_bytes"] / (out["device_ms"] / 1000) / 1e9 / hbm_peak()[0],
+                         "algorithmic_bytes": out["device_bytes"],
+                         "bytes_are": "each row's records, prepared terms and adjoints per pass, each body's per "
+                                      "substep (bg_backward_bytes), over the adjoint kernels' device time"},
             "check": {"worlds": sample, "max_rel_err_vs_dual_numbers": worst},
             "cpu_baseline": {"value": 1 / cpu_s, "unit": "tower-gradients/s", "cores": 1, "kind": "port",
                              "sample": f"{sample} towers' dual-number runs (the oracle, 5 directions) on one "
                                        f"thread"}}
+
+
+def measure_narrowphase(lib, ctx, world, steps, warmup, threads, log):
+    """The narrowphase of the same step on the device: bg_collide over the pairs the step's own
+    narrowphase handed to collide() (bw_narrow_pairs), with the world's bodies; the kernel's
+    device time and the call end to end (pairs and body columns in, manifolds out, on the host
+    clock), against the host's narrowphase over the same list on every host thread
+    (bw_collide_pairs), and the two results compared bit for bit."""
+    import numpy as np
+    import narrow_io
+    pairs = narrow_io.world_pairs(world)
+    B, _, S = world.views()
+    g = np.asarray(S.gravity, np.float64)
+    out = narrow_io.ManifoldSet(pairs.count)
+    view = pairs.view()
+    kernel, e2e = [], []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        rc = lib.bg_collide(ctx, C.byref(B), g.ctypes.data_as(C.POINTER(C.c_double)), C.byref(view), C.byref(out.s))
+        t1 = time.perf_counter()
+        assert rc == 0, lib.bg_last_error(ctx)
+        if i >= warmup:
+            e2e.append((t1 - t0) * 1000)
+            kernel.append(lib.bg_last_collide_ms(ctx))
+    cpu = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        host = narrow_io.host_collide(B, tuple(S.gravity), pairs, threads=threads)
+        cpu.append((time.perf_counter() - t0) * 1000)
+    same = narrow_io.first_unequal(host, out) is None
+    n = pairs.count
+    counts = np.bincount(out.points[:n], minlength=5)
+    in_bytes = n * (2 * 4 + 2 * 8) + B.capacity * (11 * 8 + 2)
+    out_bytes = n * (1 + 3 * 8 + 12 * 8 + 4 * 8 + 4 * 4)
+    k_ms, e_ms, c_ms = statistics.mean(kernel), statistics.mean(e2e), min(cpu)
+    if log:
+        log(f"narrowphase: {n} pairs, kernel {k_ms:.3f} ms, end to end {e_ms:.3f} ms, host {c_ms:.1f} ms "
+            f"({threads} threads), bit-identical {same}")
+    return {"workload": f"the pile's step-{world.stats()['step'] + 1} narrowphase: the pairs whose boxes meet",
+            "pairs": n, "manifolds_by_points": [int(x) for x in counts], "unit": "pairs/s",
+            "value": n / (k_ms / 1000), "kernel_ms": k_ms,
+            "e2e": {"value": n / (e_ms / 1000), "ms_per_step": e_ms, "h2d_bytes_per_step": int(in_bytes),
+                    "d2h_bytes_per_step": int(out_bytes)},
+            "cpu_baseline": {"value": n / (c_ms / 1000), "unit": "pairs/s", "cores": threads, "kind": "port",
+                             "ms": c_ms, "sample": "the same pair list through the host's narrowphase "
+                                                   "(bw_collide_pairs), every host thread"},
+            "bit_identical": same}
 
 
 def batch_roofline(algo, ms, cta_threads):
@@ -610,6 +663,9 @@ def main():
     batch = None
     if not args.no_batch and not args.resident_only:   # every rank, or none: it holds collectives
         batch = measure_batch(args, lib, torch, local, log, rank, world_size, dist)
+    narrow = None
+    if not args.resident_only and rank == 0:
+        narrow = measure_narrowphase(lib, ctx, w, args.steps, args.warmup, host_threads(), log)
     adj = None
     if not args.no_adjoint and not args.resident_only and rank == 0 and world_size == 1:
         adj = measure_adjoint(args, local, log)
@@ -631,7 +687,8 @@ def main():
                              "frac": achieved / hbm, "traffic": measured_traffic(args.bodies, algo),
                              "traffic_source": "ncu capture at step 101, scaled by algorithmic bytes", "kernel_ms": ms_stage,
                              "algorithmic_bytes": algo, "peak_source": peak_source},
-                "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches, "batch": batch, "adjoint": adj}
+                "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches, "batch": batch, "adjoint": adj,
+                "narrowphase": narrow}
         print(json.dumps(line), flush=True)
     lib.bg_destroy(ctx)
     solver.close()

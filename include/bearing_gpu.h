@@ -320,6 +320,10 @@ int32_t bg_backward(bg_ctx* ctx, const bg_bodies* bodies, const bg_rows* rows, c
 #define BG_TAPE_NODES 4096
 int32_t bg_backward_tape_peak(const bg_ctx* ctx);
 double bg_backward_ms(bg_ctx* ctx);
+/* The bytes the last bg_backward's kernel moves by its design (records written by the recompute
+ * and read by the replays, each replay's prepared terms and the adjoints it reads and writes):
+ * the numerator of its roofline. */
+int64_t bg_backward_bytes(const bg_ctx* ctx);
 
 /*
  * The solve stage without allocating: no counterpart in the reference.
