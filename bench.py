@@ -56,6 +56,10 @@ def parse():
     p.add_argument("--adjoint-worlds", type=int, default=1024, help="towers in the backward-pass measurement")
     p.add_argument("--adjoint-steps", type=int, default=120)
     p.add_argument("--no-adjoint", action="store_true", help="skip the backward-pass measurement")
+    p.add_argument("--save-input", default=None, help="write the timed solve stage's input to this .npz")
+    p.add_argument("--load-input", default=None,
+                   help="time the solve stage of an input written by --save-input instead of building the pile "
+                        "(a profiler then sees no launches of the pile's first steps)")
     return p.parse_args()
 
 
@@ -264,24 +268,26 @@ def cpu_solve_times(copy, workers, sample):
     return times
 
 
-def measured_traffic(bodies, algorithmic):
-    """DRAM bytes per launch of the stage kernel, from the committed ncu capture of the same pile
-    (profiles/stage_grid_pile50k_dram.md), scaled from the captured launch to this one by their
+def profiled(name):
+    """One entry of profiles/counters.json (the ncu counters the bench's rooflines use), or None."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "counters.json")))[name]
+    except (OSError, ValueError, KeyError):
+        return None
+
+
+def measured_traffic(bodies, at, algorithmic):
+    """DRAM bytes per launch of the stage kernel, from the committed ncu capture of the same input
+    (the pile's step 301); for another step of the same pile, scaled by the two launches'
     algorithmic bytes (the traffic grows with the rows and points a launch works through); None
     for another workload."""
-    if bodies != 50_000:
-        return None
-    got = {}
-    try:
-        for line in open(os.path.join(ROOT, "profiles", "stage_grid_pile50k_dram.md")):
-            key, _, value = line.partition(":")
-            if key in ("traffic_bytes_per_launch", "algorithmic_bytes_per_launch"):
-                got[key] = int(value)
-    except (OSError, ValueError):
-        return None
-    if len(got) != 2:
-        return None
-    return int(round(got["traffic_bytes_per_launch"] * algorithmic / got["algorithmic_bytes_per_launch"]))
+    got = profiled("stage_grid_pile50k_step301")
+    if bodies != 50_000 or got is None:
+        return None, None
+    if at == 300:
+        return int(got["traffic_bytes_per_launch"]), "ncu capture of this launch (profiles/counters.json)"
+    return int(round(got["traffic_bytes_per_launch"] * algorithmic / got["algorithmic_bytes_per_launch"])), \
+        "ncu capture at step 301, scaled by algorithmic bytes"
 
 
 def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None):
@@ -521,21 +527,14 @@ def batch_roofline(algo, ms, cta_threads):
     hbm, peak_source = hbm_peak()
     achieved = algo / (ms / 1000) / 1e9
     traffic = None
-    try:
-        got = {}
-        if cta_threads != 1:   # the capture is of the grid's kernel
-            raise OSError
-        for line in open(os.path.join(ROOT, "profiles", "stage_grid_batch_1024worlds.md")):
-            key, _, value = line.partition(":")
-            if key in ("traffic_bytes_per_launch", "algorithmic_bytes_per_launch"):
-                got[key] = int(value)
+    got = profiled("stage_grid_batch_1024worlds")
+    if got is not None and cta_threads == 1:   # the capture is of the grid's kernel
         traffic = int(round(got["traffic_bytes_per_launch"] * algo / got["algorithmic_bytes_per_launch"]))
-    except (OSError, ValueError, KeyError):
-        pass
     kernel = "stage_grid_batch" if cta_threads == 1 else f"stage_block ({cta_threads} threads a world)"
     return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "algorithmic_bytes": algo, "traffic": traffic,
-            "traffic_source": "ncu capture of 1,024 of the worlds, scaled by algorithmic bytes",
+            "traffic_source": "ncu capture of 1,024 of the worlds at step 61 (profiles/counters.json), scaled by "
+                              "algorithmic bytes",
             "peak_source": peak_source}
 
 
@@ -614,10 +613,16 @@ def main():
     lib = _ffi.gpu()
     solver = GpuSolver(local)
     t0 = time.time()
-    w = build_pile(solver, args.bodies, args.at, log)
-    if log:
-        log(f"pile built to step {args.at} in {time.time() - t0:.0f} s: {w.stats()}")
-    copy = StageCopy(w)
+    w = None
+    if args.load_input:
+        copy = StageCopy.load(args.load_input)
+    else:
+        w = build_pile(solver, args.bodies, args.at, log)
+        if log:
+            log(f"pile built to step {args.at} in {time.time() - t0:.0f} s: {w.stats()}")
+        copy = StageCopy(w)
+        if args.save_input:
+            copy.save(args.save_input)
     ctx = lib.bg_create(local, 0)
     assert ctx, "bg_create failed"
     h2d, d2h = io_bytes(copy)
@@ -664,11 +669,12 @@ def main():
     if not args.no_batch and not args.resident_only:   # every rank, or none: it holds collectives
         batch = measure_batch(args, lib, torch, local, log, rank, world_size, dist)
     narrow = None
-    if not args.resident_only and rank == 0:
+    if not args.resident_only and rank == 0 and w is not None:
         narrow = measure_narrowphase(lib, ctx, w, args.steps, args.warmup, host_threads(), log)
     adj = None
     if not args.no_adjoint and not args.resident_only and rank == 0 and world_size == 1:
         adj = measure_adjoint(args, local, log)
+    traffic, traffic_source = measured_traffic(args.bodies, args.at, algo)
     if rank == 0:
         line = {"metric": "contact rows/s", "value": value, "unit": "rows/s", "n_gpus": world_size,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -684,8 +690,8 @@ def main():
                                    "ms_per_step": ms_registered,
                                    "host_memory": "ordinary numpy arrays page-locked in place once by bg_register_host"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                             "frac": achieved / hbm, "traffic": measured_traffic(args.bodies, algo),
-                             "traffic_source": "ncu capture at step 101, scaled by algorithmic bytes", "kernel_ms": ms_stage,
+                             "frac": achieved / hbm, "traffic": traffic, "traffic_source": traffic_source,
+                             "kernel_ms": ms_stage,
                              "algorithmic_bytes": algo, "peak_source": peak_source},
                 "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches, "batch": batch, "adjoint": adj,
                 "narrowphase": narrow}

@@ -82,6 +82,24 @@ class StageCopy:
             starts=self.starts.copy(), rows={k: v.copy() for k, v in self.rows.items()}, dt=self.dt,
             substeps=self.substeps, gravity=self.gravity))
 
+    def save(self, path):
+        """Every array and count into one .npz file (StageCopy.load reads it back)."""
+        arrays = {"b_" + k: v for k, v in self.body.items()}
+        arrays.update({"r_" + k: v for k, v in self.rows.items()})
+        np.savez(path, awake_list=self.awake_list, starts=self.starts, gravity=np.asarray(self.gravity),
+                 counts=np.array([self.capacity, self.awake_count, self.count, self.solved, self.substeps]),
+                 dt=np.array([self.dt]), **arrays)
+
+    @staticmethod
+    def load(path):
+        z = np.load(path)
+        capacity, awake_count, count, solved, substeps = (int(x) for x in z["counts"])
+        return StageCopy(arrays=dict(
+            capacity=capacity, awake_count=awake_count, awake_list=z["awake_list"].copy(),
+            body={k[2:]: z[k].copy() for k in z.files if k.startswith("b_")}, count=count, solved=solved,
+            starts=z["starts"].copy(), rows={k[2:]: z[k].copy() for k in z.files if k.startswith("r_")},
+            dt=float(z["dt"][0]), substeps=substeps, gravity=tuple(float(x) for x in z["gravity"])))
+
     def pinned(self):
         """The same arrays in page-locked host memory (torch's pinned allocator), which the CUDA
         library copies to and from directly."""
