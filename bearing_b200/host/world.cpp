@@ -198,6 +198,13 @@ struct bw_world {
   Contacts c;
   bw_solver solver = nullptr;
   void* solverUser = nullptr;
+  // the narrowphase over the step's pair list on another device (bw_set_narrowphase), or none
+  bw_narrowphase narrowFn = nullptr;
+  void* narrowUser = nullptr;
+  std::vector<uint8_t> nmPoints;
+  std::vector<uint32_t> nmPid;
+  std::vector<double> nmNormal, nmPoint, nmSeparation;
+  std::vector<int32_t> nmPair;
   bool begun = false;
   bw_stats stats = {};
 
@@ -469,6 +476,66 @@ struct bw_world {
   // The pairs narrow() handed to collide() this step, with the margin and tolerance it passed.
   std::vector<int32_t> narrowA, narrowB;
   std::vector<double> narrowMargin, narrowTol;
+
+  // narrow() with the narrowphase itself on another device (bw_set_narrowphase): the same walk
+  // over the pairs (src/contact.js:312-327), in two passes.  The first drops the pairs whose fat
+  // boxes no longer meet (each removal moves the last pair into its place, as in one pass) and
+  // forgets those whose boxes miss, listing the rest with their margins; the device finds their
+  // manifolds; the second emits and carries the pairs that touch and forgets the others, in pair
+  // order.  No decision of the first pass depends on a manifold, so the rows, their order and the
+  // pairs' memory are the one-pass walk's.
+  int narrowOnDevice() {
+    narrowA.clear(); narrowB.clear(); narrowMargin.clear(); narrowTol.clear(); nmPair.clear();
+    for (int p = 0; p < pairs.active;) {
+      const int a = pairs.a[p], b = pairs.b[p];
+      if (!fatOverlap(a, b)) {
+        pairs.remove(p);
+        continue;
+      }
+      const double tol = jmin(size[a], size[b]) * PIXEL;
+      const int a6 = a * 6, b6 = b * 6;
+      if (box[a6] > box[b6 + 3] || box[b6] > box[a6 + 3] || box[a6 + 1] > box[b6 + 4]
+          || box[b6 + 1] > box[a6 + 4] || box[a6 + 2] > box[b6 + 5] || box[b6 + 2] > box[a6 + 5]) {
+        pairs.forget(p);
+      } else {
+        narrowA.push_back(a); narrowB.push_back(b); narrowMargin.push_back(motion[a] + motion[b] + tol);
+        narrowTol.push_back(tol); nmPair.push_back(p);
+      }
+      p++;
+    }
+    const size_t n = narrowA.size();
+    nmPoints.resize(std::max<size_t>(n, 1)); nmPid.resize(P * std::max<size_t>(n, 1));
+    nmNormal.resize(3 * std::max<size_t>(n, 1)); nmPoint.resize(3 * P * std::max<size_t>(n, 1));
+    nmSeparation.resize(P * std::max<size_t>(n, 1));
+    if (n > 0) {
+      bg_bodies B;
+      fillBodies(&B);
+      const bg_pairs list = {static_cast<int32_t>(n), narrowA.data(), narrowB.data(), narrowMargin.data(),
+                             narrowTol.data()};
+      bg_manifolds out = {nmPoints.data(), nmNormal.data(), nmPoint.data(), nmSeparation.data(), nmPid.data()};
+      const int32_t rc = narrowFn(narrowUser, &B, gravity, &list, &out);
+      if (rc != BG_OK) return rc;
+    }
+    Manifold mf;
+    for (size_t i = 0; i < n; i++) {
+      const int p = nmPair[i];
+      const int count = nmPoints[i];
+      if (count == 0) {
+        pairs.forget(p);
+        continue;
+      }
+      mf.count = count;
+      for (int k = 0; k < 3; k++) mf.normal[k] = nmNormal[3 * i + k];
+      for (int k = 0; k < count; k++) {
+        for (int q = 0; q < 3; q++) mf.points[3 * k + q] = nmPoint[3 * (P * i + k) + q];
+        mf.separations[k] = nmSeparation[P * i + k];
+        mf.ids[k] = nmPid[P * i + k];
+      }
+      const int m = emit(p, narrowA[i], narrowB[i], mf, narrowTol[i]);
+      carry(p, m);
+    }
+    return BG_OK;
+  }
 
   // narrow(): src/contact.js:296-327 with find() 334-368 (no reuse cache, no time of impact).
   void narrow() {
@@ -782,6 +849,13 @@ int32_t bw_add_body(bw_world* w, const bw_body* spec) {
   return s;
 }
 
+int32_t bw_set_narrowphase(bw_world* w, bw_narrowphase fn, void* user) {
+  if (w == nullptr) return BG_EINVAL;
+  w->narrowFn = fn;
+  w->narrowUser = user;
+  return BG_OK;
+}
+
 int32_t bw_set_solver(bw_world* w, bw_solver solver, void* user) {
   if (w == nullptr) return BG_EINVAL;
   w->solver = solver;
@@ -802,7 +876,15 @@ int32_t bw_begin_step(bw_world* w, double dt) {
   for (int i = 0; i < w->awakeCount; i++) w->boundsOf(w->awakeList[i], dt, gl);
   w->broadphase(dt);
   w->c.count = 0;
-  w->narrow();
+  if (w->narrowFn != nullptr) {
+    const int32_t rc = w->narrowOnDevice();
+    if (rc != BG_OK) {
+      w->error = "step: the narrowphase failed";
+      return rc;
+    }
+  } else {
+    w->narrow();
+  }
   if (w->c.count > 0) {
     w->colourRows();
     if (w->c.solved < w->c.count) w->rest();

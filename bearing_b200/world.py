@@ -46,6 +46,8 @@ class GpuSolver:
         self.fn = C.cast(self.lib.bg_solve_step, C.c_void_p).value
         # bw_solver takes (user, bodies, rows, step); bg_solve_step takes (ctx, bodies, rows, step).
         self.user = self.ctx
+        # bw_narrowphase takes (user, bodies, gravity, pairs, out), bg_collide (ctx, ...) alike.
+        self.collide_fn = C.cast(self.lib.bg_collide, C.c_void_p).value
 
     def error(self) -> str:
         return self.lib.bg_last_error(self.ctx).decode()
@@ -84,9 +86,22 @@ class World:
         self._count = 0
         self._solver = None
         self._solver_keep = None
+        self._narrowphase = None
         if solver is None:
             solver = GpuSolver()
         self.set_solver(solver)
+
+    # -- the narrowphase ---------------------------------------------------------------------
+    def set_narrowphase(self, device):
+        """device: a GpuSolver, whose context then runs each step's narrowphase (bg_collide), or
+        None for the host's own.  The step's rows are the same either way."""
+        if device is None:
+            fn, user = None, None
+        else:
+            fn, user = device.collide_fn, device.ctx
+        if self._lib.bw_set_narrowphase(self._w, fn, user) != 0:
+            raise BearingError("set_narrowphase failed")
+        self._narrowphase = device
 
     # -- the solve stage ---------------------------------------------------------------------
     def set_solver(self, solver):

@@ -481,6 +481,7 @@ def measure_narrowphase(lib, ctx, world, steps, warmup, threads, log):
     (bw_collide_pairs), and the two results compared bit for bit."""
     import numpy as np
     import narrow_io
+    from bearing_b200 import _ffi
     pairs = narrow_io.world_pairs(world)
     B, _, S = world.views()
     g = np.asarray(S.gravity, np.float64)
@@ -501,6 +502,26 @@ def measure_narrowphase(lib, ctx, world, steps, warmup, threads, log):
         host = narrow_io.host_collide(B, tuple(S.gravity), pairs, threads=threads)
         cpu.append((time.perf_counter() - t0) * 1000)
     same = narrow_io.first_unequal(host, out) is None
+    # The host side of one step (bounds, broadphase, narrowphase, emit, carry, colour), on copies of
+    # the world: with the host's own narrowphase (one thread, as the step runs it), and with the
+    # narrowphase handed to bg_collide (bw_set_narrowphase).
+    h = _ffi.host()
+
+    def host_side(fn, user):
+        best = None
+        for _ in range(3):
+            clone = h.bw_clone(world._w)
+            assert clone and h.bw_set_narrowphase(clone, fn, user) == 0
+            t0 = time.perf_counter()
+            rc = h.bw_begin_step(clone, DT)
+            dt_ms = (time.perf_counter() - t0) * 1000
+            h.bw_destroy(clone)
+            assert rc == 0
+            best = dt_ms if best is None else min(best, dt_ms)
+        return best
+
+    step_host = host_side(None, None)
+    step_device = host_side(C.cast(lib.bg_collide, C.c_void_p).value, ctx)
     n = pairs.count
     counts = np.bincount(out.points[:n], minlength=5)
     in_bytes = n * (2 * 4 + 2 * 8) + B.capacity * (11 * 8 + 2)
@@ -508,7 +529,8 @@ def measure_narrowphase(lib, ctx, world, steps, warmup, threads, log):
     k_ms, e_ms, c_ms = statistics.mean(kernel), statistics.mean(e2e), min(cpu)
     if log:
         log(f"narrowphase: {n} pairs, kernel {k_ms:.3f} ms, end to end {e_ms:.3f} ms, host {c_ms:.1f} ms "
-            f"({threads} threads), bit-identical {same}")
+            f"({threads} threads), bit-identical {same}; host side of a step {step_host:.1f} ms, "
+            f"{step_device:.1f} ms with bg_collide")
     return {"workload": f"the pile's step-{world.stats()['step'] + 1} narrowphase: the pairs whose boxes meet",
             "pairs": n, "manifolds_by_points": [int(x) for x in counts], "unit": "pairs/s",
             "value": n / (k_ms / 1000), "kernel_ms": k_ms,
@@ -517,7 +539,10 @@ def measure_narrowphase(lib, ctx, world, steps, warmup, threads, log):
             "cpu_baseline": {"value": n / (c_ms / 1000), "unit": "pairs/s", "cores": threads, "kind": "port",
                              "ms": c_ms, "sample": "the same pair list through the host's narrowphase "
                                                    "(bw_collide_pairs), every host thread"},
-            "bit_identical": same}
+            "bit_identical": same,
+            "host_step_ms": {"host_narrowphase": step_host, "device_narrowphase": step_device,
+                             "what": "the host side of one step of the pile (bounds, broadphase, narrowphase, emit, "
+                                     "carry, colour), best of 3 on copies of the world"}}
 
 
 def batch_roofline(algo, ms, cta_threads):

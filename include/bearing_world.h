@@ -78,6 +78,14 @@ int32_t bw_add_body(bw_world* world, const bw_body* body);
 /* The solve stage to call; NULL restores none (bw_step then fails with BG_EUNSUPPORTED). */
 int32_t bw_set_solver(bw_world* world, bw_solver solver, void* user);
 
+/* The narrowphase on another device: fn (bg_collide's signature, with `user` for its context) is
+ * handed each step's pairs whose boxes meet and returns their manifolds, which the step then
+ * emits and carries as it would its own (src/contact.js:312-327).  NULL (the default) runs the
+ * host's own.  The rows, their order and the pairs' memory are the same either way. */
+typedef int32_t (*bw_narrowphase)(void* user, const bg_bodies* bodies, const double* gravity, const bg_pairs* pairs,
+                                  bg_manifolds* out);
+int32_t bw_set_narrowphase(bw_world* world, bw_narrowphase fn, void* user);
+
 /* A whole World.step(dt): bw_begin_step, the solver, bw_end_step. */
 int32_t bw_step(bw_world* world, double dt);
 

@@ -103,3 +103,26 @@ def test_refusals_write_nothing():
                         C.byref(out.s))
     assert rc == 0
     w.destroy()
+
+
+@pytest.mark.parametrize("build,steps", [(pile3000, 60), (rain, 80)], ids=["pile3000", "rain300"])
+def test_a_world_stepping_with_the_device_narrowphase_is_the_same_world(build, steps):
+    # bw_set_narrowphase: each step's pairs go to bg_collide, and the step emits and carries its
+    # manifolds; the state after every step equals the host narrowphase's, bit for bit.
+    a = World({}, solver=oracle_io.solver(0))
+    b = World({}, solver=oracle_io.solver(0))
+    build(a)
+    build(b)
+    device = GpuSolver()
+    b.set_narrowphase(device)
+    for i in range(steps):
+        a.step(DT)
+        b.step(DT)
+        sa, sb = a.state(), b.state()
+        for k in ("position", "rotation", "velocity", "angular"):
+            assert sa[k].tobytes() == sb[k].tobytes(), f"step {i + 1}: {k}"
+    assert a.stats()["rows"] == b.stats()["rows"] > 0
+    b.set_narrowphase(None)
+    a.destroy()
+    b.destroy()
+    device.close()

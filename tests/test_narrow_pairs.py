@@ -73,3 +73,48 @@ def test_bad_slots_are_refused():
                                       C.byref(out.s), 1)
     assert rc == _ffi.BG_EINVAL
     w.destroy()
+
+
+NARROWPHASE = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(_ffi.Bodies), C.POINTER(C.c_double),
+                          C.POINTER(_ffi.Pairs), C.POINTER(_ffi.Manifolds))
+
+
+@pytest.mark.parametrize("build,steps", [(boxes_and_balls, 60), (raining, 100)], ids=["pile600", "rain150"])
+def test_a_world_with_its_narrowphase_handed_out_is_the_same_world(build, steps):
+    # bw_set_narrowphase with the host's own narrowphase behind it (what bg_collide computes on
+    # the device, bit for bit): the two-pass walk over the pairs gives the same world, step by step.
+    host = _ffi.host()
+    calls = []
+
+    def collide(user, bodies, gravity, pairs, out):
+        calls.append(pairs.contents.count)
+        return host.bw_collide_pairs(bodies, gravity, pairs, out, 2)
+
+    hook = NARROWPHASE(collide)
+    a = World({}, solver=oracle_io.solver(0))
+    b = World({}, solver=oracle_io.solver(0))
+    build(a)
+    build(b)
+    assert host.bw_set_narrowphase(b._w, C.cast(hook, C.c_void_p), None) == 0
+    for i in range(steps):
+        a.step(DT)
+        b.step(DT)
+        sa, sb = a.state(), b.state()
+        for k in ("position", "rotation", "velocity", "angular"):
+            assert sa[k].tobytes() == sb[k].tobytes(), f"step {i + 1}: {k}"
+    assert len(calls) > 0 and max(calls) > 0
+    assert a.stats()["rows"] == b.stats()["rows"]
+    assert host.bw_set_narrowphase(b._w, None, None) == 0
+    a.destroy()
+    b.destroy()
+
+
+def test_a_failing_narrowphase_fails_the_step():
+    host = _ffi.host()
+    hook = NARROWPHASE(lambda *args: _ffi.BG_ECUDA)
+    w = World({}, solver=oracle_io.solver(0))
+    scenes.pyramid(w, rows=3)
+    assert host.bw_set_narrowphase(w._w, C.cast(hook, C.c_void_p), None) == 0
+    assert host.bw_begin_step(w._w, DT) == _ffi.BG_ECUDA
+    assert host.bw_set_narrowphase(w._w, None, None) == 0
+    w.destroy()
