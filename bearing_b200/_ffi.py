@@ -257,12 +257,13 @@ def host() -> C.CDLL:
         lib.bw_copy.argtypes = [C.c_void_p, C.c_void_p]
         lib.bw_narrow_pairs.argtypes = [C.c_void_p, C.POINTER(Pairs)]
         lib.bw_set_narrowphase.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.bw_colour_rows.argtypes = [C.POINTER(Bodies), C.c_int32, _i32, _i32, _i32, _i32, _i32, _i32]
         lib.bw_collide_pairs.argtypes = [C.POINTER(Bodies), _d, C.POINTER(Pairs), C.POINTER(Manifolds), C.c_int32]
         for f in ("bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step", "bw_end_step",
                   "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_stats_get", "bw_batch_begin_step",
                   "bw_batch_views", "bw_batch_end_step", "bw_row_memory_get", "bw_batch_row_memory", "bw_copy",
                   "bw_keep_backward", "bw_narrow_backward", "bw_materials", "bw_narrow_pairs", "bw_collide_pairs",
-                  "bw_set_narrowphase"):
+                  "bw_set_narrowphase", "bw_colour_rows"):
             getattr(lib, f).restype = C.c_int32
         _host = lib
     return _host
@@ -305,6 +306,10 @@ def gpu() -> C.CDLL:
         lib.bg_backward_bytes.restype = C.c_int64
         lib.bg_collide.argtypes = [C.c_void_p, C.POINTER(Bodies), _d, C.POINTER(Pairs), C.POINTER(Manifolds)]
         lib.bg_collide.restype = C.c_int32
+        lib.bg_colour.argtypes = [C.c_void_p, C.POINTER(Bodies), C.c_int32, _i32, _i32, _i32, _i32, _i32, _i32]
+        lib.bg_colour.restype = C.c_int32
+        lib.bg_last_colour_ms.argtypes = [C.c_void_p]
+        lib.bg_last_colour_ms.restype = C.c_double
         lib.bg_last_collide_ms.argtypes = [C.c_void_p]
         lib.bg_last_collide_ms.restype = C.c_double
         lib.bg_last_launches.argtypes = [C.c_void_p]
@@ -341,12 +346,12 @@ GPU_SYMBOLS = [
     "bg_batch_download", "bg_stream", "bg_last_launches", "bg_last_stage_ms", "bg_set_wait_budget", "bg_set_block_threads",
     "bg_block_threads", "bg_set_batch_groups", "bg_backward", "bg_backward_tape_peak", "bg_backward_ms",
     "bg_solve_step_static", "bg_register_host", "bg_unregister_host", "bg_registered_bytes", "bg_collide",
-    "bg_last_collide_ms", "bg_backward_bytes",
+    "bg_last_collide_ms", "bg_backward_bytes", "bg_colour", "bg_last_colour_ms",
 ]
 HOST_SYMBOLS = [
     "bw_create", "bw_destroy", "bw_last_error", "bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step",
     "bw_end_step", "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_transforms", "bw_stats_get",
     "bw_batch_create", "bw_batch_destroy", "bw_batch_begin_step", "bw_batch_views", "bw_batch_end_step",
     "bw_row_memory_get", "bw_batch_row_memory", "bw_clone", "bw_copy", "bw_keep_backward", "bw_narrow_backward",
-    "bw_materials", "bw_narrow_pairs", "bw_collide_pairs", "bw_set_narrowphase",
+    "bw_materials", "bw_narrow_pairs", "bw_collide_pairs", "bw_set_narrowphase", "bw_colour_rows",
 ]

@@ -33,6 +33,7 @@
 #include "stage.cuh"
 #include "adjoint.cuh"
 #include "../host/collide_impl.hpp"
+#include "colour.cuh"
 
 namespace {
 
@@ -514,6 +515,13 @@ struct bg_ctx {
     cudaEvent_t begin = nullptr, end = nullptr;
     bool timed = false;
   } nw;
+  // bg_colour's device block and its events
+  struct Colouring {
+    unsigned char* block = nullptr;
+    size_t bodies = 0, rows = 0;
+    cudaEvent_t begin = nullptr, end = nullptr;
+    bool timed = false;
+  } col;
   // bg_backward's own device memory (grown by doubling, freed with the context)
   struct Adjoint {
     std::vector<void*> allocs;
@@ -1319,6 +1327,9 @@ void bg_destroy(bg_ctx* c) {
   for (void* p : c->adj.allocs) cudaFree(p);
   c->adj.allocs.clear();
   if (c->nw.block) cudaFree(c->nw.block);
+  if (c->col.block) cudaFree(c->col.block);
+  if (c->col.begin) cudaEventDestroy(c->col.begin);
+  if (c->col.end) cudaEventDestroy(c->col.end);
   if (c->nw.begin) cudaEventDestroy(c->nw.begin);
   if (c->nw.end) cudaEventDestroy(c->nw.end);
   if (c->adj.begin) cudaEventDestroy(c->adj.begin);
@@ -2789,6 +2800,153 @@ double bg_last_collide_ms(bg_ctx* c) {
   if (c == nullptr || !c->nw.timed) return -1;
   float ms = 0;
   if (cudaEventSynchronize(c->nw.end) != cudaSuccess || cudaEventElapsedTime(&ms, c->nw.begin, c->nw.end) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return ms;
+}
+
+}  // extern "C"
+
+// ---- the colouring on the device (bg_colour) -----------------------------------------------
+
+namespace {
+
+struct ColourLayout {
+  int32_t *a, *b, *deg, *off, *cursor, *list, *rank, *colour, *bins, *bincur, *order, *starts, *status;
+  uint8_t *type, *frozen;
+  uint32_t* used;
+  unsigned int* done;
+  size_t bytes;
+};
+
+ColourLayout colour_layout(unsigned char* base, size_t nb, size_t n) {
+  Carve k{base};
+  ColourLayout L;
+  L.a = k.take<int32_t>(n); L.b = k.take<int32_t>(n);
+  L.type = k.take<uint8_t>(nb); L.frozen = k.take<uint8_t>(nb);
+  // zeroed together before each call: deg, cursor, used, done, bins, bincur, status
+  L.deg = k.take<int32_t>(nb); L.cursor = k.take<int32_t>(nb); L.used = k.take<uint32_t>(nb);
+  L.done = k.take<unsigned int>(nb); L.bins = k.take<int32_t>(bgcol::kRuns * nb + 1);
+  L.bincur = k.take<int32_t>(bgcol::kRuns * nb); L.status = k.take<int32_t>(1);
+  L.off = k.take<int32_t>(nb + 1); L.list = k.take<int32_t>(2 * n); L.rank = k.take<int32_t>(2 * n);
+  L.colour = k.take<int32_t>(n); L.order = k.take<int32_t>(n); L.starts = k.take<int32_t>(bgcol::kStarts);
+  L.bytes = k.end;
+  return L;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t bg_colour(bg_ctx* c, const bg_bodies* B, int32_t count, const int32_t* a, const int32_t* b, int32_t* colour,
+                  int32_t* order, int32_t* starts, int32_t* solved) {
+  if (c == nullptr) return BG_EINVAL;
+  if (B == nullptr || starts == nullptr || solved == nullptr || count < 0 || B->capacity < 0) {
+    set_error(c, "bg_colour: bodies, starts or solved is NULL, or a count is negative");
+    return BG_EINVAL;
+  }
+  const int64_t n = count, nb = B->capacity;
+  if (n > 0 && (a == nullptr || b == nullptr || colour == nullptr || order == nullptr || B->type == nullptr ||
+                B->frozen == nullptr)) {
+    set_error(c, "bg_colour: a column is NULL");
+    return BG_EINVAL;
+  }
+  if (static_cast<int64_t>(bgcol::kRuns) * nb + 1 > INT32_MAX || 2 * n > INT32_MAX) {
+    set_error(c, "bg_colour: too many slots or manifolds");
+    return BG_EINVAL;
+  }
+  for (int64_t f = 0; f < n; f++)
+    if (a[f] < 0 || a[f] >= nb || b[f] < 0 || b[f] >= nb || a[f] == b[f]) {
+      set_error(c, "bg_colour: manifold %lld has slots %d, %d of %lld", static_cast<long long>(f), a[f], b[f],
+                static_cast<long long>(nb));
+      return BG_EINVAL;
+    }
+  std::fill(starts, starts + BG_STARTS, 0);
+  *solved = 0;
+  if (n == 0) return BG_OK;
+  int32_t any_frozen = 0;
+  for (int64_t x = 0; x < nb && !any_frozen; x++) any_frozen = B->frozen[x] != 0;
+  cudaSetDevice(c->device);
+  bg_ctx::Colouring& d = c->col;
+  if (d.block == nullptr || static_cast<size_t>(nb) > d.bodies || static_cast<size_t>(n) > d.rows) {
+    cudaStreamSynchronize(c->stream);
+    if (d.block) cudaFree(d.block);
+    d.block = nullptr;
+    d.bodies = grown(d.bodies, static_cast<size_t>(nb));
+    d.rows = grown(d.rows, static_cast<size_t>(n));
+    void* block = nullptr;
+    if (cudaMalloc(&block, colour_layout(nullptr, d.bodies, d.rows).bytes) != cudaSuccess) {
+      cudaGetLastError();
+      d.bodies = d.rows = 0;
+      set_error(c, "bg_colour: cudaMalloc failed");
+      return BG_ENOMEM;
+    }
+    d.block = static_cast<unsigned char*>(block);
+  }
+  if (d.begin == nullptr) {
+    cudaEventCreate(&d.begin);
+    cudaEventCreate(&d.end);
+  }
+  // laid out for this call's sizes (the block holds at least that much)
+  const ColourLayout L = colour_layout(d.block, static_cast<size_t>(nb), static_cast<size_t>(n));
+  cudaStream_t st = c->stream;
+  bool ok = cuda_ok(c, cudaMemcpyAsync(L.a, a, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st), "bg_colour") &&
+            cuda_ok(c, cudaMemcpyAsync(L.b, b, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st), "bg_colour") &&
+            cuda_ok(c, cudaMemcpyAsync(L.type, B->type, static_cast<size_t>(nb), cudaMemcpyHostToDevice, st), "bg_colour") &&
+            cuda_ok(c, cudaMemcpyAsync(L.frozen, B->frozen, static_cast<size_t>(nb), cudaMemcpyHostToDevice, st), "bg_colour");
+  const size_t zero = reinterpret_cast<unsigned char*>(L.off) - reinterpret_cast<unsigned char*>(L.deg);
+  ok = ok && cuda_ok(c, cudaMemsetAsync(L.deg, 0, zero, st), "bg_colour");
+  if (!ok) return BG_ECUDA;
+  bgcol::ColourParams p;
+  p.n = static_cast<int32_t>(n); p.nb = static_cast<int32_t>(nb); p.a = L.a; p.b = L.b; p.type = L.type;
+  p.frozen = L.frozen; p.any_frozen = any_frozen; p.deg = L.deg; p.off = L.off; p.cursor = L.cursor; p.list = L.list;
+  p.rank = L.rank; p.used = L.used; p.done = L.done; p.colour = L.colour; p.bins = L.bins; p.bincur = L.bincur;
+  p.order = L.order; p.starts = L.starts; p.status = L.status; p.budget = c->budget;
+  const int rows_grid = std::max(1, std::min(static_cast<int>((n + 255) / 256), 8 * c->sms));
+  const int body_grid = std::max(1, std::min(static_cast<int>((nb + 255) / 256), 8 * c->sms));
+  const int bin_grid = std::max(1, std::min(static_cast<int>((bgcol::kRuns * nb + 255) / 256), 8 * c->sms));
+  cudaEventRecord(d.begin, st);
+  bgcol::col_degrees<<<rows_grid, 256, 0, st>>>(p);
+  bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(L.deg, L.off, static_cast<int>(nb));
+  bgcol::col_fill<<<rows_grid, 256, 0, st>>>(p);
+  bgcol::col_ranks<<<body_grid, 256, 0, st>>>(p);
+  {
+    void* args[] = {&p};
+    if (!cuda_ok(c, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(bgcol::col_colour), dim3(c->sms), dim3(256),
+                                                args, 0, st), "col_colour launch"))
+      return BG_ECUDA;
+  }
+  bgcol::col_bins<<<rows_grid, 256, 0, st>>>(p);
+  bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(L.bins, L.bins, bgcol::kRuns * static_cast<int>(nb));
+  bgcol::col_scatter<<<rows_grid, 256, 0, st>>>(p);
+  bgcol::col_settle<<<bin_grid, 256, 0, st>>>(p);
+  bgcol::col_starts<<<1, 64, 0, st>>>(p);
+  cudaEventRecord(d.end, st);
+  d.timed = true;
+  c->last_launches += 10;
+  if (!cuda_ok(c, cudaGetLastError(), "bg_colour launch")) return BG_ECUDA;
+  int32_t status = 0;
+  ok = cuda_ok(c, cudaMemcpyAsync(&status, L.status, sizeof status, cudaMemcpyDeviceToHost, st), "bg_colour") &&
+       cuda_ok(c, cudaStreamSynchronize(st), "bg_colour");
+  if (!ok) return BG_ECUDA;
+  if (status != 0) {
+    set_error(c, "bg_colour: a wait ran past its budget");
+    return BG_ETIMEOUT;
+  }
+  ok = cuda_ok(c, cudaMemcpyAsync(colour, L.colour, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st), "bg_colour") &&
+       cuda_ok(c, cudaMemcpyAsync(order, L.order, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st), "bg_colour") &&
+       cuda_ok(c, cudaMemcpyAsync(starts, L.starts, sizeof(int32_t) * BG_STARTS, cudaMemcpyDeviceToHost, st), "bg_colour") &&
+       cuda_ok(c, cudaStreamSynchronize(st), "bg_colour");
+  if (!ok) return BG_ECUDA;
+  *solved = starts[BG_RESTING];
+  return BG_OK;
+}
+
+double bg_last_colour_ms(bg_ctx* c) {
+  if (c == nullptr || !c->col.timed) return -1;
+  float ms = 0;
+  if (cudaEventSynchronize(c->col.end) != cudaSuccess || cudaEventElapsedTime(&ms, c->col.begin, c->col.end) != cudaSuccess) {
     cudaGetLastError();
     return -1;
   }

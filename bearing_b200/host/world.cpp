@@ -171,6 +171,65 @@ struct Pairs {
 
 }  // namespace
 
+// colour(): src/graph.js:105-170 over cnt manifolds in found order (A[m], Bs[m]): each manifold's
+// colour, then the row order (order: row o holds manifold order[o]; `scratch` cnt entries,
+// `count` DIGITS + 1) and the colour starts, as the reference lays them out.
+static void colour_manifolds(int cnt, const int32_t* A, const int32_t* Bs, const uint8_t* type, const uint8_t* frozen,
+                             int nslots, int32_t* colour, int32_t* order, int32_t* scratch, int32_t* count,
+                             int32_t* starts) {
+  std::vector<int32_t> used(static_cast<size_t>(nslots), 0);
+  const bool anyFrozen = std::any_of(frozen, frozen + nslots, [](uint8_t f) { return f != 0; });
+  for (int m = 0; m < cnt; m++) {
+    const int a = A[m], b = Bs[m];
+    bool da = type[a] == BG_DYNAMIC, db = type[b] == BG_DYNAMIC;
+    if (anyFrozen) {
+      const bool fa = frozen[a] != 0, fb = frozen[b] != 0;
+      if ((fa || type[a] == BG_STATIC) && (fb || type[b] == BG_STATIC)) {
+        colour[m] = RESTING;
+        continue;
+      }
+      if (fa) da = false;
+      if (fb) db = false;
+    }
+    const int32_t held = (da ? used[a] : 0) | (db ? used[b] : 0);
+    if (held == -1) {
+      colour[m] = OVERFLOW_;
+      continue;
+    }
+    const uint32_t uheld = static_cast<uint32_t>(held);
+    const uint32_t bit = ~uheld & (uheld + 1u);
+    colour[m] = 31 - __builtin_clz(bit);
+    if (da) used[a] |= static_cast<int32_t>(bit);
+    if (db) used[b] |= static_cast<int32_t>(bit);
+  }
+  // stable counting sorts by b's low digit, its high one (past DIGITS slots), then colour
+  std::fill(count, count + DIGITS + 1, 0);
+  const bool high = nslots > DIGITS;
+  int32_t* from = high ? order : scratch;
+  for (int m = 0; m < cnt; m++) count[(Bs[m] & (DIGITS - 1)) + 1]++;
+  for (int k = 0; k < DIGITS; k++) count[k + 1] += count[k];
+  for (int m = 0; m < cnt; m++) from[count[Bs[m] & (DIGITS - 1)]++] = m;
+  if (high) {
+    std::fill(count, count + DIGITS + 1, 0);
+    for (int i = 0; i < cnt; i++) count[(static_cast<uint32_t>(Bs[order[i]]) >> DIGIT) + 1]++;
+    for (int k = 0; k < DIGITS; k++) count[k + 1] += count[k];
+    for (int i = 0; i < cnt; i++) {
+      const int m = order[i];
+      scratch[count[static_cast<uint32_t>(Bs[m]) >> DIGIT]++] = m;
+    }
+    from = scratch;
+  }
+  std::fill(starts, starts + COLOURS + 3, 0);
+  for (int m = 0; m < cnt; m++) starts[colour[m] + 1]++;
+  for (int k = 0; k <= RESTING; k++) starts[k + 1] += starts[k];
+  for (int i = 0; i < cnt; i++) {
+    const int m = from[i];
+    order[starts[colour[m]]++] = m;
+  }
+  for (int k = RESTING; k > 0; k--) starts[k] = starts[k - 1];
+  starts[0] = 0;
+}
+
 struct bw_world {
   std::string error;
   double gravity[3] = {0, -9.81, 0};
@@ -576,59 +635,10 @@ struct bw_world {
   // colour(): src/graph.js:105-170, and arrange() 178-214.
   void colourRows() {
     const int cnt = c.count;
-    std::vector<int32_t> used(static_cast<size_t>(n), 0);
-    const bool anyFrozen = std::any_of(frozen.begin(), frozen.begin() + n, [](uint8_t f) { return f != 0; });
-    for (int m = 0; m < cnt; m++) {
-      const int a = c.a[m], b = c.b[m];
-      bool da = type[a] == BG_DYNAMIC, db = type[b] == BG_DYNAMIC;
-      if (anyFrozen) {
-        const bool fa = frozen[a] != 0, fb = frozen[b] != 0;
-        if ((fa || type[a] == BG_STATIC) && (fb || type[b] == BG_STATIC)) {
-          c.colour[m] = RESTING;
-          continue;
-        }
-        if (fa) da = false;
-        if (fb) db = false;
-      }
-      const int32_t held = (da ? used[a] : 0) | (db ? used[b] : 0);
-      if (held == -1) {
-        c.colour[m] = OVERFLOW_;
-        continue;
-      }
-      const uint32_t uheld = static_cast<uint32_t>(held);
-      const uint32_t bit = ~uheld & (uheld + 1u);
-      c.colour[m] = 31 - __builtin_clz(bit);
-      if (da) used[a] |= static_cast<int32_t>(bit);
-      if (db) used[b] |= static_cast<int32_t>(bit);
-    }
     c.digits.assign(DIGITS + 1, 0);
-    std::vector<int32_t>& count = c.digits;
-    const bool high = n > DIGITS;
-    int32_t* from = high ? c.order.data() : c.row.data();
-    for (int m = 0; m < cnt; m++) count[(c.b[m] & (DIGITS - 1)) + 1]++;
-    for (int k = 0; k < DIGITS; k++) count[k + 1] += count[k];
-    for (int m = 0; m < cnt; m++) from[count[c.b[m] & (DIGITS - 1)]++] = m;
-    if (high) {
-      std::fill(count.begin(), count.end(), 0);
-      for (int i = 0; i < cnt; i++) count[(static_cast<uint32_t>(c.b[c.order[i]]) >> DIGIT) + 1]++;
-      for (int k = 0; k < DIGITS; k++) count[k + 1] += count[k];
-      for (int i = 0; i < cnt; i++) {
-        const int m = c.order[i];
-        c.row[count[static_cast<uint32_t>(c.b[m]) >> DIGIT]++] = m;
-      }
-      from = c.row.data();
-    }
-    int* starts = c.starts;
-    std::fill(starts, starts + COLOURS + 3, 0);
-    for (int m = 0; m < cnt; m++) starts[c.colour[m] + 1]++;
-    for (int k = 0; k <= RESTING; k++) starts[k + 1] += starts[k];
-    for (int i = 0; i < cnt; i++) {
-      const int m = from[i];
-      c.order[starts[c.colour[m]]++] = m;
-    }
-    for (int k = RESTING; k > 0; k--) starts[k] = starts[k - 1];
-    starts[0] = 0;
-    c.solved = starts[RESTING];
+    colour_manifolds(cnt, c.a.data(), c.b.data(), type.data(), frozen.data(), n, c.colour.data(), c.order.data(),
+                     c.row.data(), c.digits.data(), c.starts);
+    c.solved = c.starts[RESTING];
     arrange(cnt);
   }
   template <class T>
@@ -977,6 +987,20 @@ int32_t bw_copy(bw_world* dst, const bw_world* src) {
   } catch (const std::exception&) {
     return BG_ENOMEM;
   }
+  return BG_OK;
+}
+
+int32_t bw_colour_rows(const bg_bodies* B, int32_t count, const int32_t* a, const int32_t* b, int32_t* colour,
+                       int32_t* order, int32_t* starts, int32_t* solved) {
+  if (B == nullptr || starts == nullptr || solved == nullptr || count < 0 || B->capacity < 0) return BG_EINVAL;
+  if (count > 0 && (a == nullptr || b == nullptr || colour == nullptr || order == nullptr || B->type == nullptr ||
+                    B->frozen == nullptr))
+    return BG_EINVAL;
+  for (int m = 0; m < count; m++)
+    if (a[m] < 0 || a[m] >= B->capacity || b[m] < 0 || b[m] >= B->capacity || a[m] == b[m]) return BG_EINVAL;
+  std::vector<int32_t> scratch(static_cast<size_t>(std::max(count, 1))), digits(DIGITS + 1);
+  colour_manifolds(count, a, b, B->type, B->frozen, B->capacity, colour, order, scratch.data(), digits.data(), starts);
+  *solved = starts[RESTING];
   return BG_OK;
 }
 

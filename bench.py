@@ -68,8 +68,10 @@ def parse():
 def build_pile(solver, bodies, at, log=None):
     """The pile stepped `at` times with `solver`, then the host side of step at+1."""
     from bearing_b200 import scenes
-    from bearing_b200.world import World
+    from bearing_b200.world import GpuSolver, World
     w = World({}, solver=solver)
+    if isinstance(solver, GpuSolver):
+        w.set_narrowphase(solver)   # the same rows as the host's narrowphase, found on the device
     scenes.pile(w, count=bodies, seed=50_000)
     t0 = time.time()
     for i in range(at):
@@ -545,6 +547,61 @@ def measure_narrowphase(lib, ctx, world, steps, warmup, threads, log):
                                      "carry, colour), best of 3 on copies of the world"}}
 
 
+def measure_colouring(lib, ctx, copy, steps, warmup, log):
+    """The colouring of the same step on the device: bg_colour over the step's manifolds in found
+    order (recovered from the rows' found-order map), its kernels' device time and the call end to
+    end, against the host's colouring of the same list (bw_colour_rows, one thread, as the step runs
+    it), and both against the step's own row order."""
+    import numpy as np
+    from bearing_b200 import _ffi
+    n = copy.count
+    row = copy.rows["row"][:n]
+    a = np.ascontiguousarray(copy.rows["a"][row], np.int32)
+    b = np.ascontiguousarray(copy.rows["b"][row], np.int32)
+    B = _ffi.Bodies()
+    B.capacity = copy.capacity
+    B.type = copy.body["type"].ctypes.data_as(C.POINTER(C.c_uint8))
+    B.frozen = copy.body["frozen"].ctypes.data_as(C.POINTER(C.c_uint8))
+    pi = C.POINTER(C.c_int32)
+
+    def arrays():
+        return (np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(_ffi.BG_STARTS, np.int32), C.c_int32())
+
+    def call(fn, *lead):
+        colour, order, starts, solved = arrays()
+        t0 = time.perf_counter()
+        rc = fn(*lead, C.byref(B), n, a.ctypes.data_as(pi), b.ctypes.data_as(pi), colour.ctypes.data_as(pi),
+                order.ctypes.data_as(pi), starts.ctypes.data_as(pi), C.byref(solved))
+        ms = (time.perf_counter() - t0) * 1000
+        assert rc == 0
+        return ms, order, starts
+
+    kernel, e2e = [], []
+    for i in range(warmup + steps):
+        ms, order, starts = call(lib.bg_colour, ctx)
+        if i >= warmup:
+            e2e.append(ms)
+            kernel.append(lib.bg_last_colour_ms(ctx))
+    host = _ffi.host()
+    cpu = [call(host.bw_colour_rows)[0] for _ in range(3)]
+    _, horder, hstarts = call(host.bw_colour_rows)
+    found = np.empty(n, np.int32)
+    found[row] = np.arange(n, dtype=np.int32)
+    same = bool(np.array_equal(order, found) and np.array_equal(horder, found) and
+                np.array_equal(starts, copy.starts) and np.array_equal(hstarts, copy.starts))
+    k_ms, e_ms, c_ms = statistics.mean(kernel), statistics.mean(e2e), min(cpu)
+    if log:
+        log(f"colouring: {n} manifolds, kernels {k_ms:.3f} ms, end to end {e_ms:.3f} ms, host {c_ms:.2f} ms, "
+            f"the step's own order {same}")
+    return {"workload": "the pile's step-301 manifolds in found order: colours, row order and colour starts",
+            "manifolds": n, "unit": "manifolds/s", "value": n / (k_ms / 1000), "kernel_ms": k_ms,
+            "e2e": {"value": n / (e_ms / 1000), "ms_per_step": e_ms, "h2d_bytes_per_step": 8 * n + 2 * copy.capacity,
+                    "d2h_bytes_per_step": 8 * n + 4 * 35},
+            "cpu_baseline": {"value": n / (c_ms / 1000), "unit": "manifolds/s", "cores": 1, "kind": "port", "ms": c_ms,
+                             "sample": "the same list through the host's colouring (bw_colour_rows)"},
+            "same_as_the_step": same}
+
+
 def batch_roofline(algo, ms, cta_threads):
     """The batched kernel's roofline line: this rank's algorithmic bytes over the resident solve's
     time (the max over ranks), against the measured HBM copy rate; DRAM traffic scaled from the
@@ -696,6 +753,9 @@ def main():
     narrow = None
     if not args.resident_only and rank == 0 and w is not None:
         narrow = measure_narrowphase(lib, ctx, w, args.steps, args.warmup, host_threads(), log)
+    colouring = None
+    if not args.resident_only and rank == 0:
+        colouring = measure_colouring(lib, ctx, copy, args.steps, args.warmup, log)
     adj = None
     if not args.no_adjoint and not args.resident_only and rank == 0 and world_size == 1:
         adj = measure_adjoint(args, local, log)
@@ -719,7 +779,7 @@ def main():
                              "kernel_ms": ms_stage,
                              "algorithmic_bytes": algo, "peak_source": peak_source},
                 "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches, "batch": batch, "adjoint": adj,
-                "narrowphase": narrow}
+                "narrowphase": narrow, "colouring": colouring}
         print(json.dumps(line), flush=True)
     lib.bg_destroy(ctx)
     solver.close()

@@ -387,6 +387,21 @@ int32_t bg_collide(bg_ctx* ctx, const bg_bodies* bodies, const double* gravity, 
 /* Device time in milliseconds of the last bg_collide's kernel (synchronises; negative if none). */
 double bg_last_collide_ms(bg_ctx* ctx);
 
+/*
+ * The constraint-graph colouring on the device (src/graph.js:105-214), exactly: colour() gives each
+ * manifold the lowest colour none of the manifolds found before it on its moving bodies holds
+ * (OVERFLOW when all 32 are held, RESTING between frozen or static bodies), and arrange()'s row
+ * order puts them colour by colour, each colour's by b's slot, ties in found order.
+ * In: bodies' capacity, type and frozen (the rest may be NULL); the step's `count` manifolds in the
+ * order narrow() found them, a[f] and b[f] (slots).  Out: colour[f]; order[o], the found index of
+ * the manifold row o holds (c.order); starts[BG_STARTS] (Contacts.starts); *solved, the rows
+ * before the resting run.  Synchronous; a wait past its budget returns BG_ETIMEOUT.
+ */
+int32_t bg_colour(bg_ctx* ctx, const bg_bodies* bodies, int32_t count, const int32_t* a, const int32_t* b,
+                  int32_t* colour, int32_t* order, int32_t* starts, int32_t* solved);
+/* Device time in milliseconds of the last bg_colour's kernels (synchronises; negative if none). */
+double bg_last_colour_ms(bg_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -137,6 +137,10 @@ int32_t bw_batch_row_memory(const bw_batch* batch, bw_row_memory* out);
  * narrowphase (the one the step itself uses) over any such list, with the bodies' current poses:
  * what bg_collide does on the device. */
 int32_t bw_narrow_pairs(const bw_world* world, bg_pairs* out);
+/* The host's colouring (src/graph.js:105-170, what each step's colour() runs) over any list of
+ * manifolds in found order: bg_colour's arguments and results, on the CPU. */
+int32_t bw_colour_rows(const bg_bodies* bodies, int32_t count, const int32_t* a, const int32_t* b, int32_t* colour,
+                       int32_t* order, int32_t* starts, int32_t* solved);
 int32_t bw_collide_pairs(const bg_bodies* bodies, const double* gravity, const bg_pairs* pairs, bg_manifolds* out,
                          int32_t threads);
 
