@@ -2813,7 +2813,7 @@ double bg_last_collide_ms(bg_ctx* c) {
 namespace {
 
 struct ColourLayout {
-  int32_t *a, *b, *deg, *off, *cursor, *list, *rank, *colour, *bins, *bincur, *order, *starts, *status;
+  int32_t *a, *b, *deg, *off, *cursor, *list, *rank, *colour, *bins, *bincur, *order, *starts, *status, *tiles;
   uint8_t *type, *frozen;
   uint32_t* used;
   unsigned int* done;
@@ -2831,6 +2831,7 @@ ColourLayout colour_layout(unsigned char* base, size_t nb, size_t n) {
   L.bincur = k.take<int32_t>(bgcol::kRuns * nb); L.status = k.take<int32_t>(1);
   L.off = k.take<int32_t>(nb + 1); L.list = k.take<int32_t>(2 * n); L.rank = k.take<int32_t>(2 * n);
   L.colour = k.take<int32_t>(n); L.order = k.take<int32_t>(n); L.starts = k.take<int32_t>(bgcol::kStarts);
+  L.tiles = k.take<int32_t>(bgcol::kRuns * nb / bgcol::kTile + 2);
   L.bytes = k.end;
   return L;
 }
@@ -2918,13 +2919,19 @@ int32_t bg_colour(bg_ctx* c, const bg_bodies* B, int32_t count, const int32_t* a
       return BG_ECUDA;
   }
   bgcol::col_bins<<<rows_grid, 256, 0, st>>>(p);
-  bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(L.bins, L.bins, bgcol::kRuns * static_cast<int>(nb));
+  {
+    const int nbins = bgcol::kRuns * static_cast<int>(nb);
+    const int tiles = (nbins + bgcol::kTile - 1) / bgcol::kTile;
+    bgcol::col_tile_sums<<<tiles, bgcol::kScanThreads, 0, st>>>(L.bins, nbins, L.tiles);
+    bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(L.tiles, L.tiles, tiles);
+    bgcol::col_tile_scan<<<tiles, bgcol::kScanThreads, 0, st>>>(L.bins, L.bins, nbins, L.tiles);
+  }
   bgcol::col_scatter<<<rows_grid, 256, 0, st>>>(p);
   bgcol::col_settle<<<bin_grid, 256, 0, st>>>(p);
   bgcol::col_starts<<<1, 64, 0, st>>>(p);
   cudaEventRecord(d.end, st);
   d.timed = true;
-  c->last_launches += 10;
+  c->last_launches += 12;
   if (!cuda_ok(c, cudaGetLastError(), "bg_colour launch")) return BG_ECUDA;
   int32_t status = 0;
   ok = cuda_ok(c, cudaMemcpyAsync(&status, L.status, sizeof status, cudaMemcpyDeviceToHost, st), "bg_colour") &&

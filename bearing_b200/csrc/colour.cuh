@@ -104,6 +104,55 @@ __global__ void __launch_bounds__(kScanThreads) col_scan(const int32_t* in, int3
   if (t == kScanThreads - 1) out[n] = sums[t];
 }
 
+// The same scan across many blocks, for long arrays (the (colour, b) bins): each block sums a tile
+// of kTile entries (col_tile_sums), one block scans the tiles' sums in place (col_scan, n = the
+// tile count), and each block then scans its tile from its offset (col_tile_scan).  in and out may
+// be the same array.
+constexpr int kTile = kScanThreads * 8;
+__global__ void __launch_bounds__(kScanThreads) col_tile_sums(const int32_t* in, int n, int32_t* tile_sums) {
+  __shared__ int32_t part[kScanThreads / 32];
+  const int base = blockIdx.x * kTile;
+  int32_t s = 0;
+  for (int i = base + threadIdx.x; i < min(n, base + kTile); i += kScanThreads) s += in[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int32_t t = part[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads) col_tile_scan(const int32_t* in, int32_t* out, int n,
+                                                             const int32_t* tile_offsets) {
+  __shared__ int32_t sums[kScanThreads];
+  const int t = threadIdx.x;
+  const int lo = min(n, blockIdx.x * kTile + t * 8), hi = min(n, lo + 8);
+  int32_t v[8];
+  int32_t s = 0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    v[j] = lo + j < hi ? in[lo + j] : 0;
+    s += v[j];
+  }
+  sums[t] = s;
+  __syncthreads();
+  for (int d = 1; d < kScanThreads; d <<= 1) {
+    const int32_t x = t >= d ? sums[t - d] : 0;
+    __syncthreads();
+    sums[t] += x;
+    __syncthreads();
+  }
+  int32_t at = tile_offsets[blockIdx.x] + sums[t] - s;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    if (lo + j < hi) out[lo + j] = at;
+    at += v[j];
+  }
+  if (blockIdx.x == gridDim.x - 1 && t == kScanThreads - 1) out[n] = tile_offsets[gridDim.x];
+}
+
 // Each body's manifolds into its stretch of `list` (in any order; col_ranks sorts them).
 __global__ void col_fill(ColourParams p) {
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < p.n; f += gridDim.x * blockDim.x) {
