@@ -511,6 +511,30 @@ struct SoftK {
   double biasRate, massScale, impulseScale;
 };
 
+// The friction cone's projection (src/contact.js:2015-2033): (n1, n2) outside the ellipse of the
+// inverse tangent mass (ma mb; mb mc) scaled to `limit`, brought onto it by Newton's method on the
+// multiplier al, in place.
+template <class T>
+AHD void cone(const T& limit, const T& ma, const T& mb, const T& mc, T& n1, T& n2) {
+  T al = 0, x = n1, y = n2, ll = n1 * n1 + n2 * n2;
+  while (limit > 0) {
+    const T ab = al * mb, d = (1 + al * ma) * (1 + al * mc) - ab * ab;
+    const T px = ma * x + mb * y, py = mb * x + mc * y;
+    const T wx = ((1 + al * mc) * px - ab * py) / d, wy = ((1 + al * ma) * py - ab * px) / d;
+    const T lw = x * wx + y * wy;
+    if (!(lw > 0)) break;
+    const T next = al + (sqrt(ll) / limit - 1) * ll / lw;
+    if (!(next > al)) break;
+    al = next;
+    const T ab2 = al * mb, d2 = (1 + al * ma) * (1 + al * mc) - ab2 * ab2;
+    x = ((1 + al * mc) * n1 - ab2 * n2) / d2; y = ((1 + al * ma) * n2 - ab2 * n1) / d2;
+    ll = x * x + y * y;
+    if (!(ll > limit * limit)) break;
+  }
+  const T scale = limit / sqrt(ll);
+  n1 = x * scale; n2 = y * scale;
+}
+
 // solveRows for one row: src/contact.js:1805-2090.  bias: a solving pass (else relaxing);
 // known: the separations the last relaxing pass left in now[] still hold.
 template <class T>
@@ -644,24 +668,7 @@ AHD void solve_row(const RowIO<T>& r, double h, bool bias, bool known, const Sof
     T n1 = o1 - (tm[0] * v1 + tm[1] * v2), n2 = o2 - (tm[1] * v1 + tm[2] * v2);
     const T limit = mu * pressed, l2 = n1 * n1 + n2 * n2;
     if (l2 > limit * limit) {
-      const T ma = tm[0], mb = tm[1], mc = tm[2];
-      T al = 0, x = n1, y = n2, ll = l2;
-      while (limit > 0) {
-        const T ab = al * mb, d = (1 + al * ma) * (1 + al * mc) - ab * ab;
-        const T px = ma * x + mb * y, py = mb * x + mc * y;
-        const T wx = ((1 + al * mc) * px - ab * py) / d, wy = ((1 + al * ma) * py - ab * px) / d;
-        const T lw = x * wx + y * wy;
-        if (!(lw > 0)) break;
-        const T next = al + (sqrt(ll) / limit - 1) * ll / lw;
-        if (!(next > al)) break;
-        al = next;
-        const T ab2 = al * mb, d2 = (1 + al * ma) * (1 + al * mc) - ab2 * ab2;
-        x = ((1 + al * mc) * n1 - ab2 * n2) / d2; y = ((1 + al * ma) * n2 - ab2 * n1) / d2;
-        ll = x * x + y * y;
-        if (!(ll > limit * limit)) break;
-      }
-      const T scale = limit / sqrt(ll);
-      n1 = x * scale; n2 = y * scale;
+      cone(limit, tm[0], tm[1], tm[2], n1, n2);
       st[RS_SLID] = 1;
     } else {
       st[RS_SLID] = 0;
@@ -1029,87 +1036,644 @@ AHD void forward(const AdjParams& A, const AdjWorld& W, const Lane& lane) {
 // A body whose adjoints the sweep carries: one that moves (the others' values are constants).
 AHD inline bool moving(const AdjParams& A, int s) { return A.type[s] == BG_DYNAMIC && A.inv_mass[s] != 0; }
 
+// ---- the row passes' reverse, by hand ----
+//
+// The warm start and the solve / relax row are the bulk of the replays (three a row a substep), so
+// their vector-Jacobian products are written out instead of recorded: each runs the row forward in
+// double from its record, keeping what the reverse needs, then carries the adjoints back through
+// the same steps in reverse order, with the branches the forward took (the block's active set, the
+// clamps that held, whether the cone projected).  Only the cone's Newton rounds, a short loop whose
+// length varies, are replayed on the thread's tape.  The derivatives are those the recorded replay
+// gives (the same functions of the same branches), to rounding.
+
+// b += M^T g for the symmetric 3x3 M stored xx xy xz yy yz zz, with M's adjoints: for w -= M l
+// (sign -1) or w += M l (sign 1), given w's adjoint g, returns l's adjoint contribution in bl and
+// adds to M's adjoint bm.
+AHD inline void sym_apply_vjp(const double* M, const double* l, const double* g, double sign, double* bl, double* bm) {
+  bl[0] += sign * (M[0] * g[0] + M[1] * g[1] + M[2] * g[2]);
+  bl[1] += sign * (M[1] * g[0] + M[3] * g[1] + M[4] * g[2]);
+  bl[2] += sign * (M[2] * g[0] + M[4] * g[1] + M[5] * g[2]);
+  if (bm == nullptr) return;
+  bm[0] += sign * g[0] * l[0];
+  bm[1] += sign * (g[0] * l[1] + g[1] * l[0]);
+  bm[2] += sign * (g[0] * l[2] + g[2] * l[0]);
+  bm[3] += sign * g[1] * l[1];
+  bm[4] += sign * (g[1] * l[2] + g[2] * l[1]);
+  bm[5] += sign * g[2] * l[2];
+}
+
+AHD inline double dot3(const double* x, const double* y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; }
+
+// rotate(q, v, inverse)'s reverse (src/core/math.js:211-219): adds q's and v's adjoints, given the
+// result's (g).  u = s q.xyz, t = 2 u x v, out = v + w t + u x t.
+AHD inline void rotate_vjp(const double* q, const double* v, bool inverse, const double* g, double* bq, double* bv) {
+  const double s = inverse ? -1 : 1;
+  const double u[3] = {q[0] * s, q[1] * s, q[2] * s}, w = q[3];
+  const double t[3] = {2 * (u[1] * v[2] - u[2] * v[1]), 2 * (u[2] * v[0] - u[0] * v[2]), 2 * (u[0] * v[1] - u[1] * v[0])};
+  // out = v + w t + u x t
+  double bt[3] = {w * g[0] + (g[1] * u[2] - g[2] * u[1]), w * g[1] + (g[2] * u[0] - g[0] * u[2]),
+                  w * g[2] + (g[0] * u[1] - g[1] * u[0])};   // w g + g x u
+  double bu[3] = {t[1] * g[2] - t[2] * g[1], t[2] * g[0] - t[0] * g[2], t[0] * g[1] - t[1] * g[0]};   // t x g
+  const double bw = dot3(g, t);
+  // t = 2 u x v
+  bu[0] += 2 * (v[1] * bt[2] - v[2] * bt[1]); bu[1] += 2 * (v[2] * bt[0] - v[0] * bt[2]);
+  bu[2] += 2 * (v[0] * bt[1] - v[1] * bt[0]);
+  if (bv != nullptr) {
+    bv[0] += g[0] + 2 * (bt[1] * u[2] - bt[2] * u[1]);
+    bv[1] += g[1] + 2 * (bt[2] * u[0] - bt[0] * u[2]);
+    bv[2] += g[2] + 2 * (bt[0] * u[1] - bt[1] * u[0]);
+  }
+  bq[0] += s * bu[0]; bq[1] += s * bu[1]; bq[2] += s * bu[2]; bq[3] += bw;
+}
+
+// Which argument Math.max (jsmax) returns: true for the first.
+AHD inline bool jsmax_first(double a, double b) {
+  if (a != a) return true;
+  if (b != b) return false;
+  if (a > b) return true;
+  if (b > a) return false;
+  if (a == 0 && b == 0) return !signbit(a);
+  return true;
+}
+
+// The adjoints one row replay leaves: its bodies' velocities (v a, w a, v b, w b), its state, and
+// additions to its prepared terms, its basis and materials, drift, poses and inertias.
+struct RowBar {
+  double v[12];                  // v a, w a, v b, w b
+  double st[RSTATE];
+  double pr[PREP];
+  double n[3], t1[3], t2[3], mu, d1, d2;
+  double pa[3], pb[3], qa[4], qb[4], sa[3], sb[3], ia[6], ib[6];
+};
+
+AHD inline void zero(double* x, int n) {
+  for (int k = 0; k < n; k++) x[k] = 0;
+}
+
+// warmRows' reverse (src/contact.js:1616-1663).  The row moves its bodies by its impulses and
+// leaves its state as it was: velocities' adjoints pass through, and the impulses, levers, basis
+// and inertias gather theirs.  o: the row's record (state, velocities); b: in, the adjoints of the
+// row's results (v, st); out, those of its input, plus the additions.
+AHD inline void warm_row_vjp(const RowIO<double>& r, RowBar& b) {
+  const double* st = r.st;
+  const double* pr = r.pr;
+  const double* n = r.normal;
+  const double* t1 = r.t1;
+  const double* t2 = r.t2;
+  const double* ga = b.v + 3;   // w a's adjoint
+  const double* gb = b.v + 9;   // w b's adjoint
+  const double bP[3] = {-r.ima * b.v[0] + r.imb * b.v[6], -r.ima * b.v[1] + r.imb * b.v[7],
+                        -r.ima * b.v[2] + r.imb * b.v[8]};
+  for (int k = 0; k < r.count; k++) {
+    const double* jac = &pr[PR_JAC + 12 * k];
+    double* bj = &b.pr[PR_JAC + 12 * k];
+    const double ln = st[RS_NI + k];
+    for (int c = 0; c < 3; c++) {
+      b.n[c] += bP[c] * ln;
+      bj[6 + c] -= ga[c] * ln;
+      bj[9 + c] += gb[c] * ln;
+    }
+    b.st[RS_NI + k] += dot3(bP, n) - dot3(ga, jac + 6) + dot3(gb, jac + 9);
+  }
+  {
+    const double* fj = &pr[PR_FJ];
+    double* bf = &b.pr[PR_FJ];
+    const double l1 = st[RS_TI1], l2 = st[RS_TI2];
+    for (int c = 0; c < 3; c++) {
+      b.t1[c] += bP[c] * l1;
+      b.t2[c] += bP[c] * l2;
+      bf[6 + c] -= ga[c] * l1; bf[18 + c] -= ga[c] * l2;
+      bf[9 + c] += gb[c] * l1; bf[21 + c] += gb[c] * l2;
+    }
+    b.st[RS_TI1] += dot3(bP, t1) - dot3(ga, fj + 6) + dot3(gb, fj + 9);
+    b.st[RS_TI2] += dot3(bP, t2) - dot3(ga, fj + 18) + dot3(gb, fj + 21);
+  }
+  {
+    const double r1 = st[RS_RI1], r2 = st[RS_RI2], sp = st[RS_SI];
+    const double L[3] = {t1[0] * r1 + t2[0] * r2 + n[0] * sp, t1[1] * r1 + t2[1] * r2 + n[1] * sp,
+                         t1[2] * r1 + t2[2] * r2 + n[2] * sp};
+    double bL[3] = {0, 0, 0};
+    sym_apply_vjp(r.ia, L, ga, -1, bL, b.ia);
+    sym_apply_vjp(r.ib, L, gb, 1, bL, b.ib);
+    for (int c = 0; c < 3; c++) {
+      b.t1[c] += bL[c] * r1;
+      b.t2[c] += bL[c] * r2;
+      b.n[c] += bL[c] * sp;
+    }
+    b.st[RS_RI1] += dot3(bL, t1);
+    b.st[RS_RI2] += dot3(bL, t2);
+    b.st[RS_SI] += dot3(bL, n);
+  }
+}
+
+// solveRows' reverse for one row (src/contact.js:1805-2090): the forward in double from the row's
+// record (r: its state and velocities before the pass, poses, prepared terms), then the reverse,
+// block by block from the last: twist, rolling, friction, the normal impulses (the block LCP on
+// its final active set, or the per-point update), the targets and the separations.  b: in, the
+// adjoints of the row's results; out, those of its input, plus the additions.  Returns false if
+// the cone's replay did not fit the tape.
+AHD inline bool solve_row_vjp(const RowIO<double>& r, double h, bool bias, bool known, const SoftK& soft, RowBar& b) {
+  const double* st = r.st;
+  const double* pr = r.pr;
+  const double* n = r.normal;
+  const double* t1 = r.t1;
+  const double* t2 = r.t2;
+  const double inv = 1 / h;
+  const double springy = soft.impulseScale / soft.massScale + COMPLIANCE;
+  const double maxBias = r.tolerance * inv;
+  const int count = r.count;
+  const double ima = r.ima, imb = r.imb;
+  // ---- forward, keeping what the reverse reads ----
+  double dx3[3] = {0, 0, 0}, na[3] = {0, 0, 0}, nb[3] = {0, 0, 0};
+  double sep[P], target[P], ms[P], is[P], give[P];
+  bool tfirst[P];   // the bias clamp returned its first argument
+  if (!known) {
+    for (int c = 0; c < 3; c++) dx3[c] = (r.pb[c] - r.sb[c]) - (r.pa[c] - r.sa[c]);
+    const double dn = dx3[0] * n[0] + dx3[1] * n[1] + dx3[2] * n[2];
+    rotate(r.qa, n[0], n[1], n[2], true, na);
+    rotate(r.qb, n[0], n[1], n[2], true, nb);
+    for (int k = 0; k < count; k++) {
+      const int i3 = 3 * k;
+      sep[k] = dn + (pr[PR_LB + i3] * nb[0] + pr[PR_LB + i3 + 1] * nb[1] + pr[PR_LB + i3 + 2] * nb[2]) -
+               (pr[PR_LA + i3] * na[0] + pr[PR_LA + i3 + 1] * na[1] + pr[PR_LA + i3 + 2] * na[2]) + pr[PR_ADJ + k];
+    }
+  } else {
+    for (int k = 0; k < count; k++) sep[k] = st[RS_NOW + k];
+  }
+  int least_k = -1;
+  {
+    double least = INFINITY;
+    for (int k = 0; k < count; k++)
+      if (sep[k] < least) { least = sep[k]; least_k = k; }
+  }
+  for (int k = 0; k < count; k++) {
+    const double sv = sep[k];
+    tfirst[k] = false;
+    if (sv > 0) {
+      target[k] = sv * inv; ms[k] = 1; is[k] = 0; give[k] = COMPLIANCE;
+    } else if (bias) {
+      tfirst[k] = jsmax_first(soft.biasRate * sv, -maxBias);
+      target[k] = jsmax(soft.biasRate * sv, -maxBias);
+      ms[k] = soft.massScale; is[k] = soft.impulseScale; give[k] = springy;
+    } else {
+      target[k] = 0; ms[k] = 1; is[k] = 0; give[k] = COMPLIANCE;
+    }
+  }
+  const double* K = &pr[PR_K];
+  double V[12];
+  for (int c = 0; c < 3; c++) { V[c] = r.va[c]; V[3 + c] = r.wa[c]; V[6 + c] = r.vb[c]; V[9 + c] = r.wb[c]; }
+  const double V0c[12] = {V[0], V[1], V[2], V[3], V[4], V[5], V[6], V[7], V[8], V[9], V[10], V[11]};
+  double closing[P], solved[P], nraw[P];
+  const bool block = !(count == 1 || !(K[0] > 0));
+  int set = 0;
+  double wanted[P];
+  for (int k = 0; k < count; k++) {
+    const double* jac = &pr[PR_JAC + 12 * k];
+    closing[k] = (V[6] - V[0]) * n[0] + (V[7] - V[1]) * n[1] + (V[8] - V[2]) * n[2] + V[9] * jac[3] +
+                 V[10] * jac[4] + V[11] * jac[5] - V[3] * jac[0] - V[4] * jac[1] - V[5] * jac[2];
+  }
+  if (!block) {
+    for (int k = 0; k < count; k++) {
+      const double old = st[RS_NI + k];
+      nraw[k] = old - pr[PR_NM + k] * ms[k] * (closing[k] + target[k]) - is[k] * old;
+      solved[k] = nraw[k] < 0 ? 0 : nraw[k];
+    }
+  } else {
+    for (int k = 0; k < count; k++) {
+      double rr = -closing[k] - target[k];
+      for (int l = 0; l < count; l++) rr += K[P * k + l] * st[RS_NI + l];
+      wanted[k] = rr;
+      if (rr > 0) set |= 1 << k;
+    }
+    for (int round = 0;; round++) {
+      pushes(K, count, set, give, wanted, solved);
+      int flip = -1;
+      for (int k = 0; k < count && flip < 0; k++) {
+        if (set >> k & 1) {
+          if (solved[k] < 0) flip = k;
+        } else {
+          double rr = -wanted[k];
+          for (int l = 0; l < count; l++) rr += K[P * k + l] * solved[l];
+          if (rr < 0) flip = k;
+        }
+      }
+      if (flip < 0 || round == 1 << count) break;
+      set ^= 1 << flip;
+    }
+  }
+  double next[P], d[P];
+  bool rvset[P], mxset[P];
+  double pressed = 0, twisted = 0;
+  for (int k = 0; k < count; k++) {
+    const double* jac = &pr[PR_JAC + 12 * k];
+    next[k] = solved[k] > 0 ? solved[k] : 0;
+    d[k] = next[k] - st[RS_NI + k];
+    rvset[k] = d[k] > 0 && st[RS_MAXNI + k] == 0;
+    mxset[k] = d[k] > st[RS_MAXNI + k];
+    for (int c = 0; c < 3; c++) {
+      V[c] -= ima * (n[c] * d[k]);
+      V[6 + c] += imb * (n[c] * d[k]);
+      V[3 + c] -= jac[6 + c] * d[k];
+      V[9 + c] += jac[9 + c] * d[k];
+    }
+  }
+  for (int k = 0; k < count; k++) {
+    pressed += next[k];
+    twisted += pr[PR_LEV + k] * next[k];
+  }
+  // friction
+  const double V1[12] = {V[0], V[1], V[2], V[3], V[4], V[5], V[6], V[7], V[8], V[9], V[10], V[11]};
+  const double* fj = &pr[PR_FJ];
+  const double* gj = fj + 12;
+  const double* tm = &pr[PR_TM];
+  const double mu = r.friction[0];
+  const double dv[3] = {V[6] - V[0], V[7] - V[1], V[8] - V[2]};
+  double v1 = dot3(dv, t1) + V[9] * fj[3] + V[10] * fj[4] + V[11] * fj[5] - V[3] * fj[0] - V[4] * fj[1] - V[5] * fj[2];
+  double v2 = dot3(dv, t2) + V[9] * gj[3] + V[10] * gj[4] + V[11] * gj[5] - V[3] * gj[0] - V[4] * gj[1] - V[5] * gj[2];
+  const double s1d = r.drift1[0], s2d = r.drift2[0];
+  const bool drifts = bias && (s1d != 0 || s2d != 0);
+  double b1r = 0, b2r = 0, bsc = 1, bq = 0;
+  bool bscaled = false;
+  if (drifts) {
+    b1r = soft.biasRate * s1d; b2r = soft.biasRate * s2d;
+    const double bb = b1r * b1r + b2r * b2r;
+    double b1 = b1r, b2 = b2r;
+    if (bb > maxBias * maxBias) {
+      bscaled = true;
+      bq = sqrt(bb);
+      bsc = maxBias / bq;
+      b1 *= bsc; b2 *= bsc;
+    }
+    v1 += b1; v2 += b2;
+  }
+  const double o1 = st[RS_TI1], o2 = st[RS_TI2];
+  const double n1 = o1 - (tm[0] * v1 + tm[1] * v2), n2 = o2 - (tm[1] * v1 + tm[2] * v2);
+  const double limit = mu * pressed, l2 = n1 * n1 + n2 * n2;
+  const bool projected = l2 > limit * limit;
+  double n1f = n1, n2f = n2;
+  if (projected) cone(limit, tm[0], tm[1], tm[2], n1f, n2f);
+  const double dd1 = n1f - o1, dd2 = n2f - o2;
+  {
+    const double px = t1[0] * dd1 + t2[0] * dd2, py = t1[1] * dd1 + t2[1] * dd2, pz = t1[2] * dd1 + t2[2] * dd2;
+    V[0] -= ima * px; V[1] -= ima * py; V[2] -= ima * pz;
+    V[6] += imb * px; V[7] += imb * py; V[8] += imb * pz;
+    for (int c = 0; c < 3; c++) {
+      V[3 + c] -= fj[6 + c] * dd1 + gj[6 + c] * dd2;
+      V[9 + c] += fj[9 + c] * dd1 + gj[9 + c] * dd2;
+    }
+  }
+  // rolling
+  const bool rolls = count <= 2;
+  double most = 0, u[3] = {0, 0, 0}, p1 = 0, p2 = 0, n1r0 = 0, n2r0 = 0, rq = 0, rsc = 1, dr1 = 0, dr2 = 0;
+  bool rscaled = false;
+  double Lr[3] = {0, 0, 0};
+  if (rolls) {
+    most = r.patch * pressed;
+    for (int c = 0; c < 3; c++) u[c] = V[9 + c] - V[3 + c];
+    p1 = dot3(u, t1); p2 = dot3(u, t2);
+    n1r0 = st[RS_RI1] - pr[PR_RM1] * p1;
+    n2r0 = st[RS_RI2] - pr[PR_RM2] * p2;
+    const double l2r = n1r0 * n1r0 + n2r0 * n2r0;
+    double n1r = n1r0, n2r = n2r0;
+    if (l2r > most * most) {
+      rscaled = true;
+      rq = sqrt(l2r);
+      rsc = most / rq;
+      n1r *= rsc; n2r *= rsc;
+    }
+    dr1 = n1r - st[RS_RI1]; dr2 = n2r - st[RS_RI2];
+    for (int c = 0; c < 3; c++) Lr[c] = t1[c] * dr1 + t2[c] * dr2;
+    double wa[3] = {V[3], V[4], V[5]}, wb[3] = {V[9], V[10], V[11]};
+    const double* ia = r.ia;
+    const double* ib = r.ib;
+    wa[0] -= ia[0] * Lr[0] + ia[1] * Lr[1] + ia[2] * Lr[2];
+    wa[1] -= ia[1] * Lr[0] + ia[3] * Lr[1] + ia[4] * Lr[2];
+    wa[2] -= ia[2] * Lr[0] + ia[4] * Lr[1] + ia[5] * Lr[2];
+    wb[0] += ib[0] * Lr[0] + ib[1] * Lr[1] + ib[2] * Lr[2];
+    wb[1] += ib[1] * Lr[0] + ib[3] * Lr[1] + ib[4] * Lr[2];
+    wb[2] += ib[2] * Lr[0] + ib[4] * Lr[1] + ib[5] * Lr[2];
+    for (int c = 0; c < 3; c++) { V[3 + c] = wa[c]; V[9 + c] = wb[c]; }
+  }
+  // twist
+  const double limit_s = count == 1 ? SPIN_DISC * mu * r.patch * pressed : mu * twisted;
+  const double s0 = st[RS_SI];
+  const double us = (V[9] - V[3]) * n[0] + (V[10] - V[4]) * n[1] + (V[11] - V[5]) * n[2];
+  const double svr = s0 - pr[PR_SM] * us;
+  const int sclamp = svr > limit_s ? 1 : svr < -limit_s ? -1 : 0;
+  const double sv = sclamp == 1 ? limit_s : sclamp == -1 ? -limit_s : svr;
+  const double ds = sv - s0;
+  const double Ls[3] = {n[0] * ds, n[1] * ds, n[2] * ds};
+  const double V3[12] = {V[0], V[1], V[2], V[3], V[4], V[5], V[6], V[7], V[8], V[9], V[10], V[11]};
+
+  // ---- reverse ----
+  const double b_gap = b.st[RS_GAP];   // gap is the least separation; its input is overwritten
+  double* g = b.v;   // the adjoint of the velocities, from the row's results back to its input
+  double b_pressed = 0, b_twisted = 0, b_mu = 0;
+  // twist: w a -= Ia Ls, w b += Ib Ls; si = sv
+  {
+    double bL[3] = {0, 0, 0};
+    sym_apply_vjp(r.ia, Ls, g + 3, -1, bL, b.ia);
+    sym_apply_vjp(r.ib, Ls, g + 9, 1, bL, b.ib);
+    const double b_ds = dot3(bL, n);
+    for (int c = 0; c < 3; c++) b.n[c] += bL[c] * ds;
+    const double b_sv = b.st[RS_SI] + b_ds;
+    double b_s0 = -b_ds, b_svr = 0, b_limit = 0;
+    if (sclamp == 1) b_limit = b_sv;
+    else if (sclamp == -1) b_limit = -b_sv;
+    else b_svr = b_sv;
+    b_s0 += b_svr;
+    b.pr[PR_SM] += -b_svr * us;
+    const double b_us = -b_svr * pr[PR_SM];
+    for (int c = 0; c < 3; c++) {
+      g[9 + c] += b_us * n[c];
+      g[3 + c] -= b_us * n[c];
+      b.n[c] += b_us * (V3[9 + c] - V3[3 + c]);
+    }
+    if (count == 1) {
+      b_mu += b_limit * SPIN_DISC * r.patch * pressed;
+      b_pressed += b_limit * SPIN_DISC * mu * r.patch;
+    } else {
+      b_mu += b_limit * twisted;
+      b_twisted += b_limit * mu;
+    }
+    b.st[RS_SI] = b_s0;
+  }
+  // rolling
+  if (rolls) {
+    double bL[3] = {0, 0, 0};
+    sym_apply_vjp(r.ia, Lr, g + 3, -1, bL, b.ia);
+    sym_apply_vjp(r.ib, Lr, g + 9, 1, bL, b.ib);
+    for (int c = 0; c < 3; c++) { b.t1[c] += bL[c] * dr1; b.t2[c] += bL[c] * dr2; }
+    const double b_dr1 = dot3(bL, t1), b_dr2 = dot3(bL, t2);
+    const double b_n1r = b.st[RS_RI1] + b_dr1, b_n2r = b.st[RS_RI2] + b_dr2;
+    double b_r1 = -b_dr1, b_r2 = -b_dr2;
+    double b_n1r0 = b_n1r, b_n2r0 = b_n2r;
+    if (rscaled) {
+      b_n1r0 = b_n1r * rsc; b_n2r0 = b_n2r * rsc;
+      const double b_sc = b_n1r * n1r0 + b_n2r * n2r0;
+      const double b_most = b_sc / rq;
+      const double b_q = -b_sc * most / (rq * rq);
+      const double b_l2r = b_q * 0.5 / rq;
+      b_n1r0 += 2 * n1r0 * b_l2r; b_n2r0 += 2 * n2r0 * b_l2r;
+      b_pressed += b_most * r.patch;
+    }
+    b_r1 += b_n1r0; b_r2 += b_n2r0;
+    b.pr[PR_RM1] += -b_n1r0 * p1; b.pr[PR_RM2] += -b_n2r0 * p2;
+    const double b_p1 = -b_n1r0 * pr[PR_RM1], b_p2 = -b_n2r0 * pr[PR_RM2];
+    for (int c = 0; c < 3; c++) {
+      const double bu = b_p1 * t1[c] + b_p2 * t2[c];
+      b.t1[c] += b_p1 * u[c]; b.t2[c] += b_p2 * u[c];
+      g[9 + c] += bu; g[3 + c] -= bu;
+    }
+    b.st[RS_RI1] = b_r1; b.st[RS_RI2] = b_r2;
+  }
+  // friction
+  {
+    const double bP[3] = {-ima * g[0] + imb * g[6], -ima * g[1] + imb * g[7], -ima * g[2] + imb * g[8]};
+    double* bf = &b.pr[PR_FJ];
+    double* bg = bf + 12;
+    double b_dd1 = dot3(bP, t1), b_dd2 = dot3(bP, t2);
+    for (int c = 0; c < 3; c++) {
+      b.t1[c] += bP[c] * dd1; b.t2[c] += bP[c] * dd2;
+      b_dd1 += -g[3 + c] * fj[6 + c] + g[9 + c] * fj[9 + c];
+      b_dd2 += -g[3 + c] * gj[6 + c] + g[9 + c] * gj[9 + c];
+      bf[6 + c] -= g[3 + c] * dd1; bg[6 + c] -= g[3 + c] * dd2;
+      bf[9 + c] += g[9 + c] * dd1; bg[9 + c] += g[9 + c] * dd2;
+    }
+    const double b_n1f = b.st[RS_TI1] + b_dd1, b_n2f = b.st[RS_TI2] + b_dd2;
+    double b_o1 = -b_dd1, b_o2 = -b_dd2;
+    double b_n1 = b_n1f, b_n2 = b_n2f, b_limit = 0, btm[3] = {0, 0, 0};
+    if (projected) {
+      // the cone's rounds, replayed on the tape
+      bgad::Tape* t = bgad::thread_tape();
+      bgad::reset(t);
+      const TV ln1 = bgad::leaf(n1), ln2 = bgad::leaf(n2), llim = bgad::leaf(limit);
+      const TV lma = bgad::leaf(tm[0]), lmb = bgad::leaf(tm[1]), lmc = bgad::leaf(tm[2]);
+      TV x = ln1, y = ln2;
+      cone(llim, lma, lmb, lmc, x, y);
+      if (t->overflow) return false;
+      bgad::clear_adjoints(t);
+      bgad::seed(t, x, b_n1f);
+      bgad::seed(t, y, b_n2f);
+      bgad::sweep(t);
+      b_n1 = bgad::adjoint(t, ln1); b_n2 = bgad::adjoint(t, ln2); b_limit = bgad::adjoint(t, llim);
+      btm[0] = bgad::adjoint(t, lma); btm[1] = bgad::adjoint(t, lmb); btm[2] = bgad::adjoint(t, lmc);
+    }
+    b_mu += b_limit * pressed;
+    b_pressed += b_limit * mu;
+    // n1 = o1 - (tm0 v1 + tm1 v2), n2 = o2 - (tm1 v1 + tm2 v2)
+    b_o1 += b_n1; b_o2 += b_n2;
+    btm[0] += -b_n1 * v1; btm[1] += -b_n1 * v2 - b_n2 * v1; btm[2] += -b_n2 * v2;
+    const double b_v1 = -b_n1 * tm[0] - b_n2 * tm[1], b_v2 = -b_n1 * tm[1] - b_n2 * tm[2];
+    double* bt = &b.pr[PR_TM];
+    bt[0] += btm[0]; bt[1] += btm[1]; bt[2] += btm[2];
+    if (drifts) {
+      double b_b1r = b_v1, b_b2r = b_v2;
+      if (bscaled) {
+        b_b1r = b_v1 * bsc; b_b2r = b_v2 * bsc;
+        const double b_sc = b_v1 * b1r + b_v2 * b2r;
+        const double b_q = -b_sc * maxBias / (bq * bq);
+        const double b_bb = b_q * 0.5 / bq;
+        b_b1r += 2 * b1r * b_bb; b_b2r += 2 * b2r * b_bb;
+      }
+      b.d1 += soft.biasRate * b_b1r;
+      b.d2 += soft.biasRate * b_b2r;
+    }
+    // v1 = dv . t1 + wb . fj[3..5] - wa . fj[0..2]; v2 the same with t2 and g
+    const double dv1[3] = {V1[6] - V1[0], V1[7] - V1[1], V1[8] - V1[2]};
+    for (int c = 0; c < 3; c++) {
+      const double bdv = b_v1 * t1[c] + b_v2 * t2[c];
+      b.t1[c] += b_v1 * dv1[c]; b.t2[c] += b_v2 * dv1[c];
+      g[6 + c] += bdv; g[c] -= bdv;
+      g[9 + c] += b_v1 * fj[3 + c] + b_v2 * gj[3 + c];
+      g[3 + c] -= b_v1 * fj[c] + b_v2 * gj[c];
+      bf[3 + c] += b_v1 * V1[9 + c]; bg[3 + c] += b_v2 * V1[9 + c];
+      bf[c] -= b_v1 * V1[3 + c]; bg[c] -= b_v2 * V1[3 + c];
+    }
+    b.st[RS_TI1] = b_o1; b.st[RS_TI2] = b_o2;
+  }
+  b.mu += b_mu;
+  // the normal impulses
+  double b_next[P], b_closing[P], b_target[P], b_old[P];
+  for (int k = 0; k < count; k++) {
+    b_next[k] = b.st[RS_NI + k] + b_pressed + pr[PR_LEV + k] * b_twisted;
+    b.pr[PR_LEV + k] += b_twisted * next[k];
+    b_closing[k] = 0; b_target[k] = 0; b_old[k] = 0;
+  }
+  {
+    const double bP[3] = {-ima * g[0] + imb * g[6], -ima * g[1] + imb * g[7], -ima * g[2] + imb * g[8]};
+    for (int k = 0; k < count; k++) {
+      const double* jac = &pr[PR_JAC + 12 * k];
+      double* bj = &b.pr[PR_JAC + 12 * k];
+      double b_d = dot3(bP, n) - dot3(g + 3, jac + 6) + dot3(g + 9, jac + 9);
+      for (int c = 0; c < 3; c++) {
+        b.n[c] += bP[c] * d[k];
+        bj[6 + c] -= g[3 + c] * d[k];
+        bj[9 + c] += g[9 + c] * d[k];
+      }
+      if (mxset[k]) { b_d += b.st[RS_MAXNI + k]; b.st[RS_MAXNI + k] = 0; }
+      if (rvset[k]) { b_closing[k] += b.st[RS_RELVEL + k]; b.st[RS_RELVEL + k] = 0; }
+      b_next[k] += b_d;
+      b_old[k] -= b_d;
+    }
+  }
+  double b_solved[P];
+  for (int k = 0; k < count; k++) b_solved[k] = solved[k] > 0 ? b_next[k] : 0;
+  if (!block) {
+    for (int k = 0; k < count; k++) {
+      const double b_raw = nraw[k] < 0 ? 0 : b_solved[k];
+      b_old[k] += b_raw * (1 - is[k]);
+      b.pr[PR_NM + k] += -b_raw * ms[k] * (closing[k] + target[k]);
+      const double c = -b_raw * pr[PR_NM + k] * ms[k];
+      b_closing[k] += c;
+      b_target[k] += c;
+    }
+  } else {
+    // solved = A^-1 wanted on the final set S (A = K_SS, its diagonal times 1 + give): A is
+    // symmetric, so wanted's adjoint is A^-1 times solved's (the same solve), and A's is minus
+    // the outer product of the two
+    double bw[P];
+    pushes(K, count, set, give, b_solved, bw);
+    double* bK = &b.pr[PR_K];
+    for (int k = 0; k < count; k++) {
+      if (!(set >> k & 1)) continue;
+      for (int l = 0; l < count; l++) {
+        if (!(set >> l & 1)) continue;
+        const double scale = k == l ? 1 + give[k] : 1.0;
+        bK[P * k + l] += -bw[k] * solved[l] * scale;
+      }
+      // wanted_k = -closing_k - target_k + sum_l K_kl old_l
+      b_closing[k] -= bw[k];
+      b_target[k] -= bw[k];
+      for (int l = 0; l < count; l++) {
+        bK[P * k + l] += bw[k] * st[RS_NI + l];
+        b_old[l] += bw[k] * K[P * k + l];
+      }
+    }
+  }
+  for (int k = 0; k < count; k++) b.st[RS_NI + k] = b_old[k];
+  // closing_k = (vb - va) . n + wb . jac[3..5] - wa . jac[0..2], at the pass's start
+  for (int k = 0; k < count; k++) {
+    const double* jac = &pr[PR_JAC + 12 * k];
+    double* bj = &b.pr[PR_JAC + 12 * k];
+    const double bc = b_closing[k];
+    for (int c = 0; c < 3; c++) {
+      g[6 + c] += bc * n[c]; g[c] -= bc * n[c];
+      b.n[c] += bc * (V0c[6 + c] - V0c[c]);
+      g[9 + c] += bc * jac[3 + c]; bj[3 + c] += bc * V0c[9 + c];
+      g[3 + c] -= bc * jac[c]; bj[c] -= bc * V0c[3 + c];
+    }
+  }
+  // targets and separations
+  double b_sep[P];
+  for (int k = 0; k < count; k++) {
+    b_sep[k] = 0;
+    if (sep[k] > 0) b_sep[k] = b_target[k] * inv;
+    else if (bias && tfirst[k]) b_sep[k] = b_target[k] * soft.biasRate;
+  }
+  if (least_k >= 0) b_sep[least_k] += b_gap;
+  b.st[RS_GAP] = 0;
+  b.st[RS_SLID] = 0;
+  if (known) {
+    for (int k = 0; k < count; k++) b.st[RS_NOW + k] += b_sep[k];
+  } else {
+    for (int k = 0; k < count; k++)
+      if (!bias) { b_sep[k] += b.st[RS_NOW + k]; b.st[RS_NOW + k] = 0; }
+    double b_dn = 0, b_na[3] = {0, 0, 0}, b_nb[3] = {0, 0, 0};
+    for (int k = 0; k < count; k++) {
+      const int i3 = 3 * k;
+      b_dn += b_sep[k];
+      for (int c = 0; c < 3; c++) {
+        b.pr[PR_LB + i3 + c] += b_sep[k] * nb[c];
+        b_nb[c] += b_sep[k] * pr[PR_LB + i3 + c];
+        b.pr[PR_LA + i3 + c] -= b_sep[k] * na[c];
+        b_na[c] -= b_sep[k] * pr[PR_LA + i3 + c];
+      }
+      b.pr[PR_ADJ + k] += b_sep[k];
+    }
+    for (int c = 0; c < 3; c++) {
+      const double bd = b_dn * n[c];
+      b.n[c] += b_dn * dx3[c];
+      b.pb[c] += bd; b.sb[c] -= bd; b.pa[c] -= bd; b.sa[c] += bd;
+    }
+    rotate_vjp(r.qa, n, true, b_na, b.qa, b.n);
+    rotate_vjp(r.qb, n, true, b_nb, b.qb, b.n);
+  }
+  return true;
+}
+
 // Replays row m of a pass (kind WARM / SOLVE / RELAX, substep sub) from its record.  The poses it
 // reads (relax, and the first substep's solve) are those after the substep's move: the next
 // substep's record before its move, or the step's last.
 template <class Lane>
 AHD void replay_pass_row(const AdjParams& A, const AdjWorld& W, int m, int pass, int sub, double h) {
-  bgad::Tape* t = bgad::thread_tape();
-  bgad::reset(t);
   const int kind = pass % 3;
-  const RowIO<double> r = row_io(A, W, m);
+  RowIO<double> r = row_io(A, W, m);
   const int a = W.body0 + A.a[m], b = W.body0 + A.b[m];
   const double* rec = A.rec_row + (static_cast<int64_t>(pass) * A.rows_total + m) * REC_ROW;
-  RowLeaves L;
-  leaves(L.st, rec, RSTATE);
-  leaves(L.va, rec + RSTATE, 3); leaves(L.wa, rec + RSTATE + 3, 3);
-  leaves(L.vb, rec + RSTATE + 6, 3); leaves(L.wb, rec + RSTATE + 9, 3);
-  const double* pa;
-  const double* pb;
-  const double* qa;
-  const double* qb;
+  // the row's input as the record holds it: its state and its bodies' velocities before the pass
+  double st[RSTATE], va[3], wa[3], vb[3], wb[3];
+  for (int k = 0; k < RSTATE; k++) st[k] = rec[k];
+  for (int c = 0; c < 3; c++) {
+    va[c] = rec[RSTATE + c]; wa[c] = rec[RSTATE + 3 + c]; vb[c] = rec[RSTATE + 6 + c]; wb[c] = rec[RSTATE + 9 + c];
+  }
+  r.st = st; r.va = va; r.wa = wa; r.vb = vb; r.wb = wb;
+  double drift1 = A.in_drift1[m], drift2 = A.in_drift2[m];   // the step's input: only slipped() moves them
+  r.drift1 = &drift1; r.drift2 = &drift2;
   const bool reads_pose = kind == RELAX || (kind == SOLVE && sub == 0);
   // during relax(sub): after move(sub); during solve(0): before move(0)
   const int at = kind == RELAX ? sub + 1 : sub;
   if (at < A.substeps) {
     const double* ra = A.rec_body + (static_cast<int64_t>(at) * A.bodies_total + a) * REC_BODY;
     const double* rb = A.rec_body + (static_cast<int64_t>(at) * A.bodies_total + b) * REC_BODY;
-    pa = A.awake[a] ? ra + RB_P : A.p + 3 * a; qa = A.awake[a] ? ra + RB_Q : A.q + 4 * a;
-    pb = A.awake[b] ? rb + RB_P : A.p + 3 * b; qb = A.awake[b] ? rb + RB_Q : A.q + 4 * b;
+    r.pa = A.awake[a] ? ra + RB_P : A.p + 3 * a; r.qa = A.awake[a] ? ra + RB_Q : A.q + 4 * a;
+    r.pb = A.awake[b] ? rb + RB_P : A.p + 3 * b; r.qb = A.awake[b] ? rb + RB_Q : A.q + 4 * b;
   } else {
-    pa = A.p + 3 * a; qa = A.q + 4 * a; pb = A.p + 3 * b; qb = A.q + 4 * b;
+    r.pa = A.p + 3 * a; r.qa = A.q + 4 * a; r.pb = A.p + 3 * b; r.qb = A.q + 4 * b;
   }
-  leaves(L.pa, pa, 3); leaves(L.pb, pb, 3); leaves(L.qa, qa, 4); leaves(L.qb, qb, 4);
-  leaves(L.sa, r.sa, 3); leaves(L.sb, r.sb, 3);
-  leaves(L.ia, r.ia, 6); leaves(L.ib, r.ib, 6);
-  leaves(L.pr, r.pr, PREP);
-  leaves(L.normal, r.normal, 3); leaves(L.t1, r.t1, 3); leaves(L.t2, r.t2, 3);
-  L.friction = bgad::leaf(r.friction[0]);
-  L.drift1 = bgad::leaf(A.in_drift1[m]); L.drift2 = bgad::leaf(A.in_drift2[m]);
-  // The row overwrites its bodies' velocities and its state in L: keep the leaves it reads there.
-  TV in_v[12], in_st[RSTATE];
-  for (int c = 0; c < 3; c++) { in_v[c] = L.va[c]; in_v[3 + c] = L.wa[c]; in_v[6 + c] = L.vb[c]; in_v[9 + c] = L.wb[c]; }
-  for (int k = 0; k < RSTATE; k++) in_st[k] = L.st[k];
-  const RowIO<TV> o = leaf_io(L, r);
-  if (kind == WARM) warm_row(o);
-  else solve_row(o, h, kind == SOLVE, kind == SOLVE && sub > 0, A.soft);
-  if (t->overflow) {
+  const bool ma = moving(A, a), mb = moving(A, b);
+  RowBar B;
+  zero(B.v, 12); zero(B.pr, PREP); zero(B.n, 3); zero(B.t1, 3); zero(B.t2, 3); B.mu = 0; B.d1 = 0; B.d2 = 0;
+  zero(B.pa, 3); zero(B.pb, 3); zero(B.qa, 4); zero(B.qb, 4); zero(B.sa, 3); zero(B.sb, 3); zero(B.ia, 6); zero(B.ib, 6);
+  for (int c = 0; c < 3; c++) {
+    if (ma) { B.v[c] = A.bv[3 * a + c]; B.v[3 + c] = A.bw[3 * a + c]; }
+    if (mb) { B.v[6 + c] = A.bv[3 * b + c]; B.v[9 + c] = A.bw[3 * b + c]; }
+  }
+  double* bst = A.bst + RSTATE * static_cast<int64_t>(m);
+  for (int k = 0; k < RSTATE; k++) B.st[k] = bst[k];
+  if (kind == WARM) {
+    warm_row_vjp(r, B);
+  } else if (!solve_row_vjp(r, h, kind == SOLVE, kind == SOLVE && sub > 0, A.soft, B)) {
     *A.status = 1;
     return;
   }
-  bgad::clear_adjoints(t);
-  const bool ma = moving(A, a), mb = moving(A, b);
+  // results: the adjoints of the state and velocities it read replace those of what it wrote;
+  // everything else it read adds to its adjoint
+  for (int k = 0; k < RSTATE; k++) bst[k] = B.st[k];
   for (int c = 0; c < 3; c++) {
-    if (ma) { bgad::seed(t, L.va[c], A.bv[3 * a + c]); bgad::seed(t, L.wa[c], A.bw[3 * a + c]); }
-    if (mb) { bgad::seed(t, L.vb[c], A.bv[3 * b + c]); bgad::seed(t, L.wb[c], A.bw[3 * b + c]); }
+    if (ma) { A.bv[3 * a + c] = B.v[c]; A.bw[3 * a + c] = B.v[3 + c]; }
+    if (mb) { A.bv[3 * b + c] = B.v[6 + c]; A.bw[3 * b + c] = B.v[9 + c]; }
   }
-  double* bst = A.bst + RSTATE * static_cast<int64_t>(m);
-  for (int k = 0; k < RSTATE; k++) bgad::seed(t, L.st[k], bst[k]);
-  bgad::sweep(t);
-  // results: the state and velocities it read replace the adjoints of what it wrote; everything
-  // else it read adds to its adjoint
-  set_adjoints(bst, t, in_st, RSTATE);
-  if (ma) { set_adjoints(A.bv + 3 * a, t, in_v, 3); set_adjoints(A.bw + 3 * a, t, in_v + 3, 3); }
-  if (mb) { set_adjoints(A.bv + 3 * b, t, in_v + 6, 3); set_adjoints(A.bw + 3 * b, t, in_v + 9, 3); }
   if (reads_pose) {
     if (ma) {
-      add_adjoints(A.bp + 3 * a, t, L.pa, 3); add_adjoints(A.bq + 4 * a, t, L.qa, 4);
-      add_adjoints(A.bstart + 3 * a, t, L.sa, 3);
+      for (int c = 0; c < 3; c++) { A.bp[3 * a + c] += B.pa[c]; A.bstart[3 * a + c] += B.sa[c]; }
+      for (int c = 0; c < 4; c++) A.bq[4 * a + c] += B.qa[c];
     }
     if (mb) {
-      add_adjoints(A.bp + 3 * b, t, L.pb, 3); add_adjoints(A.bq + 4 * b, t, L.qb, 4);
-      add_adjoints(A.bstart + 3 * b, t, L.sb, 3);
+      for (int c = 0; c < 3; c++) { A.bp[3 * b + c] += B.pb[c]; A.bstart[3 * b + c] += B.sb[c]; }
+      for (int c = 0; c < 4; c++) A.bq[4 * b + c] += B.qb[c];
     }
   }
-  if (ma) add_adjoints(A.binvI + 6 * a, t, L.ia, 6);
-  if (mb) add_adjoints(A.binvI + 6 * b, t, L.ib, 6);
-  add_adjoints(A.bpr + PREP * static_cast<int64_t>(m), t, L.pr, PREP);
-  add_adjoints(A.bnormal + 3 * m, t, L.normal, 3);
-  add_adjoints(A.bt1 + 3 * m, t, L.t1, 3);
-  add_adjoints(A.bt2 + 3 * m, t, L.t2, 3);
-  A.bfriction[m] += bgad::adjoint(t, L.friction);
-  A.bdrift1[m] += bgad::adjoint(t, L.drift1);
-  A.bdrift2[m] += bgad::adjoint(t, L.drift2);
+  if (ma) for (int c = 0; c < 6; c++) A.binvI[6 * a + c] += B.ia[c];
+  if (mb) for (int c = 0; c < 6; c++) A.binvI[6 * b + c] += B.ib[c];
+  double* bpr = A.bpr + PREP * static_cast<int64_t>(m);
+  for (int k = PR_LA; k < PREP; k++) bpr[k] += B.pr[k];   // a row pass reads no PR_RA / PR_RB
+  for (int c = 0; c < 3; c++) {
+    A.bnormal[3 * m + c] += B.n[c]; A.bt1[3 * m + c] += B.t1[c]; A.bt2[3 * m + c] += B.t2[c];
+  }
+  A.bfriction[m] += B.mu;
+  A.bdrift1[m] += B.d1;
+  A.bdrift2[m] += B.d2;
 }
 
 template <class Lane>
