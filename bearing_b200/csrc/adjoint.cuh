@@ -1666,8 +1666,30 @@ AHD void replay_pass_row(const AdjParams& A, const AdjWorld& W, int m, int pass,
   }
   if (ma) for (int c = 0; c < 6; c++) A.binvI[6 * a + c] += B.ia[c];
   if (mb) for (int c = 0; c < 6; c++) A.binvI[6 * b + c] += B.ib[c];
+  // the prepared terms the pass read, and only those (the rest of B.pr is 0)
   double* bpr = A.bpr + PREP * static_cast<int64_t>(m);
-  for (int k = PR_LA; k < PREP; k++) bpr[k] += B.pr[k];   // a row pass reads no PR_RA / PR_RB
+  auto flush = [&](int from, int to) {
+    for (int k = from; k < to; k++) bpr[k] += B.pr[k];
+  };
+  const int count = r.count;
+  if (kind == WARM) {
+    for (int k = 0; k < count; k++) flush(PR_JAC + 12 * k + 6, PR_JAC + 12 * k + 12);
+    flush(PR_FJ + 6, PR_FJ + 12);
+    flush(PR_FJ + 18, PR_FJ + 24);
+  } else {
+    if (reads_pose) {
+      flush(PR_LA, PR_LA + 3 * count);
+      flush(PR_LB, PR_LB + 3 * count);
+      flush(PR_ADJ, PR_ADJ + count);
+    }
+    flush(PR_NM, PR_NM + count);
+    flush(PR_JAC, PR_JAC + 12 * count);
+    for (int k = 0; k < count; k++) flush(PR_K + P * k, PR_K + P * k + count);
+    flush(PR_LEV, PR_LEV + count);
+    flush(PR_FJ, PR_TM + 3);   // FJ (24) then TM (3)
+    if (count <= 2) flush(PR_RM1, PR_RM2 + 1);
+    flush(PR_SM, PR_SM + 1);
+  }
   for (int c = 0; c < 3; c++) {
     A.bnormal[3 * m + c] += B.n[c]; A.bt1[3 * m + c] += B.t1[c]; A.bt2[3 * m + c] += B.t2[c];
   }
@@ -1856,21 +1878,33 @@ AHD void reverse(const AdjParams& A, const AdjWorld& W, const Lane& lane) {
       reverse_pass(A, W, lane, 3 * sub + SOLVE, sub, h);
       reverse_pass(A, W, lane, 3 * sub + WARM, sub, h);
     }
-    // accelerate (src/world.js:1495-1530)
+    // accelerate (src/world.js:1495-1530), its reverse written out: gravity adds a constant, the
+    // dampings scale, and the spin limit scales w onto the sphere of radius `most` when it holds
     for (int i = W.awake0 + lane.id; i < W.awake0 + W.nawake; i += lane.n) {
       const int s = W.body0 + A.awake_list[i];
       if (!moving(A, s)) continue;
-      bgad::Tape* t = bgad::thread_tape();
-      bgad::reset(t);
+      const BodyConst bc = body_const(A, s);
+      if (!bc.dynamic) continue;
       const double* rec = A.rec_body + (static_cast<int64_t>(sub) * A.bodies_total + s) * REC_BODY;
-      TV v[3], w[3];
-      leaves(v, rec + RB_ACC, 3); leaves(w, rec + RB_ACC + 3, 3);
-      TV v1[3] = {v[0], v[1], v[2]}, w1[3] = {w[0], w[1], w[2]};
-      accelerate(body_const(A, s), W.gravity, h, A.substeps, v1, w1);
-      bgad::clear_adjoints(t);
-      for (int k = 0; k < 3; k++) { bgad::seed(t, v1[k], A.bv[3 * s + k]); bgad::seed(t, w1[k], A.bw[3 * s + k]); }
-      bgad::sweep(t);
-      set_adjoints(A.bv + 3 * s, t, v, 3); set_adjoints(A.bw + 3 * s, t, w, 3);
+      const double most = WORLD_SPIN / (h * A.substeps);
+      const double kv = bc.damping != 0 ? 1 / (1 + h * bc.damping) : 1.0;
+      const double kw = bc.angular_damping != 0 ? 1 / (1 + h * bc.angular_damping) : 1.0;
+      double w1[3];
+      for (int k = 0; k < 3; k++) w1[k] = bc.angular_damping != 0 ? rec[RB_ACC + 3 + k] * kw : rec[RB_ACC + 3 + k];
+      double* bw = A.bw + 3 * s;
+      if (!bc.sphere_unframed) {
+        const double w2 = w1[0] * w1[0] + w1[1] * w1[1] + w1[2] * w1[2];
+        if (w2 > most * most) {
+          const double q = sqrt(w2), c = most / q;
+          const double b_c = bw[0] * w1[0] + bw[1] * w1[1] + bw[2] * w1[2];
+          const double b_w2 = -b_c * most / (q * q) * 0.5 / q;
+          for (int k = 0; k < 3; k++) bw[k] = c * bw[k] + 2 * w1[k] * b_w2;
+        }
+      }
+      for (int k = 0; k < 3; k++) {
+        if (bc.angular_damping != 0) bw[k] *= kw;
+        if (bc.damping != 0) A.bv[3 * s + k] *= kv;
+      }
     }
     lane.sync();
   }
