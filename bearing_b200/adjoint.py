@@ -154,6 +154,15 @@ class _Memory:
                                 self.memory.ctypes.data_as(_PD))
 
 
+def _host_threads():
+    """The host threads this process may run on (its CPU affinity, which may be fewer than the
+    machine's CPUs)."""
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 class BatchBackward:
     """Steps a list of Worlds together (their host sides on the CPU, their solve stages as one batch
     on the GPU) and differentiates a loss on their final state.  The worlds are left in their
@@ -167,7 +176,7 @@ class BatchBackward:
         self.ctx = self.gpu.bg_create(device, 0)
         if not self.ctx:
             raise RuntimeError(f"bg_create({device}) failed: no usable CUDA device")
-        self.threads = threads or (os.cpu_count() or 1)
+        self.threads = threads or _host_threads()
         handles = (C.c_void_p * len(self.worlds))(*[w._w for w in self.worlds])
         self.batch = self.host.bw_batch_create(handles, len(self.worlds))
         counts = [w._count for w in self.worlds]

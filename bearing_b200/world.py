@@ -266,7 +266,11 @@ class Batch:
         self.ctx = self._gpu.bg_create(device, 0)
         if not self.ctx:
             raise BearingError(f"bg_create({device}) failed: no usable CUDA device")
-        self.threads = threads or max(1, (_os.cpu_count() or 1))
+        try:
+            affinity = len(_os.sched_getaffinity(0))   # the CPUs this process may run on
+        except AttributeError:
+            affinity = _os.cpu_count() or 1
+        self.threads = threads or max(1, affinity)
 
     def begin_step(self, dt: float):
         rc = self._lib.bw_batch_begin_step(self._b, float(dt), self.threads)
