@@ -167,6 +167,25 @@ class Manifolds(C.Structure):
                 ("pid", C.POINTER(C.c_uint32))]
 
 
+class Materials(C.Structure):
+    """bg_materials: per-slot friction, restitution and size, what emit() reads."""
+
+    _fields_ = [("friction", _d), ("restitution", _d), ("size", _d)]
+
+
+class ContactPairs(C.Structure):
+    """bg_contact_pairs: the step's pair list with each pair's contact record (or -1)."""
+
+    _fields_ = [("list", Pairs), ("memory", _i32)]
+
+
+class ContactResult(C.Structure):
+    """bg_contact_result: per-pair point counts and touching flags, and the step's row counts."""
+
+    _fields_ = [("points", _u8), ("touching", _u8), ("rows", C.c_int32), ("solved", C.c_int32),
+                ("points_solved", C.c_int32), ("starts", C.c_int32 * 35)]
+
+
 class Options(C.Structure):
     _fields_ = [("gravity", C.c_double * 3), ("substeps", C.c_int32)]
 
@@ -257,13 +276,14 @@ def host() -> C.CDLL:
         lib.bw_copy.argtypes = [C.c_void_p, C.c_void_p]
         lib.bw_narrow_pairs.argtypes = [C.c_void_p, C.POINTER(Pairs)]
         lib.bw_set_narrowphase.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.bw_set_contact_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         lib.bw_colour_rows.argtypes = [C.POINTER(Bodies), C.c_int32, _i32, _i32, _i32, _i32, _i32, _i32]
         lib.bw_collide_pairs.argtypes = [C.POINTER(Bodies), _d, C.POINTER(Pairs), C.POINTER(Manifolds), C.c_int32]
         for f in ("bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step", "bw_end_step",
                   "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_stats_get", "bw_batch_begin_step",
                   "bw_batch_views", "bw_batch_end_step", "bw_row_memory_get", "bw_batch_row_memory", "bw_copy",
                   "bw_keep_backward", "bw_narrow_backward", "bw_materials", "bw_narrow_pairs", "bw_collide_pairs",
-                  "bw_set_narrowphase", "bw_colour_rows"):
+                  "bw_set_narrowphase", "bw_colour_rows", "bw_set_contact_step"):
             getattr(lib, f).restype = C.c_int32
         _host = lib
     return _host
@@ -309,6 +329,15 @@ def gpu() -> C.CDLL:
         lib.bg_colour.argtypes = [C.c_void_p, C.POINTER(Bodies), C.c_int32, _i32, _i32, _i32, _i32, _i32, _i32]
         lib.bg_colour.restype = C.c_int32
         lib.bg_last_colour_ms.argtypes = [C.c_void_p]
+        lib.bg_contact_step.argtypes = [C.c_void_p, C.POINTER(Bodies), C.POINTER(Materials), C.POINTER(ContactPairs),
+                                        C.POINTER(Step), C.POINTER(ContactResult)]
+        lib.bg_contact_step.restype = C.c_int32
+        lib.bg_last_contact_ms.argtypes = [C.c_void_p, _d]
+        lib.bg_last_contact_ms.restype = C.c_int32
+        lib.bg_contact_records.argtypes = [C.c_void_p]
+        lib.bg_contact_records.restype = C.c_int32
+        lib.bg_contact_forget.argtypes = [C.c_void_p]
+        lib.bg_contact_forget.restype = C.c_int32
         lib.bg_last_colour_ms.restype = C.c_double
         lib.bg_last_collide_ms.argtypes = [C.c_void_p]
         lib.bg_last_collide_ms.restype = C.c_double
@@ -346,7 +375,8 @@ GPU_SYMBOLS = [
     "bg_batch_download", "bg_stream", "bg_last_launches", "bg_last_stage_ms", "bg_set_wait_budget", "bg_set_block_threads",
     "bg_block_threads", "bg_set_batch_groups", "bg_backward", "bg_backward_tape_peak", "bg_backward_ms",
     "bg_solve_step_static", "bg_register_host", "bg_unregister_host", "bg_registered_bytes", "bg_collide",
-    "bg_last_collide_ms", "bg_backward_bytes", "bg_colour", "bg_last_colour_ms",
+    "bg_last_collide_ms", "bg_backward_bytes", "bg_colour", "bg_last_colour_ms", "bg_contact_step",
+    "bg_last_contact_ms", "bg_contact_records", "bg_contact_forget",
 ]
 HOST_SYMBOLS = [
     "bw_create", "bw_destroy", "bw_last_error", "bw_add_body", "bw_set_solver", "bw_step", "bw_begin_step",
@@ -354,4 +384,5 @@ HOST_SYMBOLS = [
     "bw_batch_create", "bw_batch_destroy", "bw_batch_begin_step", "bw_batch_views", "bw_batch_end_step",
     "bw_row_memory_get", "bw_batch_row_memory", "bw_clone", "bw_copy", "bw_keep_backward", "bw_narrow_backward",
     "bw_materials", "bw_narrow_pairs", "bw_collide_pairs", "bw_set_narrowphase", "bw_colour_rows",
+    "bw_set_contact_step",
 ]

@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 CXX = os.environ.get("CXX", shutil.which("g++") or "g++")
 
 GPU_SOURCES = [os.path.join(PKG, "csrc", "bearing_gpu.cu")]
-GPU_DEPS = [os.path.join(PKG, "csrc", f) for f in ("layout.cuh", "stage.cuh", "adjoint.cuh", "tape.hpp", "colour.cuh")] + [
+GPU_DEPS = [os.path.join(PKG, "csrc", f) for f in ("layout.cuh", "stage.cuh", "adjoint.cuh", "tape.hpp", "colour.cuh", "contact.cuh")] + [
     os.path.join(PKG, "host", "collide_impl.hpp"), os.path.join(PKG, "host", "collide.hpp"),
     os.path.join(ROOT, "include", "bearing_gpu.h")]
 HOST_SOURCES = [os.path.join(PKG, "host", "world.cpp"), os.path.join(PKG, "host", "collide.cpp")]

@@ -34,6 +34,7 @@
 #include "adjoint.cuh"
 #include "../host/collide_impl.hpp"
 #include "colour.cuh"
+#include "contact.cuh"
 
 namespace {
 
@@ -439,8 +440,9 @@ struct bg_ctx {
   int last_launches = 0;
   cudaEvent_t stage_begin = nullptr, stage_end = nullptr;
   bool stage_timed = false;
-  // capacities
-  int body_cap = 0, row_cap = 0, awake_cap = 0, world_cap = 0;
+  // capacities (stage_row_cap: rows the staging blocks hold; in_bytes: the upload block's size)
+  int body_cap = 0, row_cap = 0, awake_cap = 0, world_cap = 0, stage_row_cap = 0;
+  size_t in_bytes = 0;
   // device allocations, all freed in bg_destroy
   std::vector<void*> allocs;
   // body records
@@ -473,6 +475,7 @@ struct bg_ctx {
   std::vector<int32_t> world_order;
   int block_threads = 0;
   std::vector<int2> chunks;
+  int32_t nchunks = 0;   // the grid's runs (chunks.size(), or as the device worked them out)
   // bg_batch_solve_step's groups of worlds (see batch_in_groups): how many (0 by the batch's rows),
   // and a context of its own for each
   int batch_groups = 0;
@@ -522,6 +525,19 @@ struct bg_ctx {
     cudaEvent_t begin = nullptr, end = nullptr;
     bool timed = false;
   } col;
+  // bg_contact_step's device memory: a scratch block for the call (grown by doubling) and two
+  // banks of contact memory, the last call's `count` records in bank `current`
+  struct Contact {
+    unsigned char* block = nullptr;
+    size_t bodies = 0, pairs = 0;
+    unsigned char* banks = nullptr;
+    size_t bank_cap = 0;
+    int current = 0;
+    int32_t count = 0;
+    int32_t* summary = nullptr;   // pinned: the call's few counts on their way to the host
+    cudaEvent_t ev[4] = {};
+    bool timed = false;
+  } ct;
   // bg_backward's own device memory (grown by doubling, freed with the context)
   struct Adjoint {
     std::vector<void*> allocs;
@@ -695,9 +711,13 @@ size_t meta_bytes(size_t nb, size_t nr) {
 }
 
 // (Re)allocates every buffer for at least the given sizes.  Everything is reallocated together,
-// so a resize never leaves a stale pointer behind.
-bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
-  if (nbodies <= c->body_cap && nrows <= c->row_cap && nawake <= c->awake_cap && nworlds <= c->world_cap && c->bar)
+// so a resize never leaves a stale pointer behind.  The staging blocks hold the columns of
+// `stage_rows` rows (-1: nrows) and at least `in_need` bytes on the way in (bg_contact_step stages
+// bodies and pairs, not rows).
+bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds, int stage_rows = -1, size_t in_need = 0) {
+  if (stage_rows < 0) stage_rows = nrows;
+  if (nbodies <= c->body_cap && nrows <= c->row_cap && nawake <= c->awake_cap && nworlds <= c->world_cap &&
+      stage_rows <= c->stage_row_cap && in_need <= c->in_bytes && c->bar)
     return true;
   cudaStreamSynchronize(c->stream);
   free_all(c);
@@ -705,6 +725,8 @@ bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
   const size_t nr = grown(c->row_cap, static_cast<size_t>(nrows));
   const size_t na = grown(c->awake_cap, static_cast<size_t>(nawake));
   const size_t nw = grown(c->world_cap, static_cast<size_t>(nworlds));
+  const size_t sr = static_cast<size_t>(stage_rows) <= static_cast<size_t>(c->stage_row_cap)
+                        ? static_cast<size_t>(c->stage_row_cap) : grown(c->stage_row_cap, static_cast<size_t>(stage_rows));
   bool ok = true;
   bg::BodiesDev& B = c->B;
   B.deg = nullptr;
@@ -734,12 +756,13 @@ bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
        dev_alloc(c, &c->deg_dev, nb) && dev_alloc(c, &c->done_dev, nb) && dev_alloc(c, &c->chunks_dev, nr + 64) &&
        dev_alloc(c, &c->body_world_dev, nb) && dev_alloc(c, &c->brun_rows_dev, nr) && dev_alloc(c, &c->bruns_dev, nr + 64);
   // staging blocks, sized for the capacities (a call's own layout is never larger)
+  size_t in_bytes = 0;
   {
-    const size_t in_bytes = plan_in(c, nullptr, nullptr, nb, nr, na, nullptr).end;
-    const size_t out_bytes = plan_out(c, nullptr, nullptr, nb, nr, nullptr).end;
+    in_bytes = std::max(plan_in(c, nullptr, nullptr, nb, sr, na, nullptr).end, in_need);
+    const size_t out_bytes = plan_out(c, nullptr, nullptr, nb, sr, nullptr).end;
     ok = ok && dev_alloc(c, &c->d_in, in_bytes) && dev_alloc(c, &c->d_out, out_bytes) &&
          host_alloc(c, &c->h_in, in_bytes) && host_alloc(c, &c->h_out, out_bytes) &&
-         host_alloc(c, &c->h_meta, meta_bytes(nb, nr));
+         host_alloc(c, &c->h_meta, meta_bytes(nb, sr));
   }
   // worlds
   ok = ok && dev_alloc(c, &c->worlds_dev, nw) && dev_alloc(c, &c->order_dev, nw) && dev_alloc(c, &c->body_offset_dev, nw + 1) &&
@@ -752,6 +775,8 @@ bool ensure(bg_ctx* c, int nbodies, int nrows, int nawake, int nworlds) {
   c->row_cap = static_cast<int>(nr);
   c->awake_cap = static_cast<int>(na);
   c->world_cap = static_cast<int>(nw);
+  c->stage_row_cap = static_cast<int>(sr);
+  c->in_bytes = in_bytes;
   return true;
 }
 
@@ -848,8 +873,14 @@ const char* index_problem(const bg_bodies* B, const bg_rows* R, const std::vecto
 // page-locked column is copied straight from the caller's memory; the others are gathered by the
 // pool into the library's pinned block a group at a time, each group's copy to the device starting
 // as soon as it is gathered, while the next group is.  Returns with the copies in flight.
+int upload_plan(bg_ctx* c, const Plan& plan);
+
 int upload_columns(bg_ctx* c, const bg_bodies* B, const bg_rows* R, int nb, int nr, int na) {
-  Plan plan = plan_in(c, B, R, static_cast<size_t>(nb), static_cast<size_t>(nr), static_cast<size_t>(na), c->d_in);
+  return upload_plan(c, plan_in(c, B, R, static_cast<size_t>(nb), static_cast<size_t>(nr), static_cast<size_t>(na), c->d_in));
+}
+
+// The columns a plan lists, copied into the device block at their places (see upload_columns).
+int upload_plan(bg_ctx* c, const Plan& plan) {
   for (const Piece& pc : plan.pieces)
     if (pc.bytes > 0 && pc.from == nullptr) {
       set_error(c, "upload: column %s is NULL", pc.name);
@@ -976,6 +1007,7 @@ int order_rows(bg_ctx* c, const bg_bodies* B, const bg_rows* R, std::string& err
     }
     for (int m = w.starts[bg::OVERFLOW_RUN]; m < w.starts[bg::OVERFLOW_RUN + 1]; m++) c->chunks.push_back(make_int2(w.row0 + m, 1));
   }
+  c->nchunks = static_cast<int32_t>(c->chunks.size());
   // A batch's runs for the grid: every world's rows of one colour and one point count together
   // (rows of different worlds share no body), 32 a run, colour after colour; then each world's
   // overflow rows, one a run, in their order.  Each run's rows wait only on rows of earlier runs.
@@ -1128,7 +1160,7 @@ int launch_stage(bg_ctx* c, const bg_step* step) {
   p.R.rank_a = c->rank_dev;
   p.R.rank_b = c->rank_dev + c->nrows;
   p.chunks = c->chunks_dev;
-  p.nchunks = static_cast<int32_t>(c->chunks.size());
+  p.nchunks = c->nchunks;
   p.world_order = c->batch ? c->order_dev : nullptr;
   p.body_world = c->body_world_dev;
   p.nawake_total = c->nawake;
@@ -1327,6 +1359,11 @@ void bg_destroy(bg_ctx* c) {
   for (void* p : c->adj.allocs) cudaFree(p);
   c->adj.allocs.clear();
   if (c->nw.block) cudaFree(c->nw.block);
+  if (c->ct.block) cudaFree(c->ct.block);
+  if (c->ct.banks) cudaFree(c->ct.banks);
+  if (c->ct.summary) cudaFreeHost(c->ct.summary);
+  for (cudaEvent_t e : c->ct.ev)
+    if (e) cudaEventDestroy(e);
   if (c->col.block) cudaFree(c->col.block);
   if (c->col.begin) cudaEventDestroy(c->col.begin);
   if (c->col.end) cudaEventDestroy(c->col.end);
@@ -2836,6 +2873,58 @@ ColourLayout colour_layout(unsigned char* base, size_t nb, size_t n) {
   return L;
 }
 
+// The colouring's block, grown (by doubling) to hold nb slots and n manifolds.
+bool colour_block(bg_ctx* c, size_t nb, size_t n) {
+  bg_ctx::Colouring& d = c->col;
+  if (d.block != nullptr && nb <= d.bodies && n <= d.rows) return true;
+  cudaStreamSynchronize(c->stream);
+  if (d.block) cudaFree(d.block);
+  d.block = nullptr;
+  d.bodies = grown(d.bodies, nb);
+  d.rows = grown(d.rows, n);
+  void* block = nullptr;
+  if (cudaMalloc(&block, colour_layout(nullptr, d.bodies, d.rows).bytes) != cudaSuccess) {
+    cudaGetLastError();
+    d.bodies = d.rows = 0;
+    return false;
+  }
+  d.block = static_cast<unsigned char*>(block);
+  return true;
+}
+
+// colour() and arrange()'s order for p.n manifolds over p.nb slots, queued on the context's
+// stream (p's arrays zeroed as colour_layout() says; `tiles` holds kRuns * nb / kTile + 2).
+bool colour_kernels(bg_ctx* c, bgcol::ColourParams& p, int32_t* tiles) {
+  cudaStream_t st = c->stream;
+  const int64_t n = p.n, nb = p.nb;
+  const int rows_grid = std::max(1, std::min(static_cast<int>((n + 255) / 256), 8 * c->sms));
+  const int body_grid = std::max(1, std::min(static_cast<int>((nb + 255) / 256), 8 * c->sms));
+  const int bin_grid = std::max(1, std::min(static_cast<int>((bgcol::kRuns * nb + 255) / 256), 8 * c->sms));
+  bgcol::col_degrees<<<rows_grid, 256, 0, st>>>(p);
+  bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(p.deg, p.off, static_cast<int>(nb));
+  bgcol::col_fill<<<rows_grid, 256, 0, st>>>(p);
+  bgcol::col_ranks<<<body_grid, 256, 0, st>>>(p);
+  {
+    void* args[] = {&p};
+    if (!cuda_ok(c, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(bgcol::col_colour), dim3(c->sms), dim3(256),
+                                                args, 0, st), "col_colour launch"))
+      return false;
+  }
+  bgcol::col_bins<<<rows_grid, 256, 0, st>>>(p);
+  {
+    const int nbins = bgcol::kRuns * static_cast<int>(nb);
+    const int ntiles = (nbins + bgcol::kTile - 1) / bgcol::kTile;
+    bgcol::col_tile_sums<<<ntiles, bgcol::kScanThreads, 0, st>>>(p.bins, nbins, tiles);
+    bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(tiles, tiles, ntiles);
+    bgcol::col_tile_scan<<<ntiles, bgcol::kScanThreads, 0, st>>>(p.bins, p.bins, nbins, tiles);
+  }
+  bgcol::col_scatter<<<rows_grid, 256, 0, st>>>(p);
+  bgcol::col_settle<<<bin_grid, 256, 0, st>>>(p);
+  bgcol::col_starts<<<1, 64, 0, st>>>(p);
+  c->last_launches += 12;
+  return cuda_ok(c, cudaGetLastError(), "colour launch");
+}
+
 }  // namespace
 
 extern "C" {
@@ -2870,20 +2959,9 @@ int32_t bg_colour(bg_ctx* c, const bg_bodies* B, int32_t count, const int32_t* a
   for (int64_t x = 0; x < nb && !any_frozen; x++) any_frozen = B->frozen[x] != 0;
   cudaSetDevice(c->device);
   bg_ctx::Colouring& d = c->col;
-  if (d.block == nullptr || static_cast<size_t>(nb) > d.bodies || static_cast<size_t>(n) > d.rows) {
-    cudaStreamSynchronize(c->stream);
-    if (d.block) cudaFree(d.block);
-    d.block = nullptr;
-    d.bodies = grown(d.bodies, static_cast<size_t>(nb));
-    d.rows = grown(d.rows, static_cast<size_t>(n));
-    void* block = nullptr;
-    if (cudaMalloc(&block, colour_layout(nullptr, d.bodies, d.rows).bytes) != cudaSuccess) {
-      cudaGetLastError();
-      d.bodies = d.rows = 0;
-      set_error(c, "bg_colour: cudaMalloc failed");
-      return BG_ENOMEM;
-    }
-    d.block = static_cast<unsigned char*>(block);
+  if (!colour_block(c, static_cast<size_t>(nb), static_cast<size_t>(n))) {
+    set_error(c, "bg_colour: cudaMalloc failed");
+    return BG_ENOMEM;
   }
   if (d.begin == nullptr) {
     cudaEventCreate(&d.begin);
@@ -2904,34 +2982,10 @@ int32_t bg_colour(bg_ctx* c, const bg_bodies* B, int32_t count, const int32_t* a
   p.frozen = L.frozen; p.any_frozen = any_frozen; p.deg = L.deg; p.off = L.off; p.cursor = L.cursor; p.list = L.list;
   p.rank = L.rank; p.used = L.used; p.done = L.done; p.colour = L.colour; p.bins = L.bins; p.bincur = L.bincur;
   p.order = L.order; p.starts = L.starts; p.status = L.status; p.budget = c->budget;
-  const int rows_grid = std::max(1, std::min(static_cast<int>((n + 255) / 256), 8 * c->sms));
-  const int body_grid = std::max(1, std::min(static_cast<int>((nb + 255) / 256), 8 * c->sms));
-  const int bin_grid = std::max(1, std::min(static_cast<int>((bgcol::kRuns * nb + 255) / 256), 8 * c->sms));
   cudaEventRecord(d.begin, st);
-  bgcol::col_degrees<<<rows_grid, 256, 0, st>>>(p);
-  bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(L.deg, L.off, static_cast<int>(nb));
-  bgcol::col_fill<<<rows_grid, 256, 0, st>>>(p);
-  bgcol::col_ranks<<<body_grid, 256, 0, st>>>(p);
-  {
-    void* args[] = {&p};
-    if (!cuda_ok(c, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(bgcol::col_colour), dim3(c->sms), dim3(256),
-                                                args, 0, st), "col_colour launch"))
-      return BG_ECUDA;
-  }
-  bgcol::col_bins<<<rows_grid, 256, 0, st>>>(p);
-  {
-    const int nbins = bgcol::kRuns * static_cast<int>(nb);
-    const int tiles = (nbins + bgcol::kTile - 1) / bgcol::kTile;
-    bgcol::col_tile_sums<<<tiles, bgcol::kScanThreads, 0, st>>>(L.bins, nbins, L.tiles);
-    bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(L.tiles, L.tiles, tiles);
-    bgcol::col_tile_scan<<<tiles, bgcol::kScanThreads, 0, st>>>(L.bins, L.bins, nbins, L.tiles);
-  }
-  bgcol::col_scatter<<<rows_grid, 256, 0, st>>>(p);
-  bgcol::col_settle<<<bin_grid, 256, 0, st>>>(p);
-  bgcol::col_starts<<<1, 64, 0, st>>>(p);
+  if (!colour_kernels(c, p, L.tiles)) return BG_ECUDA;
   cudaEventRecord(d.end, st);
   d.timed = true;
-  c->last_launches += 12;
   if (!cuda_ok(c, cudaGetLastError(), "bg_colour launch")) return BG_ECUDA;
   int32_t status = 0;
   ok = cuda_ok(c, cudaMemcpyAsync(&status, L.status, sizeof status, cudaMemcpyDeviceToHost, st), "bg_colour") &&
@@ -2958,6 +3012,466 @@ double bg_last_colour_ms(bg_ctx* c) {
     return -1;
   }
   return ms;
+}
+
+}  // extern "C"
+
+// ---- a step's contacts on the device (bg_contact_step) -------------------------------------
+//
+// One call runs the step's contact pipeline on the context's stream: the narrowphase over the
+// pair list (bg_collide's kernels), the rows emitted and warm-started from the contact memory
+// (contact.cuh), colour() and arrange() (colour.cuh), the solve order and the grid's dataflow
+// tables (contact.cuh, what order_rows() works out on the host for bg_solve_step), the solve
+// stage, and store()/touched() into the other bank of contact memory.  The host waits on the
+// device twice: for the number of rows (the colouring's launch sizes), and for the colour starts
+// and the number of runs (the stage's launch parameters).
+
+namespace {
+
+// Where the pairs and the materials land in the upload block, after the bodies.
+struct ContactIn {
+  const int32_t *a = nullptr, *b = nullptr, *memory = nullptr;
+  const double *margin = nullptr, *tol = nullptr, *friction = nullptr, *restitution = nullptr, *size = nullptr;
+};
+
+Plan plan_contact_in(bg_ctx* c, const bg_bodies* B, const bg_materials* M, const bg_contact_pairs* CP, size_t nb,
+                     size_t np, size_t na, unsigned char* base, ContactIn& in) {
+  Plan P = plan_in(c, B, nullptr, nb, 0, na, base);
+  const bg_pairs* L = CP ? &CP->list : nullptr;
+  in.a = P.in<int32_t>(L ? L->a : nullptr, np, "pairs.a");
+  in.b = P.in<int32_t>(L ? L->b : nullptr, np, "pairs.b");
+  in.margin = P.in<double>(L ? L->margin : nullptr, np, "pairs.margin");
+  in.tol = P.in<double>(L ? L->tolerance : nullptr, np, "pairs.tolerance");
+  in.memory = P.in<int32_t>(CP ? CP->memory : nullptr, np, "pairs.memory");
+  in.friction = P.in<double>(M ? M->friction : nullptr, nb, "materials.friction");
+  in.restitution = P.in<double>(M ? M->restitution : nullptr, nb, "materials.restitution");
+  in.size = P.in<double>(M ? M->size : nullptr, nb, "materials.size");
+  return P;
+}
+
+// The call's scratch for nb slots and np pairs (so at most np rows), carved from `base` (NULL:
+// only measures).
+struct ContactLayout {
+  int32_t *counts, *corder;        // the narrowphase's class sort
+  uint8_t* points;                 // the manifolds, per pair
+  double *normal, *point, *separation;
+  uint32_t* pid;
+  int32_t *rowof, *scan_tiles;     // np + 1 found rows, and the scan's tile sums
+  bgct::FoundRows r;               // the rows in found order
+  int32_t *ocounts, *groups, *chunk_base;   // the solve order
+  int32_t *off, *cursor, *list;    // each body's solved rows (the dataflow's ranks)
+  uint8_t* touching;
+  int32_t* points_solved;
+  size_t bytes;
+};
+
+ContactLayout contact_layout(unsigned char* base, size_t nb, size_t np) {
+  Carve k{base};
+  ContactLayout L;
+  const size_t tiles = (np + bgct::kOrderThreads - 1) / bgct::kOrderThreads;
+  L.counts = k.take<int32_t>(2 * kPairClasses); L.corder = k.take<int32_t>(np);
+  L.points = k.take<uint8_t>(np); L.normal = k.take<double>(3 * np); L.point = k.take<double>(3 * bg::P * np);
+  L.separation = k.take<double>(bg::P * np); L.pid = k.take<uint32_t>(bg::P * np);
+  L.rowof = k.take<int32_t>(np + 1); L.scan_tiles = k.take<int32_t>(np / bgcol::kTile + 2);
+  bgct::FoundRows& r = L.r;
+  r.row = k.take<int32_t>(np); r.a = k.take<int32_t>(np); r.b = k.take<int32_t>(np); r.pair = k.take<int32_t>(np);
+  r.points = k.take<uint8_t>(np); r.pid = k.take<uint32_t>(bg::P * np);
+  r.normal = k.take<double>(3 * np); r.t1 = k.take<double>(3 * np); r.t2 = k.take<double>(3 * np);
+  r.friction = k.take<double>(np); r.restitution = k.take<double>(np); r.tolerance = k.take<double>(np);
+  r.patch = k.take<double>(np); r.separation = k.take<double>(bg::P * np); r.point = k.take<double>(3 * bg::P * np);
+  r.shift = k.take<double>(3 * bg::P * np); r.ni = k.take<double>(bg::P * np);
+  r.ti1 = k.take<double>(np); r.ti2 = k.take<double>(np); r.ri1 = k.take<double>(np); r.ri2 = k.take<double>(np);
+  r.si = k.take<double>(np); r.drift1 = k.take<double>(np); r.drift2 = k.take<double>(np);
+  r.maxni = k.take<double>(bg::P * np); r.relvel = k.take<double>(bg::P * np); r.gap = k.take<double>(np);
+  L.ocounts = k.take<int32_t>(bgct::kKeys * tiles + 1);
+  L.groups = k.take<int32_t>(bgct::kKeys + 1); L.chunk_base = k.take<int32_t>(bgct::kKeys + 1);
+  L.off = k.take<int32_t>(nb + 1); L.cursor = k.take<int32_t>(nb); L.list = k.take<int32_t>(2 * np);
+  L.touching = k.take<uint8_t>(np); L.points_solved = k.take<int32_t>(1);
+  L.bytes = k.end;
+  return L;
+}
+
+// One bank of contact memory for `cap` records, carved from `base` (NULL: only measures).
+bgct::Memory bank_at(unsigned char* base, size_t cap, size_t* bytes = nullptr) {
+  Carve k{base};
+  bgct::Memory m;
+  m.points = k.take<uint8_t>(cap); m.pid = k.take<uint32_t>(bg::P * cap); m.ni = k.take<double>(bg::P * cap);
+  m.friction = k.take<double>(3 * cap); m.twist = k.take<double>(3 * cap); m.slip = k.take<double>(3 * cap);
+  if (bytes) *bytes = k.end;
+  return m;
+}
+
+size_t bank_bytes(size_t cap) {
+  size_t n = 0;
+  bank_at(nullptr, cap, &n);
+  return n;
+}
+
+bgct::Memory bank(const bg_ctx::Contact& d, int which) {
+  return bank_at(d.banks + static_cast<size_t>(which) * bank_bytes(d.bank_cap), d.bank_cap);
+}
+
+// The scratch block and the banks, grown (by doubling) for nb slots and np pairs; a grown pair of
+// banks takes the last call's records with it.
+bool contact_blocks(bg_ctx* c, size_t nb, size_t np) {
+  bg_ctx::Contact& d = c->ct;
+  if (d.block == nullptr || nb > d.bodies || np > d.pairs) {
+    cudaStreamSynchronize(c->stream);
+    if (d.block) cudaFree(d.block);
+    d.block = nullptr;
+    d.bodies = grown(d.bodies, nb);
+    d.pairs = grown(d.pairs, np);
+    void* block = nullptr;
+    if (cudaMalloc(&block, contact_layout(nullptr, d.bodies, d.pairs).bytes) != cudaSuccess) {
+      cudaGetLastError();
+      d.bodies = d.pairs = 0;
+      set_error(c, "bg_contact_step: cudaMalloc failed");
+      return false;
+    }
+    d.block = static_cast<unsigned char*>(block);
+  }
+  if (d.banks == nullptr || np > d.bank_cap) {
+    const size_t cap = grown(d.bank_cap, np);
+    void* banks = nullptr;
+    if (cudaMalloc(&banks, 2 * bank_bytes(cap)) != cudaSuccess) {
+      cudaGetLastError();
+      set_error(c, "bg_contact_step: cudaMalloc failed");
+      return false;
+    }
+    bool ok = true;
+    if (d.banks != nullptr && d.count > 0) {
+      const bgct::Memory from = bank(d, d.current), to = bank_at(static_cast<unsigned char*>(banks), cap);
+      const size_t n = static_cast<size_t>(d.count);
+      auto copy = [&](void* dst, const void* src, size_t bytes) {
+        ok = ok && cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->stream) == cudaSuccess;
+      };
+      copy(to.points, from.points, n); copy(to.pid, from.pid, sizeof(uint32_t) * bg::P * n);
+      copy(to.ni, from.ni, sizeof(double) * bg::P * n); copy(to.friction, from.friction, sizeof(double) * 3 * n);
+      copy(to.twist, from.twist, sizeof(double) * 3 * n); copy(to.slip, from.slip, sizeof(double) * 3 * n);
+      ok = ok && cudaStreamSynchronize(c->stream) == cudaSuccess;
+    }
+    if (!ok) {
+      cudaGetLastError();
+      cudaFree(banks);
+      set_error(c, "bg_contact_step: the contact memory could not be moved");
+      return false;
+    }
+    if (d.banks) cudaFree(d.banks);
+    d.banks = static_cast<unsigned char*>(banks);
+    d.bank_cap = cap;
+    d.current = 0;
+  }
+  if (d.summary == nullptr) {
+    void* h = nullptr;
+    if (cudaHostAlloc(&h, 4096, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      set_error(c, "bg_contact_step: cudaHostAlloc failed");
+      return false;
+    }
+    d.summary = static_cast<int32_t*>(h);
+  }
+  if (d.ev[0] == nullptr)
+    for (cudaEvent_t& e : d.ev) cudaEventCreate(&e);
+  return true;
+}
+
+// Exclusive scan of in[0..n) into out[0..n] (out[n] the total) on the stream, across blocks.
+void scan_into(cudaStream_t st, const int32_t* in, int32_t* out, int n, int32_t* tiles) {
+  const int ntiles = (n + bgcol::kTile - 1) / bgcol::kTile;
+  bgcol::col_tile_sums<<<ntiles, bgcol::kScanThreads, 0, st>>>(in, n, tiles);
+  bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(tiles, tiles, ntiles);
+  bgcol::col_tile_scan<<<ntiles, bgcol::kScanThreads, 0, st>>>(in, out, n, tiles);
+}
+
+// What the host checks before anything is copied: every index a kernel addresses memory with.
+int contact_problem(bg_ctx* c, const bg_bodies* B, const bg_materials* M, const bg_contact_pairs* CP,
+                    const bg_step* step) {
+  if (B == nullptr || M == nullptr || CP == nullptr || step == nullptr) {
+    set_error(c, "bg_contact_step: bodies, materials, pairs, step or out is NULL");
+    return BG_EINVAL;
+  }
+  if (!(step->dt > 0) || step->substeps < 1) {
+    set_error(c, "step: dt must be positive and substeps at least 1");
+    return BG_EINVAL;
+  }
+  const int64_t nb = B->capacity, np = CP->list.count, na = B->awake_count;
+  if (nb < 0 || na < 0 || na > nb || np < 0) {
+    set_error(c, "bg_contact_step: negative or inconsistent counts");
+    return BG_EINVAL;
+  }
+  if (static_cast<int64_t>(bgcol::kRuns) * nb + 1 > INT32_MAX || 2 * np + 64 > INT32_MAX) {
+    set_error(c, "bg_contact_step: too many slots or pairs");
+    return BG_EINVAL;
+  }
+  if (np > 0 && (CP->list.a == nullptr || CP->list.b == nullptr || CP->list.margin == nullptr ||
+                 CP->list.tolerance == nullptr || CP->memory == nullptr)) {
+    set_error(c, "bg_contact_step: a pair column is NULL");
+    return BG_EINVAL;
+  }
+  if (nb > 0 && (B->shape == nullptr || B->frozen == nullptr || B->inv_mass == nullptr)) {
+    set_error(c, "bg_contact_step: bodies.shape, frozen and inv_mass must be given");
+    return BG_EINVAL;
+  }
+  if (na > 0 && B->awake_list == nullptr) {
+    set_error(c, "bg_contact_step: bodies.awake_list must be given");
+    return BG_EINVAL;
+  }
+  const int32_t records = c->ct.count;
+  for (int64_t i = 0; i < np; i++) {
+    const int32_t a = CP->list.a[i], b = CP->list.b[i], j = CP->memory[i];
+    if (a < 0 || a >= nb || b < 0 || b >= nb || a == b) {
+      set_error(c, "bg_contact_step: pair %lld has slots %d, %d of %lld", static_cast<long long>(i), a, b,
+                static_cast<long long>(nb));
+      return BG_EINVAL;
+    }
+    for (const int32_t s : {a, b})
+      if (B->shape[s] != BG_BOX && B->shape[s] != BG_SPHERE && B->shape[s] != BG_CAPSULE) {
+        set_error(c, "bg_contact_step: slot %d is not a box, sphere or capsule", s);
+        return BG_EUNSUPPORTED;
+      }
+    if (j < -1 || j >= records) {
+      set_error(c, "bg_contact_step: pair %lld names contact record %d of %d", static_cast<long long>(i), j, records);
+      return BG_EINVAL;
+    }
+  }
+  for (int64_t i = 0; i < na; i++)
+    if (static_cast<uint32_t>(B->awake_list[i]) >= static_cast<uint32_t>(nb)) {
+      set_error(c, "bg_contact_step: bodies.awake_list entry %lld is not one of the %lld slots", static_cast<long long>(i),
+                static_cast<long long>(nb));
+      return BG_EINVAL;
+    }
+  return BG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t bg_contact_step(bg_ctx* c, const bg_bodies* B, const bg_materials* M, const bg_contact_pairs* CP,
+                        const bg_step* step, bg_contact_result* out) {
+  if (c == nullptr) return BG_EINVAL;
+  if (out == nullptr) {
+    set_error(c, "bg_contact_step: out is NULL");
+    return BG_EINVAL;
+  }
+  int rc = contact_problem(c, B, M, CP, step);
+  if (rc != BG_OK) return rc;
+  const int nb = B->capacity, np = CP->list.count, na = B->awake_count;
+  int32_t any_frozen = 0;
+  for (int x = 0; x < nb && !any_frozen; x++) any_frozen = B->frozen[x] != 0;
+  cudaSetDevice(c->device);
+  c->last_launches = 0;
+  c->uploaded = false;
+  bg_ctx::Contact& d = c->ct;
+  ContactIn in;
+  const size_t in_need = plan_contact_in(c, nullptr, nullptr, nullptr, static_cast<size_t>(nb), static_cast<size_t>(np),
+                                         static_cast<size_t>(na), nullptr, in).end;
+  if (!ensure(c, nb, std::max(np, 1), na, 1, 0, in_need)) return BG_ENOMEM;
+  if (!contact_blocks(c, static_cast<size_t>(nb), static_cast<size_t>(np))) return BG_ENOMEM;
+  const ContactLayout L = contact_layout(d.block, static_cast<size_t>(nb), static_cast<size_t>(np));
+  const bgct::Memory old = bank(d, d.current), next = bank(d, 1 - d.current);
+  c->nbodies = nb;
+  c->nawake = na;
+  c->nworlds = 1;
+  c->batch = false;
+  rc = upload_plan(c, plan_contact_in(c, B, M, CP, static_cast<size_t>(nb), static_cast<size_t>(np),
+                                      static_cast<size_t>(na), c->d_in, in));
+  if (rc != BG_OK) return rc;
+  cudaStream_t st = c->stream;
+  int32_t* sum = d.summary;
+  auto fetch = [&](void* dst, const void* src, size_t bytes, const char* what) {
+    return cuda_ok(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st), what);
+  };
+  const int sweep = std::max(1, std::min((np + 255) / 256, 8 * c->sms));
+  // the narrowphase, as bg_collide runs it, on the uploaded bodies and pairs
+  cudaEventRecord(d.ev[0], st);
+  if (np > 0) {
+    if (!cuda_ok(c, cudaMemsetAsync(L.counts, 0, 2 * kPairClasses * sizeof(int32_t), st), "bg_contact_step")) return BG_ECUDA;
+    CollideParams k;
+    k.p = c->bin.position; k.q = c->bin.rotation; k.dims = c->bin.dims; k.gscale = c->bin.gravity_scale;
+    k.shape = c->bin.shape; k.type = c->bin.type;
+    k.a = in.a; k.b = in.b; k.margin = in.margin; k.tol = in.tol; k.n = np;
+    for (int e = 0; e < 3; e++) k.gravity[e] = step->gravity[e];
+    k.counts = L.counts; k.order = L.corder; k.points = L.points; k.normal = L.normal; k.point = L.point;
+    k.separation = L.separation; k.pid = L.pid;
+    collide_count<<<sweep, 256, 0, st>>>(k);
+    collide_starts<<<1, 32, 0, st>>>(k);
+    collide_scatter<<<sweep, 256, 0, st>>>(k);
+    const int blocks = std::min((np + kCollideThreads - 1) / kCollideThreads, 64 * c->sms);
+    collide_pairs<<<blocks, kCollideThreads, 0, st>>>(k);
+    c->last_launches += 4;
+  }
+  cudaEventRecord(d.ev[1], st);
+  // the rows: which pairs touch, and their found rows (the host waits for the count)
+  bgct::EmitParams e;
+  e.np = np; e.a = in.a; e.b = in.b; e.tol = in.tol; e.memory = in.memory;
+  e.points = L.points; e.normal = L.normal; e.point = L.point; e.separation = L.separation; e.pid = L.pid;
+  e.friction = in.friction; e.restitution = in.restitution; e.size = in.size; e.type = c->bin.type;
+  e.rowof = L.rowof; e.old = old; e.r = L.r;
+  int nrows = 0;
+  if (np > 0) {
+    bgct::ct_flags<<<sweep, 256, 0, st>>>(e);
+    scan_into(st, L.rowof, L.rowof, np, L.scan_tiles);
+    c->last_launches += 4;
+    if (!fetch(sum, L.rowof + np, sizeof(int32_t), "bg_contact_step") ||
+        !cuda_ok(c, cudaStreamSynchronize(st), "bg_contact_step"))
+      return BG_ECUDA;
+    nrows = sum[0];
+  }
+  c->nrows = nrows;
+  int32_t starts[bg::NSTARTS] = {0};
+  int32_t nchunks = 0;
+  if (nrows > 0) {
+    const int rgrid = std::max(1, std::min((nrows + 255) / 256, 8 * c->sms));
+    bgct::ct_emit<<<sweep, 256, 0, st>>>(e);
+    // colour() and arrange()'s order, on the found rows
+    if (!colour_block(c, static_cast<size_t>(nb), static_cast<size_t>(nrows))) {
+      set_error(c, "bg_contact_step: cudaMalloc failed");
+      return BG_ENOMEM;
+    }
+    const ColourLayout CL = colour_layout(c->col.block, static_cast<size_t>(nb), static_cast<size_t>(nrows));
+    const size_t zero = reinterpret_cast<unsigned char*>(CL.off) - reinterpret_cast<unsigned char*>(CL.deg);
+    if (!cuda_ok(c, cudaMemsetAsync(CL.deg, 0, zero, st), "bg_contact_step")) return BG_ECUDA;
+    bgcol::ColourParams p;
+    p.n = nrows; p.nb = nb; p.a = L.r.a; p.b = L.r.b; p.type = c->bin.type; p.frozen = c->bin.frozen;
+    p.any_frozen = any_frozen; p.deg = CL.deg; p.off = CL.off; p.cursor = CL.cursor; p.list = CL.list;
+    p.rank = CL.rank; p.used = CL.used; p.done = CL.done; p.colour = CL.colour; p.bins = CL.bins;
+    p.bincur = CL.bincur; p.order = CL.order; p.starts = CL.starts; p.status = CL.status; p.budget = c->budget;
+    if (!colour_kernels(c, p, CL.tiles)) return BG_ECUDA;
+    bgct::ct_rest<<<rgrid, 256, 0, st>>>(L.r, CL.colour, nrows);
+    // the solve order and its runs
+    bgct::OrderParams op;
+    op.n = nrows; op.tiles = (nrows + bgct::kOrderThreads - 1) / bgct::kOrderThreads;
+    op.order = CL.order; op.colour = CL.colour; op.points = L.r.points; op.counts = L.ocounts;
+    op.perm = c->perm_dev; op.iperm = c->iperm_dev; op.groups = L.groups; op.chunks = c->chunks_dev;
+    op.chunk_base = L.chunk_base;
+    bgct::ct_order_count<<<op.tiles, bgct::kOrderThreads, 0, st>>>(op);
+    bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(L.ocounts, L.ocounts, bgct::kKeys * op.tiles);
+    bgct::ct_order_place<<<op.tiles, bgct::kOrderThreads, 0, st>>>(op);
+    bgct::ct_order_runs<<<1, 32, 0, st>>>(op);
+    bgct::ct_order_chunks<<<rgrid, 256, 0, st>>>(op);
+    c->last_launches += 7;
+    if (!cuda_ok(c, cudaGetLastError(), "bg_contact_step launch")) return BG_ECUDA;
+    // the host waits for what the stage's launch needs
+    if (!fetch(sum, CL.starts, sizeof(int32_t) * bg::NSTARTS, "bg_contact_step") ||
+        !fetch(sum + 64, L.chunk_base + bgct::kKeys, sizeof(int32_t), "bg_contact_step") ||
+        !fetch(sum + 65, CL.status, sizeof(int32_t), "bg_contact_step") ||
+        !cuda_ok(c, cudaStreamSynchronize(st), "bg_contact_step"))
+      return BG_ECUDA;
+    if (sum[65] != 0) {
+      set_error(c, "bg_contact_step: a colouring wait ran past its budget; the step is lost");
+      return BG_ETIMEOUT;
+    }
+    for (int k = 0; k < bg::NSTARTS; k++) starts[k] = sum[k];
+    nchunks = sum[64];
+  }
+  const int solved = starts[bg::RESTING_RUN];
+  // the world the stage solves, and the grid's dataflow tables
+  bg::WorldDesc w = {};
+  w.body0 = 0; w.nbodies = nb; w.awake0 = 0; w.nawake = na; w.row0 = 0; w.nrows = nrows; w.solved = solved;
+  for (int k = 0; k < bg::NSTARTS; k++) w.starts[k] = starts[k];
+  for (int k = 0; k < 3; k++) w.gravity[k] = step->gravity[k];
+  c->worlds.assign(1, w);
+  {
+    std::vector<int32_t> bo = {0, nb}, ao = {0, na}, ro = {0, nrows};
+    rc = upload_worlds(c, bo, ao, ro);
+    if (rc != BG_OK) return rc;
+  }
+  const size_t nb4 = sizeof(int32_t) * static_cast<size_t>(std::max(nb, 1));
+  if (!cuda_ok(c, cudaMemsetAsync(c->deg_dev, 0, nb4, st), "bg_contact_step") ||
+      !cuda_ok(c, cudaMemsetAsync(L.cursor, 0, nb4, st), "bg_contact_step") ||
+      !cuda_ok(c, cudaMemsetAsync(c->body_world_dev, 0, nb4, st), "bg_contact_step"))
+    return BG_ECUDA;
+  if (nrows > 0) {
+    bgct::FlowParams f;
+    f.solved = solved; f.nrows = nrows; f.nb = nb; f.perm = c->perm_dev; f.a = L.r.a; f.b = L.r.b;
+    f.inv_mass = c->bin.inv_mass; f.deg = c->deg_dev; f.off = L.off; f.cursor = L.cursor; f.list = L.list;
+    f.rank = c->rank_dev;
+    const int rgrid = std::max(1, std::min((nrows + 255) / 256, 8 * c->sms));
+    const int bgrid = std::max(1, std::min((nb + 255) / 256, 8 * c->sms));
+    bgct::ct_flow_degrees<<<rgrid, 256, 0, st>>>(f);
+    bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(c->deg_dev, L.off, nb);
+    bgct::ct_flow_fill<<<rgrid, 256, 0, st>>>(f);
+    bgct::ct_flow_ranks<<<bgrid, 256, 0, st>>>(f);
+    c->last_launches += 4;
+  }
+  c->nchunks = nchunks;
+  c->chunks.clear();
+  c->bruns.clear();
+  c->brun_rows.clear();
+  // the found rows in the caller's row layout are what the stage's unpack reads
+  RowStage& q = c->rin;
+  q.row = L.r.row; q.a = L.r.a; q.b = L.r.b; q.points = L.r.points; q.normal = L.r.normal; q.t1 = L.r.t1;
+  q.t2 = L.r.t2; q.friction = L.r.friction; q.restitution = L.r.restitution; q.tolerance = L.r.tolerance;
+  q.patch = L.r.patch; q.separation = L.r.separation; q.point = L.r.point; q.shift = L.r.shift;
+  q.normal_impulse = L.r.ni; q.ti1 = L.r.ti1; q.ti2 = L.r.ti2; q.ri1 = L.r.ri1; q.ri2 = L.r.ri2; q.si = L.r.si;
+  q.drift1 = L.r.drift1; q.drift2 = L.r.drift2;
+  c->maxni_in = L.r.maxni;
+  c->relvel_in = L.r.relvel;
+  c->gap_in = L.r.gap;
+  c->uploaded = true;
+  rc = unpack(c);
+  if (rc != BG_OK) return rc;
+  rc = launch_stage(c, step);
+  if (rc != BG_OK) return rc;
+  // store() and touched(), into the other bank
+  if (!cuda_ok(c, cudaMemsetAsync(L.points_solved, 0, sizeof(int32_t), st), "bg_contact_step")) return BG_ECUDA;
+  if (np > 0) {
+    bgct::KeepParams kp;
+    kp.np = np; kp.solved = solved; kp.points = L.points; kp.rowof = L.rowof; kp.memory = in.memory;
+    kp.iperm = c->iperm_dev; kp.pid = L.r.pid; kp.R = c->R; kp.old = old; kp.next = next; kp.touching = L.touching;
+    kp.points_solved = L.points_solved;
+    bgct::ct_keep<<<sweep, 256, 0, st>>>(kp);
+    c->last_launches += 1;
+  }
+  cudaEventRecord(d.ev[3], st);
+  // the bodies back, with each pair's count and flag
+  plan_out(c, nullptr, nullptr, static_cast<size_t>(nb), 0, c->d_out);
+  {
+    const int blocks = std::max(1, std::min(4 * c->sms, (nb + kUnpackThreads - 1) / kUnpackThreads));
+    pack_bodies<<<blocks, kUnpackThreads, 0, st>>>(c->B, c->bout, nb);
+    c->last_launches += 1;
+  }
+  if (!cuda_ok(c, cudaGetLastError(), "bg_contact_step launch")) return BG_ECUDA;
+  if (!fetch(sum + 66, L.points_solved, sizeof(int32_t), "bg_contact_step")) return BG_ECUDA;
+  rc = download_columns(c, B, nullptr);
+  if (rc != BG_OK) return rc;
+  if (np > 0 && ((out->points != nullptr && !fetch(out->points, L.points, static_cast<size_t>(np), "bg_contact_step")) ||
+                 (out->touching != nullptr && !fetch(out->touching, L.touching, static_cast<size_t>(np), "bg_contact_step")) ||
+                 !cuda_ok(c, cudaStreamSynchronize(st), "bg_contact_step")))
+    return BG_ECUDA;
+  // the records the next call reads are this call's
+  d.current = 1 - d.current;
+  d.count = np;
+  d.timed = true;
+  out->rows = nrows;
+  out->solved = solved;
+  out->points_solved = sum[66];
+  for (int k = 0; k < bg::NSTARTS; k++) out->starts[k] = starts[k];
+  return BG_OK;
+}
+
+int32_t bg_last_contact_ms(bg_ctx* c, double* ms) {
+  if (c == nullptr || ms == nullptr || !c->ct.timed) return BG_EINVAL;
+  const bg_ctx::Contact& d = c->ct;
+  float t[4] = {0, 0, 0, 0};
+  if (cudaEventSynchronize(d.ev[3]) != cudaSuccess || cudaEventElapsedTime(&t[0], d.ev[0], d.ev[1]) != cudaSuccess ||
+      cudaEventElapsedTime(&t[1], d.ev[1], c->stage_begin) != cudaSuccess ||
+      cudaEventElapsedTime(&t[2], c->stage_begin, c->stage_end) != cudaSuccess ||
+      cudaEventElapsedTime(&t[3], c->stage_end, d.ev[3]) != cudaSuccess) {
+    cudaGetLastError();
+    return BG_ECUDA;
+  }
+  for (int k = 0; k < 4; k++) ms[k] = t[k];
+  return BG_OK;
+}
+
+int32_t bg_contact_records(const bg_ctx* c) { return c == nullptr ? BG_EINVAL : c->ct.count; }
+
+int32_t bg_contact_forget(bg_ctx* c) {
+  if (c == nullptr) return BG_EINVAL;
+  c->ct.count = 0;
+  return BG_OK;
 }
 
 }  // extern "C"

@@ -121,6 +121,9 @@ struct Pairs {
   std::vector<uint8_t> points, touching;
   std::vector<uint32_t> pid;
   std::vector<double> normalImpulse, friction, slip, twist;
+  // with the contact step on another device (bw_set_contact_step): where the pair's memory is, its
+  // index in the last list handed over, or -1 (nothing remembered)
+  std::vector<int32_t> record;
   std::unordered_map<uint64_t, int32_t> index;
 
   static uint64_t key(int x, int y) { return (static_cast<uint64_t>(x) << 32) | static_cast<uint32_t>(y); }
@@ -129,7 +132,7 @@ struct Pairs {
     if (a.size() >= c) return;
     size_t cap = a.size() > 16 ? a.size() : 16;
     while (cap < c) cap *= 2;
-    a.resize(cap); b.resize(cap); points.resize(cap); touching.resize(cap);
+    a.resize(cap); b.resize(cap); points.resize(cap); touching.resize(cap); record.resize(cap, -1);
     pid.resize(P * cap); normalImpulse.resize(P * cap);
     friction.resize(3 * cap); slip.resize(3 * cap); twist.resize(3 * cap);
   }
@@ -140,13 +143,14 @@ struct Pairs {
     if (index.count(key(lo, hi))) return;
     const int p = count;
     reserve(p + 1);
-    a[p] = lo; b[p] = hi; points[p] = 0; touching[p] = 0;
+    a[p] = lo; b[p] = hi; points[p] = 0; touching[p] = 0; record[p] = -1;
     index[key(lo, hi)] = p;
     count++;
     active = count;
   }
   void moveTo(int from, int to) {
     a[to] = a[from]; b[to] = b[from]; points[to] = points[from]; touching[to] = touching[from];
+    record[to] = record[from];
     for (int k = 0; k < P; k++) { pid[P * to + k] = pid[P * from + k]; normalImpulse[P * to + k] = normalImpulse[P * from + k]; }
     for (int k = 0; k < 3; k++) {
       friction[3 * to + k] = friction[3 * from + k];
@@ -166,6 +170,7 @@ struct Pairs {
   void forget(int p) {
     points[p] = 0;
     touching[p] = 0;
+    record[p] = -1;
   }
 };
 
@@ -264,6 +269,11 @@ struct bw_world {
   std::vector<uint32_t> nmPid;
   std::vector<double> nmNormal, nmPoint, nmSeparation;
   std::vector<int32_t> nmPair;
+  // the whole contact side of the step on another device (bw_set_contact_step), or none
+  bw_contact_solver contactFn = nullptr;
+  void* contactUser = nullptr;
+  std::vector<int32_t> nmRecord;
+  std::vector<uint8_t> nmTouching;
   bool begun = false;
   bw_stats stats = {};
 
@@ -543,8 +553,10 @@ struct bw_world {
   // manifolds; the second emits and carries the pairs that touch and forgets the others, in pair
   // order.  No decision of the first pass depends on a manifold, so the rows, their order and the
   // pairs' memory are the one-pass walk's.
-  int narrowOnDevice() {
-    narrowA.clear(); narrowB.clear(); narrowMargin.clear(); narrowTol.clear(); nmPair.clear();
+  // The first pass: the list of pairs whose boxes meet, each with its slot, margin, tolerance and
+  // contact record (nmRecord, for bw_set_contact_step).
+  void listPairs() {
+    narrowA.clear(); narrowB.clear(); narrowMargin.clear(); narrowTol.clear(); nmPair.clear(); nmRecord.clear();
     for (int p = 0; p < pairs.active;) {
       const int a = pairs.a[p], b = pairs.b[p];
       if (!fatOverlap(a, b)) {
@@ -558,10 +570,14 @@ struct bw_world {
         pairs.forget(p);
       } else {
         narrowA.push_back(a); narrowB.push_back(b); narrowMargin.push_back(motion[a] + motion[b] + tol);
-        narrowTol.push_back(tol); nmPair.push_back(p);
+        narrowTol.push_back(tol); nmPair.push_back(p); nmRecord.push_back(pairs.record[p]);
       }
       p++;
     }
+  }
+
+  int narrowOnDevice() {
+    listPairs();
     const size_t n = narrowA.size();
     nmPoints.resize(std::max<size_t>(n, 1)); nmPid.resize(P * std::max<size_t>(n, 1));
     nmNormal.resize(3 * std::max<size_t>(n, 1)); nmPoint.resize(3 * P * std::max<size_t>(n, 1));
@@ -716,6 +732,81 @@ struct bw_world {
       memory[10 + k] = pairs.slip[3 * p + k];
     }
     memory[13] = memory[14] = memory[15] = 0;
+  }
+
+  // The end of a step: transforms (src/world.js:1040-1057) and the step's stats.
+  void finish(int rows, int solved, int points, const int32_t* starts) {
+    for (int i = 0; i < awakeCount; i++) {
+      const int s = awakeList[i], t7 = 7 * s;
+      if (frozen[s] == 1) continue;
+      for (int k = 0; k < 3; k++) transforms[t7 + k] = static_cast<float>(position[3 * s + k]);
+      for (int k = 0; k < 4; k++) transforms[t7 + 3 + k] = static_cast<float>(rotation[4 * s + k]);
+    }
+    bw_stats& st = stats;
+    st.bodies = n;
+    st.awake = awakeCount;
+    st.pairs = pairs.count;
+    st.rows = rows;
+    st.solved = solved;
+    st.points = points;
+    int colours = 0;
+    for (int k = 0; k < COLOURS; k++) if (starts[k + 1] > starts[k]) colours++;
+    st.colours = colours;
+    st.overflow = rows > 0 ? starts[OVERFLOW_ + 1] - starts[OVERFLOW_] : 0;
+    st.step = stepCount;
+    stepDt = 0;
+  }
+
+  // A step with its contact side on another device (bw_set_contact_step): the host's share of
+  // narrow() (src/contact.js:312-327: the pair list's upkeep), then everything from the narrowphase
+  // to store() in one call, then the pairs reported apart forgotten and the touching flags kept.
+  int32_t contactStep(double dt) {
+    if (!(dt > 0) || !std::isfinite(dt)) {
+      error = "step: dt must be a positive number of seconds";
+      return BG_EINVAL;
+    }
+    stepCount++;
+    stepDt = dt;
+    const double gl = std::sqrt(gravity[0] * gravity[0] + gravity[1] * gravity[1] + gravity[2] * gravity[2]);
+    for (int i = 0; i < awakeCount; i++) boundsOf(awakeList[i], dt, gl);
+    broadphase(dt);
+    c.count = 0;
+    c.solved = 0;
+    std::fill(c.starts, c.starts + COLOURS + 3, 0);
+    listPairs();
+    const size_t np = narrowA.size();
+    nmPoints.assign(std::max<size_t>(np, 1), 0);
+    nmTouching.assign(std::max<size_t>(np, 1), 0);
+    bg_bodies B;
+    fillBodies(&B);
+    const bg_materials M = {friction.data(), restitution.data(), size.data()};
+    const bg_contact_pairs CP = {{static_cast<int32_t>(np), narrowA.data(), narrowB.data(), narrowMargin.data(),
+                                  narrowTol.data()},
+                                 nmRecord.data()};
+    bg_step S;
+    S.dt = dt;
+    S.substeps = substeps;
+    for (int k = 0; k < 3; k++) S.gravity[k] = gravity[k];
+    bg_contact_result R = {};
+    R.points = nmPoints.data();
+    R.touching = nmTouching.data();
+    const int32_t rc = contactFn(contactUser, &B, &M, &CP, &S, &R);
+    if (rc != BG_OK) {
+      error = "step: the contact step failed";
+      stepDt = 0;
+      return rc;
+    }
+    for (size_t i = 0; i < np; i++) {
+      const int p = nmPair[i];
+      if (nmPoints[i] == 0) {
+        pairs.forget(p);
+        continue;
+      }
+      pairs.record[p] = static_cast<int32_t>(i);
+      pairs.touching[p] = nmTouching[i];
+    }
+    finish(R.rows, R.solved, R.points_solved, R.starts);
+    return BG_OK;
   }
 
   void fillBodies(bg_bodies* B) {
@@ -873,8 +964,23 @@ int32_t bw_set_solver(bw_world* w, bw_solver solver, void* user) {
   return BG_OK;
 }
 
+int32_t bw_set_contact_step(bw_world* w, bw_contact_solver fn, void* user) {
+  if (w == nullptr) return BG_EINVAL;
+  if (w->stepCount > 0) {
+    w->error = "set_contact_step: the contact memory would be lost; set it before the first step";
+    return BG_EINVAL;
+  }
+  w->contactFn = fn;
+  w->contactUser = user;
+  return BG_OK;
+}
+
 int32_t bw_begin_step(bw_world* w, double dt) {
   if (w == nullptr) return BG_EINVAL;
+  if (w->contactFn != nullptr) {
+    w->error = "begin_step: the world's rows live on the contact step's device (bw_set_contact_step)";
+    return BG_EUNSUPPORTED;
+  }
   if (!(dt > 0) || !std::isfinite(dt)) {
     w->error = "step: dt must be a positive number of seconds";
     return BG_EINVAL;
@@ -923,29 +1029,9 @@ int32_t bw_end_step(bw_world* w) {
     for (int k = 0; k < c.points[m] && !meets; k++) meets = c.maxNormalImpulse[m * P + k] > 0;
     w->pairs.touching[c.pair[m]] = meets ? 1 : 0;
   }
-  // transforms: src/world.js:1040-1057.
-  for (int i = 0; i < w->awakeCount; i++) {
-    const int s = w->awakeList[i], t7 = 7 * s;
-    if (w->frozen[s] == 1) continue;
-    for (int k = 0; k < 3; k++) w->transforms[t7 + k] = static_cast<float>(w->position[3 * s + k]);
-    for (int k = 0; k < 4; k++) w->transforms[t7 + 3 + k] = static_cast<float>(w->rotation[4 * s + k]);
-  }
-  // stats
-  bw_stats& st = w->stats;
-  st.bodies = w->n;
-  st.awake = w->awakeCount;
-  st.pairs = w->pairs.count;
-  st.rows = c.count;
-  st.solved = c.solved;
   int pts = 0;
   for (int m = 0; m < c.solved; m++) pts += c.points[m];
-  st.points = pts;
-  int colours = 0;
-  for (int k = 0; k < COLOURS; k++) if (c.starts[k + 1] > c.starts[k]) colours++;
-  st.colours = colours;
-  st.overflow = c.count > 0 ? c.starts[OVERFLOW_ + 1] - c.starts[OVERFLOW_] : 0;
-  st.step = w->stepCount;
-  w->stepDt = 0;
+  w->finish(c.count, c.solved, pts, c.starts);
   return BG_OK;
 }
 
@@ -1090,6 +1176,7 @@ int32_t bw_step_params(const bw_world* w, bg_step* out) {
 
 int32_t bw_step(bw_world* w, double dt) {
   if (w == nullptr) return BG_EINVAL;
+  if (w->contactFn != nullptr) return w->contactStep(dt);
   if (w->solver == nullptr) {
     w->error = "step: no solve stage set (bw_set_solver)";
     return BG_EUNSUPPORTED;

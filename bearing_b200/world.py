@@ -48,6 +48,15 @@ class GpuSolver:
         self.user = self.ctx
         # bw_narrowphase takes (user, bodies, gravity, pairs, out), bg_collide (ctx, ...) alike.
         self.collide_fn = C.cast(self.lib.bg_collide, C.c_void_p).value
+        # bw_contact_solver and bg_contact_step alike.
+        self.contact_fn = C.cast(self.lib.bg_contact_step, C.c_void_p).value
+
+    def contact_ms(self):
+        """The last bg_contact_step's device times in ms: narrowphase, rows/colours/order, stage, store."""
+        ms = (C.c_double * 4)()
+        if self.lib.bg_last_contact_ms(self.ctx, ms) != 0:
+            return None
+        return list(ms)
 
     def error(self) -> str:
         return self.lib.bg_last_error(self.ctx).decode()
@@ -87,6 +96,7 @@ class World:
         self._solver = None
         self._solver_keep = None
         self._narrowphase = None
+        self._contact = None
         if solver is None:
             solver = GpuSolver()
         self.set_solver(solver)
@@ -102,6 +112,16 @@ class World:
         if self._lib.bw_set_narrowphase(self._w, fn, user) != 0:
             raise BearingError("set_narrowphase failed")
         self._narrowphase = device
+
+    def set_contact_step(self, device):
+        """device: a GpuSolver, whose context then runs each step's whole contact side, from the
+        narrowphase to store() (bg_contact_step); the rows stay on the device, so contacts() and
+        begin_step() are not available.  Set it before the first step."""
+        if not isinstance(device, GpuSolver):
+            raise BearingError("set_contact_step takes a GpuSolver")
+        if self._lib.bw_set_contact_step(self._w, C.c_void_p(device.contact_fn), C.c_void_p(device.ctx)) != 0:
+            raise BearingError(self._error())
+        self._contact = device
 
     # -- the solve stage ---------------------------------------------------------------------
     def set_solver(self, solver):
@@ -162,7 +182,9 @@ class World:
         rc = self._lib.bw_step(self._w, float(dt))
         if rc != 0:
             extra = ""
-            if isinstance(self._solver, GpuSolver):
+            if self._contact is not None:
+                extra = f" ({self._contact.error()})"
+            elif isinstance(self._solver, GpuSolver):
                 extra = f" ({self._solver.error()})"
             raise BearingError(f"step failed ({rc}): {self._error()}{extra}")
 

@@ -56,6 +56,7 @@ def parse():
     p.add_argument("--adjoint-worlds", type=int, default=1024, help="towers in the backward-pass measurement")
     p.add_argument("--adjoint-steps", type=int, default=120)
     p.add_argument("--no-adjoint", action="store_true", help="skip the backward-pass measurement")
+    p.add_argument("--no-contact", action="store_true", help="skip the device contact-step measurement")
     p.add_argument("--save-input", default=None, help="write the timed solve stage's input to this .npz")
     p.add_argument("--load-input", default=None,
                    help="time the solve stage of an input written by --save-input instead of building the pile "
@@ -602,6 +603,81 @@ def measure_colouring(lib, ctx, copy, steps, warmup, log):
             "same_as_the_step": same}
 
 
+def measure_contact_step(args, lib, solver, world, device, steps, warmup, log):
+    """A World step with its whole contact side on the device (bg_contact_step: narrowphase, rows,
+    warm start, colouring, order, solve stage and store, the rows never on the host) against the same
+    World step on the host path (the host's emit, carry, colour and keep around bg_collide and
+    bg_solve_step), at the same steps of the same pile.  A second world is built in contact mode and
+    stepped to the headline step; `world` (the headline's, begun at that step) finishes its step with
+    bg_solve_step; both then take the same timed steps, their row counts compared at each."""
+    from bearing_b200 import _ffi, scenes
+    from bearing_b200.world import GpuSolver, World
+    B, R, S = world.views()
+    assert lib.bg_solve_step(solver.ctx, C.byref(B), C.byref(R), C.byref(S)) == 0
+    world.end_step()
+    dev = GpuSolver(device)
+    wb = World({}, solver=dev)
+    calls = []
+    proto = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(_ffi.Bodies), C.POINTER(_ffi.Materials),
+                        C.POINTER(_ffi.ContactPairs), C.POINTER(_ffi.Step), C.POINTER(_ffi.ContactResult))
+
+    def timed(user, bodies, materials, pairs, step, out):   # bg_contact_step, timed on the host clock
+        t0 = time.perf_counter()
+        rc = lib.bg_contact_step(user, bodies, materials, pairs, step, out)
+        calls.append(((time.perf_counter() - t0) * 1000, pairs.contents.list.count, bodies.contents.capacity,
+                      out.contents.rows))
+        return rc
+    hook = proto(timed)
+    assert wb._lib.bw_set_contact_step(wb._w, C.cast(hook, C.c_void_p), C.c_void_p(dev.ctx)) == 0
+    scenes.pile(wb, count=args.bodies, seed=50_000)
+    t0 = time.time()
+    for _ in range(args.at + 1):
+        wb.step(DT)
+    if log:
+        log(f"contact-mode pile stepped to {args.at + 1} in {time.time() - t0:.0f} s: {wb.stats()}")
+    same = wb.stats() == world.stats()
+    host_ms, dev_ms, call_ms, parts = [], [], [], []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        world.step(DT)
+        t1 = time.perf_counter()
+        wb.step(DT)
+        t2 = time.perf_counter()
+        same = same and wb.stats() == world.stats()
+        if i >= warmup:
+            host_ms.append((t1 - t0) * 1000)
+            dev_ms.append((t2 - t1) * 1000)
+            call_ms.append(calls[-1][0])
+            parts.append(dev.contact_ms())
+    np_, nb, rows = calls[-1][1], calls[-1][2], calls[-1][3]
+    # in: 43 FP64 body columns, 6 byte columns, joint_head, the awake list and 3 materials a slot, and the
+    # pair list (a, b, memory, margin, tolerance); out: the 30 FP64 body columns the step writes, and each
+    # pair's point count and touching flag
+    h2d = nb * (43 * 8 + 6 + 4 + 4 + 3 * 8) + np_ * (3 * 4 + 2 * 8)
+    d2h = nb * (30 * 8) + 2 * np_
+    part = [statistics.mean(p[k] for p in parts) for k in range(4)]
+    out = {"workload": f"World.step of the {args.bodies}-body pile at steps {args.at + 2 + warmup}.."
+                       f"{args.at + 1 + warmup + steps}, its contact side on the device",
+           "unit": "ms", "pairs_listed": np_, "rows": rows,
+           "world_step_ms": statistics.mean(dev_ms), "host_path_world_step_ms": statistics.mean(host_ms),
+           "contact_call_ms": statistics.mean(call_ms),
+           "device_ms": {"narrowphase": part[0], "rows_colours_order": part[1], "solve_stage": part[2],
+                         "store": part[3]},
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+           "same_counts_as_host_path": same,
+           "what": "world_step_ms: World.step (host bounds, broadphase and pair upkeep, then bg_contact_step); "
+                   "host_path_world_step_ms: World.step with the host's rows (bg_collide narrowphase, host emit/carry/"
+                   "colour/arrange, bg_solve_step with pageable columns, host keep); contact_call_ms: bg_contact_step "
+                   "end to end on the host clock (bodies and pair list in, bodies out)"}
+    if log:
+        log(f"contact step: World.step {out['world_step_ms']:.1f} ms against {out['host_path_world_step_ms']:.1f} ms "
+            f"on the host path; bg_contact_step {out['contact_call_ms']:.2f} ms ({np_} pairs, {rows} rows; device "
+            f"{part[0]:.3f} + {part[1]:.3f} + {part[2]:.3f} + {part[3]:.3f} ms); same counts {same}")
+    wb.destroy()
+    dev.close()
+    return out
+
+
 def batch_roofline(algo, ms, cta_threads):
     """The batched kernel's roofline line: this rank's algorithmic bytes over the resident solve's
     time (the max over ranks), against the measured HBM copy rate; DRAM traffic scaled from the
@@ -756,6 +832,9 @@ def main():
     colouring = None
     if not args.resident_only and rank == 0:
         colouring = measure_colouring(lib, ctx, copy, args.steps, args.warmup, log)
+    contact = None
+    if not args.resident_only and rank == 0 and w is not None and not args.no_contact:
+        contact = measure_contact_step(args, lib, solver, w, local, args.steps, max(3, args.warmup), log)
     adj = None
     if not args.no_adjoint and not args.resident_only and rank == 0 and world_size == 1:
         adj = measure_adjoint(args, local, log)
@@ -779,7 +858,7 @@ def main():
                              "kernel_ms": ms_stage,
                              "algorithmic_bytes": algo, "peak_source": peak_source},
                 "cpu_baseline": cpu, "clocks": clock, "gpu_launches": launches, "batch": batch, "adjoint": adj,
-                "narrowphase": narrow, "colouring": colouring}
+                "narrowphase": narrow, "colouring": colouring, "contact_step": contact}
         print(json.dumps(line), flush=True)
     lib.bg_destroy(ctx)
     solver.close()

@@ -402,6 +402,61 @@ int32_t bg_colour(bg_ctx* ctx, const bg_bodies* bodies, int32_t count, const int
 /* Device time in milliseconds of the last bg_colour's kernels (synchronises; negative if none). */
 double bg_last_colour_ms(bg_ctx* ctx);
 
+/*
+ * A step's contacts on the device, from the pair list to the stored contact memory.  For each pair
+ * of the list the narrowphase (as bg_collide); for each pair that touches, a row, emitted, given its
+ * tangent basis and warm-started from the pair's remembered contact (src/contact.js:889-921 emit,
+ * 1283-1292 basis, 999-1036 carry); the rows coloured and ordered (src/graph.js:105-214, as
+ * bg_colour) and the resting ones set aside (src/contact.js:1318-1329 rest); the solve stage (as
+ * bg_solve_step); then each solved row's impulses stored into its pair's memory (src/contact.js:
+ * 1067-1115 store/keep) and each pair's touching flag (2178-2213).  Replaces src/contact.js
+ * narrow()'s find/emit/carry (296-368), colour/arrange, the solve stage (src/world.js:962-1032)
+ * and store/touched.  The rows never leave the device: the bodies and the pair list go to it, the
+ * bodies' written columns (as bg_solve_step writes them) and each pair's point count and touching
+ * flag come back.  bodies: every column bg_solve_step reads, and those bg_collide reads.  gravity
+ * is step->gravity.  Synchronous.
+ *
+ * The contact memory (src/pairs.js:50-58: a pair's remembered point ids and normal impulses, and its
+ * friction, twist and slip) lives in the context, one record per pair of the last call's list.
+ * pairs->memory[i] names pair i's record: its index in the list the previous bg_contact_step on this
+ * context took, or -1 for a pair with nothing remembered (new, or forgotten since).  Each call
+ * leaves one record per pair of its own list for the next: what store() keeps of a solved row, the
+ * record the pair had for a resting row (store() skips those), nothing for a pair apart.
+ * Refused with BG_EINVAL before anything is copied: a pair's slot out of range or both slots
+ * equal, a shape that is not a box, sphere or capsule, a memory index outside [-1, records),
+ * an awake entry out of range.
+ */
+typedef struct bg_materials {
+  const double* friction;      /* per slot: World._friction */
+  const double* restitution;   /* per slot: World._restitution */
+  const double* size;          /* per slot: World._size (a row's patch, src/contact.js:906) */
+} bg_materials;
+
+typedef struct bg_contact_pairs {
+  bg_pairs list;               /* the pairs whose boxes meet, in pair order (src/contact.js:312-327) */
+  const int32_t* memory;       /* per pair: its record in the previous call's list, or -1 */
+} bg_contact_pairs;
+
+typedef struct bg_contact_result {
+  uint8_t* points;             /* per pair, or NULL: its manifold's point count (0: apart) */
+  uint8_t* touching;           /* per pair, or NULL: touched()'s flag (0 for a pair apart) */
+  int32_t rows;                /* Contacts.count */
+  int32_t solved;              /* rows before the resting run */
+  int32_t points_solved;       /* contact points of the solved rows */
+  int32_t starts[BG_STARTS];   /* Contacts.starts */
+} bg_contact_result;
+
+int32_t bg_contact_step(bg_ctx* ctx, const bg_bodies* bodies, const bg_materials* materials,
+                        const bg_contact_pairs* pairs, const bg_step* step, bg_contact_result* out);
+/* Device time in milliseconds of the last bg_contact_step's parts (synchronises): ms[0] the
+ * narrowphase, ms[1] rows, colours and order, ms[2] the solve stage, ms[3] store and touched.
+ * BG_EINVAL if there was none. */
+int32_t bg_last_contact_ms(bg_ctx* ctx, double* ms);
+/* Records the context holds for the next bg_contact_step (the last call's list length). */
+int32_t bg_contact_records(const bg_ctx* ctx);
+/* Forgets every record: the next call's memory entries must all be -1. */
+int32_t bg_contact_forget(bg_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

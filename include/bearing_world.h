@@ -86,6 +86,18 @@ typedef int32_t (*bw_narrowphase)(void* user, const bg_bodies* bodies, const dou
                                   bg_manifolds* out);
 int32_t bw_set_narrowphase(bw_world* world, bw_narrowphase fn, void* user);
 
+/* The whole contact side of a step on another device: fn (bg_contact_step's signature, with `user`
+ * for its context) is handed the bodies, their materials and the step's pairs whose boxes meet, with
+ * each pair's contact record from the previous call, and runs the narrowphase, the rows, colouring,
+ * the solve stage and store() there (src/contact.js:296-368, 889-1115, 2178-2213; src/graph.js:
+ * 105-214; src/world.js:962-1032).  The host keeps the pair list (src/pairs.js) and forgets the
+ * pairs fn reports apart.  The step's rows then never reach the host: bw_rows_view shows none, and
+ * bw_begin_step is refused.  Set it before the first step (BG_EINVAL after); NULL (the default)
+ * keeps the host's rows and bw_set_solver's solve stage. */
+typedef int32_t (*bw_contact_solver)(void* user, const bg_bodies* bodies, const bg_materials* materials,
+                                     const bg_contact_pairs* pairs, const bg_step* step, bg_contact_result* out);
+int32_t bw_set_contact_step(bw_world* world, bw_contact_solver fn, void* user);
+
 /* A whole World.step(dt): bw_begin_step, the solver, bw_end_step. */
 int32_t bw_step(bw_world* world, double dt);
 
