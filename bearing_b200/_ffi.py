@@ -170,13 +170,13 @@ class Manifolds(C.Structure):
 class Materials(C.Structure):
     """bg_materials: per-slot friction, restitution and size, what emit() reads."""
 
-    _fields_ = [("friction", _d), ("restitution", _d), ("size", _d)]
+    _fields_ = [("friction", _d), ("restitution", _d), ("size", _d), ("reach", _d)]
 
 
 class ContactPairs(C.Structure):
     """bg_contact_pairs: the step's pair list with each pair's contact record (or -1)."""
 
-    _fields_ = [("list", Pairs), ("memory", _i32)]
+    _fields_ = [("list", Pairs), ("memory", _i32), ("reuse", C.c_int32)]
 
 
 class ContactResult(C.Structure):
@@ -187,7 +187,7 @@ class ContactResult(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = [("gravity", C.c_double * 3), ("substeps", C.c_int32)]
+    _fields_ = [("gravity", C.c_double * 3), ("substeps", C.c_int32), ("reuse", C.c_int32)]
 
 
 class BodySpec(C.Structure):

@@ -2623,6 +2623,7 @@ struct CollideParams {
   double gravity[3];
   int32_t* counts;   // kPairClasses pairs per class, then kPairClasses cursors
   int32_t* order;    // pairs in class order
+  const uint8_t* skip;   // per pair, or NULL: 1 for a pair whose manifold is already known
   uint8_t* points;
   double *normal, *point, *separation;
   uint32_t* pid;
@@ -2644,7 +2645,7 @@ __global__ void collide_count(CollideParams c) {
   if (threadIdx.x < kPairClasses) local[threadIdx.x] = 0;
   __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x)
-    atomicAdd(&local[pair_class(c, i)], 1);
+    if (c.skip == nullptr || c.skip[i] == 0) atomicAdd(&local[pair_class(c, i)], 1);
   __syncthreads();
   if (threadIdx.x < kPairClasses && local[threadIdx.x] > 0) atomicAdd(&c.counts[threadIdx.x], local[threadIdx.x]);
 }
@@ -2661,7 +2662,7 @@ __global__ void collide_starts(CollideParams c) {
 
 __global__ void collide_scatter(CollideParams c) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x)
-    c.order[atomicAdd(&c.counts[kPairClasses + pair_class(c, i)], 1)] = i;
+    if (c.skip == nullptr || c.skip[i] == 0) c.order[atomicAdd(&c.counts[kPairClasses + pair_class(c, i)], 1)] = i;
 }
 
 // load(): src/contact.js:1244-1276, for boxes, spheres and capsules, with the axes of
@@ -2691,7 +2692,12 @@ __device__ void load_shape(const CollideParams& c, int slot, bearing::Shape& s) 
 }
 
 __global__ void __launch_bounds__(kCollideThreads) collide_pairs(CollideParams c) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < c.n; j += gridDim.x * blockDim.x) {
+  int n = c.n;   // the pairs sorted into `order`: all of them, or those not skipped
+  if (c.skip != nullptr) {
+    n = 0;
+    for (int k = 0; k < kPairClasses; k++) n += c.counts[k];
+  }
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const int i = c.order[j];
     bearing::Shape sa, sb;
     bearing::Manifold mf;
@@ -2811,7 +2817,7 @@ int32_t bg_collide(bg_ctx* c, const bg_bodies* B, const double* gravity, const b
   k.a = L.a; k.b = L.b; k.margin = L.margin; k.tol = L.tol; k.n = static_cast<int32_t>(np);
   for (int e = 0; e < 3; e++) k.gravity[e] = gravity[e];
   k.counts = L.counts; k.order = L.order; k.points = L.points; k.normal = L.normal; k.point = L.point;
-  k.separation = L.separation; k.pid = L.pid;
+  k.separation = L.separation; k.pid = L.pid; k.skip = nullptr;
   const int sweep = std::max(1, std::min(static_cast<int>((np + 255) / 256), 4 * c->sms));
   collide_count<<<sweep, 256, 0, st>>>(k);
   collide_starts<<<1, 32, 0, st>>>(k);
@@ -3032,6 +3038,7 @@ namespace {
 struct ContactIn {
   const int32_t *a = nullptr, *b = nullptr, *memory = nullptr;
   const double *margin = nullptr, *tol = nullptr, *friction = nullptr, *restitution = nullptr, *size = nullptr;
+  const double* reach = nullptr;
 };
 
 Plan plan_contact_in(bg_ctx* c, const bg_bodies* B, const bg_materials* M, const bg_contact_pairs* CP, size_t nb,
@@ -3046,6 +3053,8 @@ Plan plan_contact_in(bg_ctx* c, const bg_bodies* B, const bg_materials* M, const
   in.friction = P.in<double>(M ? M->friction : nullptr, nb, "materials.friction");
   in.restitution = P.in<double>(M ? M->restitution : nullptr, nb, "materials.restitution");
   in.size = P.in<double>(M ? M->size : nullptr, nb, "materials.size");
+  const bool reuse = CP != nullptr && CP->reuse != 0;
+  in.reach = P.in<double>(M && reuse ? M->reach : nullptr, reuse || CP == nullptr ? nb : 0, "materials.reach");
   return P;
 }
 
@@ -3062,6 +3071,7 @@ struct ContactLayout {
   int32_t *off, *cursor, *list;    // each body's solved rows (the dataflow's ranks)
   uint8_t* touching;
   int32_t* points_solved;
+  uint8_t* kept;                   // per pair: its manifold reused
   size_t bytes;
 };
 
@@ -3086,7 +3096,7 @@ ContactLayout contact_layout(unsigned char* base, size_t nb, size_t np) {
   L.ocounts = k.take<int32_t>(bgct::kKeys * tiles + 1);
   L.groups = k.take<int32_t>(bgct::kKeys + 1); L.chunk_base = k.take<int32_t>(bgct::kKeys + 1);
   L.off = k.take<int32_t>(nb + 1); L.cursor = k.take<int32_t>(nb); L.list = k.take<int32_t>(2 * np);
-  L.touching = k.take<uint8_t>(np); L.points_solved = k.take<int32_t>(1);
+  L.touching = k.take<uint8_t>(np); L.points_solved = k.take<int32_t>(1); L.kept = k.take<uint8_t>(np);
   L.bytes = k.end;
   return L;
 }
@@ -3097,6 +3107,9 @@ bgct::Memory bank_at(unsigned char* base, size_t cap, size_t* bytes = nullptr) {
   bgct::Memory m;
   m.points = k.take<uint8_t>(cap); m.pid = k.take<uint32_t>(bg::P * cap); m.ni = k.take<double>(bg::P * cap);
   m.friction = k.take<double>(3 * cap); m.twist = k.take<double>(3 * cap); m.slip = k.take<double>(3 * cap);
+  m.touching = k.take<uint8_t>(cap); m.cached = k.take<uint8_t>(cap); m.cache_points = k.take<uint8_t>(cap);
+  m.pose = k.take<double>(7 * cap); m.loss = k.take<double>(cap); m.local_normal = k.take<double>(3 * cap);
+  m.local = k.take<double>(6 * bg::P * cap); m.cache_id = k.take<uint32_t>(bg::P * cap);
   if (bytes) *bytes = k.end;
   return m;
 }
@@ -3148,6 +3161,10 @@ bool contact_blocks(bg_ctx* c, size_t nb, size_t np) {
       copy(to.points, from.points, n); copy(to.pid, from.pid, sizeof(uint32_t) * bg::P * n);
       copy(to.ni, from.ni, sizeof(double) * bg::P * n); copy(to.friction, from.friction, sizeof(double) * 3 * n);
       copy(to.twist, from.twist, sizeof(double) * 3 * n); copy(to.slip, from.slip, sizeof(double) * 3 * n);
+      copy(to.touching, from.touching, n); copy(to.cached, from.cached, n); copy(to.cache_points, from.cache_points, n);
+      copy(to.pose, from.pose, sizeof(double) * 7 * n); copy(to.loss, from.loss, sizeof(double) * n);
+      copy(to.local_normal, from.local_normal, sizeof(double) * 3 * n);
+      copy(to.local, from.local, sizeof(double) * 6 * bg::P * n); copy(to.cache_id, from.cache_id, sizeof(uint32_t) * bg::P * n);
       ok = ok && cudaStreamSynchronize(c->stream) == cudaSuccess;
     }
     if (!ok) {
@@ -3283,9 +3300,24 @@ int32_t bg_contact_step(bg_ctx* c, const bg_bodies* B, const bg_materials* M, co
     return cuda_ok(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st), what);
   };
   const int sweep = std::max(1, std::min((np + 255) / 256, 8 * c->sms));
-  // the narrowphase, as bg_collide runs it, on the uploaded bodies and pairs
+  const bool reuse = CP->reuse != 0;
+  bgct::Poses poses;
+  poses.p = c->bin.position; poses.q = c->bin.rotation; poses.v = c->bin.velocity; poses.w = c->bin.angular;
+  poses.dims = c->bin.dims; poses.reach = in.reach; poses.gscale = c->bin.gravity_scale; poses.type = c->bin.type;
+  poses.shape = c->bin.shape; poses.joint_head = c->bin.joint_head;
+  for (int k = 0; k < 3; k++) poses.gravity[k] = step->gravity[k];
+  poses.dt = step->dt;
+  // the kept manifolds that still hold, then the narrowphase, as bg_collide runs it, for the rest
   cudaEventRecord(d.ev[0], st);
   if (np > 0) {
+    if (reuse) {
+      bgct::ReuseParams rp;
+      rp.np = np; rp.a = in.a; rp.b = in.b; rp.margin = in.margin; rp.tol = in.tol; rp.memory = in.memory;
+      rp.s = poses; rp.old = old; rp.kept = L.kept; rp.points = L.points; rp.normal = L.normal; rp.point = L.point;
+      rp.separation = L.separation; rp.pid = L.pid;
+      bgct::ct_reuse<<<sweep, 256, 0, st>>>(rp);
+      c->last_launches += 1;
+    }
     if (!cuda_ok(c, cudaMemsetAsync(L.counts, 0, 2 * kPairClasses * sizeof(int32_t), st), "bg_contact_step")) return BG_ECUDA;
     CollideParams k;
     k.p = c->bin.position; k.q = c->bin.rotation; k.dims = c->bin.dims; k.gscale = c->bin.gravity_scale;
@@ -3293,7 +3325,7 @@ int32_t bg_contact_step(bg_ctx* c, const bg_bodies* B, const bg_materials* M, co
     k.a = in.a; k.b = in.b; k.margin = in.margin; k.tol = in.tol; k.n = np;
     for (int e = 0; e < 3; e++) k.gravity[e] = step->gravity[e];
     k.counts = L.counts; k.order = L.corder; k.points = L.points; k.normal = L.normal; k.point = L.point;
-    k.separation = L.separation; k.pid = L.pid;
+    k.separation = L.separation; k.pid = L.pid; k.skip = reuse ? L.kept : nullptr;
     collide_count<<<sweep, 256, 0, st>>>(k);
     collide_starts<<<1, 32, 0, st>>>(k);
     collide_scatter<<<sweep, 256, 0, st>>>(k);
@@ -3308,6 +3340,7 @@ int32_t bg_contact_step(bg_ctx* c, const bg_bodies* B, const bg_materials* M, co
   e.points = L.points; e.normal = L.normal; e.point = L.point; e.separation = L.separation; e.pid = L.pid;
   e.friction = in.friction; e.restitution = in.restitution; e.size = in.size; e.type = c->bin.type;
   e.rowof = L.rowof; e.old = old; e.r = L.r;
+  e.reuse = reuse ? 1 : 0; e.kept = L.kept; e.next = next; e.s = poses;
   int nrows = 0;
   if (np > 0) {
     bgct::ct_flags<<<sweep, 256, 0, st>>>(e);
@@ -3420,7 +3453,7 @@ int32_t bg_contact_step(bg_ctx* c, const bg_bodies* B, const bg_materials* M, co
     bgct::KeepParams kp;
     kp.np = np; kp.solved = solved; kp.points = L.points; kp.rowof = L.rowof; kp.memory = in.memory;
     kp.iperm = c->iperm_dev; kp.pid = L.r.pid; kp.R = c->R; kp.old = old; kp.next = next; kp.touching = L.touching;
-    kp.points_solved = L.points_solved;
+    kp.points_solved = L.points_solved; kp.reuse = reuse ? 1 : 0;
     bgct::ct_keep<<<sweep, 256, 0, st>>>(kp);
     c->last_launches += 1;
   }

@@ -44,7 +44,8 @@ __device__ __forceinline__ double ct_min(double a, double b) {
   return a;
 }
 
-// One bank of contact memory, `cap` records.
+// One bank of contact memory, `cap` records: what the pair remembers for carry() (src/pairs.js:
+// 50-58), its touching flag, and the manifold it keeps for reused() (src/pairs.js:55-80).
 struct Memory {
   uint8_t* points;    // remembered point count (0: nothing remembered)
   uint32_t* pid;      // P per record
@@ -52,7 +53,165 @@ struct Memory {
   double* friction;   // 3 per record
   double* twist;      // 3 per record
   double* slip;       // 3 per record
+  uint8_t* touching;  // touched()'s flag as of the call that wrote the record
+  uint8_t* cached;    // 1: a kept manifold follows
+  uint8_t* cache_points;
+  double* pose;       // 7 per record: the pose it was found at (relative())
+  double* loss;
+  double* local_normal;   // 3 per record: its normal in a's frame
+  double* local;      // 6 P per record: each point's end on a (a's frame) and on b (b's frame)
+  uint32_t* cache_id; // P per record
 };
+
+// ---- the kept manifold: src/contact.js:388-595 (REUSE) ----
+
+// What the reuse rules read of a body, besides the pair's record.
+struct Poses {
+  const double *p, *q, *v, *w, *dims, *reach, *gscale;
+  const uint8_t *type, *shape;
+  const int32_t* joint_head;
+  double gravity[3];
+  double dt;
+};
+
+// axesOf: src/core/math.js:222-227.
+__device__ __forceinline__ void ct_axes(const double* q, double* ax) {
+  const double x = q[0], y = q[1], z = q[2], w = q[3];
+  ax[0] = 1 - 2 * (y * y + z * z); ax[1] = 2 * (x * y + z * w); ax[2] = 2 * (x * z - y * w);
+  ax[3] = 2 * (x * y - z * w); ax[4] = 1 - 2 * (x * x + z * z); ax[5] = 2 * (y * z + x * w);
+  ax[6] = 2 * (x * z + y * w); ax[7] = 2 * (y * z - x * w); ax[8] = 1 - 2 * (x * x + y * y);
+}
+
+// relative(): src/contact.js:596-610.  Returns the smaller body.
+__device__ __forceinline__ int ct_relative(const Poses& s, int a, int b, double* pose) {
+  const int h = s.reach[a] >= s.reach[b] ? a : b, g = h == a ? b : a;
+  double A[9];
+  ct_axes(s.q + 4 * h, A);
+  const double dx = s.p[3 * g] - s.p[3 * h], dy = s.p[3 * g + 1] - s.p[3 * h + 1], dz = s.p[3 * g + 2] - s.p[3 * h + 2];
+  pose[0] = A[0] * dx + A[1] * dy + A[2] * dz;
+  pose[1] = A[3] * dx + A[4] * dy + A[5] * dz;
+  pose[2] = A[6] * dx + A[7] * dy + A[8] * dz;
+  const double ax = -s.q[4 * h], ay = -s.q[4 * h + 1], az = -s.q[4 * h + 2], aw = s.q[4 * h + 3];
+  const double bx = s.q[4 * g], by = s.q[4 * g + 1], bz = s.q[4 * g + 2], bw = s.q[4 * g + 3];
+  pose[3] = aw * bx + ax * bw + ay * bz - az * by;
+  pose[4] = aw * by + ay * bw + az * bx - ax * bz;
+  pose[5] = aw * bz + az * bw + ax * by - ay * bx;
+  pose[6] = aw * bw - ax * bx - ay * by - az * bz;
+  return g;
+}
+
+// moving(): src/contact.js:695-703.
+__device__ __forceinline__ double ct_moving(const Poses& s, int a, int b) {
+  const int a3 = 3 * a, b3 = 3 * b;
+  const double ga = s.type[a] == kDynamic ? s.gscale[a] : 0, gb = s.type[b] == kDynamic ? s.gscale[b] : 0;
+  const double dx = s.v[b3] - s.v[a3], dy = s.v[b3 + 1] - s.v[a3 + 1], dz = s.v[b3 + 2] - s.v[a3 + 2];
+  const double gs = gb - ga;
+  const double gl = sqrt(s.gravity[0] * s.gravity[0] + s.gravity[1] * s.gravity[1] + s.gravity[2] * s.gravity[2]) * fabs(gs);
+  const double* w = s.w;
+  const double turning = sqrt(w[a3] * w[a3] + w[a3 + 1] * w[a3 + 1] + w[a3 + 2] * w[a3 + 2]) * s.reach[a]
+    + sqrt(w[b3] * w[b3] + w[b3 + 1] * w[b3 + 1] + w[b3 + 2] * w[b3 + 2]) * s.reach[b];
+  return (sqrt(dx * dx + dy * dy + dz * dz) + 0.5 * gl * s.dt + turning) * s.dt;
+}
+
+// keeps(): src/contact.js:516-537, for record j.
+__device__ __forceinline__ bool ct_keeps(const Poses& s, const Memory& m, int j, int a, int b, double tolerance) {
+  const double* pose = m.pose + 7 * j;
+  double now[7];
+  const int g = ct_relative(s, a, b, now);
+  const double ex = now[0] - pose[0], ey = now[1] - pose[1], ez = now[2] - pose[2];
+  const double cx = -pose[3], cy = -pose[4], cz = -pose[5], cw = pose[6];
+  const double rx = now[3], ry = now[4], rz = now[5], rw = now[6];
+  const double ux = cw * rx + cx * rw + cy * rz - cz * ry;
+  const double uy = cw * ry + cy * rw + cz * rx - cx * rz;
+  const double uz = cw * rz + cz * rw + cx * ry - cy * rx;
+  const double drift = sqrt(ex * ex + ey * ey + ez * ez) + 2 * sqrt(ux * ux + uy * uy + uz * uz) * s.reach[g];
+  if (m.loss[j] + 2 * drift > tolerance) return false;
+  if (s.joint_head[a] != 0 || s.joint_head[b] != 0) return false;
+  return m.touching[j] == 1 || drift + ct_moving(s, a, b) <= tolerance;
+}
+
+// rounded(): src/contact.js:571-575.
+__device__ __forceinline__ double ct_rounded(const Poses& s, int x) {
+  return s.shape[x] == BG_SPHERE || s.shape[x] == BG_CAPSULE ? s.dims[3 * x] : 0;
+}
+
+// cored(): src/contact.js:578-585.
+__device__ __forceinline__ void ct_cored(const Poses& s, int x, double* local) {
+  if (s.shape[x] == BG_SPHERE) { local[0] = 0; local[1] = 0; local[2] = 0; return; }
+  if (s.shape[x] != BG_CAPSULE) return;
+  const double half = (s.dims[3 * x + 1] - 2 * s.dims[3 * x]) * 0.5, y = local[1];
+  local[0] = 0; local[1] = y < -half ? -half : y > half ? half : y; local[2] = 0;
+}
+
+struct ReuseParams {
+  int32_t np;
+  const int32_t *a, *b;
+  const double *margin, *tol;
+  const int32_t* memory;
+  Poses s;
+  Memory old;
+  uint8_t* kept;                    // per pair: 1 if its manifold was reused
+  uint8_t* points;                  // the manifolds, per pair (kept ones written here)
+  double *normal, *point, *separation;
+  uint32_t* pid;
+};
+
+// reused() (src/contact.js:468-510, never shifted) for each pair with a kept manifold: the manifold
+// rebuilt from the bodies' poses now, or not kept (the narrowphase then finds it afresh).
+__global__ void ct_reuse(ReuseParams r) {
+  const Poses& s = r.s;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.np; i += gridDim.x * blockDim.x) {
+    r.kept[i] = 0;
+    const int j = r.memory[i];
+    if (j < 0 || r.old.cached[j] == 0) continue;
+    const int a = r.a[i], b = r.b[i];
+    if (!ct_keeps(s, r.old, j, a, b, r.tol[i])) continue;
+    const int count = r.old.cache_points[j];
+    double A[9], Bx[9];
+    ct_axes(s.q + 4 * a, A);
+    ct_axes(s.q + 4 * b, Bx);
+    const double* ln = r.old.local_normal + 3 * j;
+    const double lx = ln[0], ly = ln[1], lz = ln[2];
+    const double nx = A[0] * lx + A[3] * ly + A[6] * lz;
+    const double ny = A[1] * lx + A[4] * ly + A[7] * lz;
+    const double nz = A[2] * lx + A[5] * ly + A[8] * lz;
+    const double ra = ct_rounded(s, a), rb = -ct_rounded(s, b);
+    const double* pa0 = s.p + 3 * a;
+    const double* pb0 = s.p + 3 * b;
+    double sep[P], pt[3 * P];
+    double least = __longlong_as_double(0x7ff0000000000000LL);   // +Infinity
+    for (int k = 0; k < count; k++) {
+      const double* l = r.old.local + 6 * (P * j + k);
+      const double ax = l[0], ay = l[1], az = l[2], bx = l[3], by = l[4], bz = l[5];
+      const double pax = pa0[0] + A[0] * ax + A[3] * ay + A[6] * az + nx * ra;
+      const double pay = pa0[1] + A[1] * ax + A[4] * ay + A[7] * az + ny * ra;
+      const double paz = pa0[2] + A[2] * ax + A[5] * ay + A[8] * az + nz * ra;
+      const double pbx = pb0[0] + Bx[0] * bx + Bx[3] * by + Bx[6] * bz + nx * rb;
+      const double pby = pb0[1] + Bx[1] * bx + Bx[4] * by + Bx[7] * bz + ny * rb;
+      const double pbz = pb0[2] + Bx[2] * bx + Bx[5] * by + Bx[8] * bz + nz * rb;
+      const double sp = (pbx - pax) * nx + (pby - pay) * ny + (pbz - paz) * nz, half = 0.5 * sp;
+      sep[k] = sp;
+      if (rb != 0) {
+        pt[3 * k] = pbx - nx * half; pt[3 * k + 1] = pby - ny * half; pt[3 * k + 2] = pbz - nz * half;
+      } else if (ra != 0) {
+        pt[3 * k] = pax + nx * half; pt[3 * k + 1] = pay + ny * half; pt[3 * k + 2] = paz + nz * half;
+      } else {
+        pt[3 * k] = (pax + pbx) * 0.5; pt[3 * k + 1] = (pay + pby) * 0.5; pt[3 * k + 2] = (paz + pbz) * 0.5;
+      }
+      if (sp < least) least = sp;
+    }
+    if (least > r.margin[i]) continue;   // least(): src/contact.js:684-688
+    r.kept[i] = 1;
+    r.points[i] = static_cast<uint8_t>(count);
+    r.normal[3 * i] = nx; r.normal[3 * i + 1] = ny; r.normal[3 * i + 2] = nz;
+    for (int k = 0; k < P; k++) {
+      const bool used = k < count;
+      for (int e = 0; e < 3; e++) r.point[3 * (P * i + k) + e] = used ? pt[3 * k + e] : 0.0;
+      r.separation[P * i + k] = used ? sep[k] : 0.0;
+      r.pid[P * i + k] = used ? r.old.cache_id[P * j + k] : 0u;
+    }
+  }
+}
 
 // The step's rows in found order, in the caller's row layout (bg_rows), so the solve stage's
 // unpack kernel reads them as it reads an upload.
@@ -77,6 +236,12 @@ struct EmitParams {
   int32_t* rowof;                   // np + 1: (points > 0), then its exclusive scan (found row)
   Memory old;
   FoundRows r;
+  // the kept manifolds, with reuse on: which pairs reused theirs, and the next bank, which keeps
+  // each touching pair's (remember(), src/contact.js:540-569, for a fresh one)
+  int32_t reuse;
+  const uint8_t* kept;
+  Memory next;
+  Poses s;
 };
 
 // Which pairs emit a row.
@@ -128,8 +293,47 @@ __global__ void ct_emit(EmitParams e) {
       r.ni[o] = 0; r.maxni[o] = 0; r.relvel[o] = 0;
     }
     ct_basis(r, m);
-    // carry(), from the pair's record
     const int j = e.memory[i];
+    if (e.reuse) {
+      Memory& n = e.next;
+      n.cached[i] = 1;
+      n.cache_points[i] = static_cast<uint8_t>(count);
+      if (e.kept[i]) {   // the record's kept manifold goes on as it was
+        for (int k = 0; k < 7; k++) n.pose[7 * i + k] = e.old.pose[7 * j + k];
+        n.loss[i] = e.old.loss[j];
+        for (int k = 0; k < 3; k++) n.local_normal[3 * i + k] = e.old.local_normal[3 * j + k];
+        for (int k = 0; k < 6 * P; k++) n.local[6 * P * i + k] = e.old.local[6 * P * j + k];
+        for (int k = 0; k < P; k++) n.cache_id[P * i + k] = e.old.cache_id[P * j + k];
+      } else {           // remember(): the manifold collide() just found
+        const Poses& s = e.s;
+        ct_relative(s, a, b, n.pose + 7 * i);
+        n.loss[i] = 0;   // collide() of boxes, spheres and capsules falls short of nothing
+        double A[9], Bx[9];
+        ct_axes(s.q + 4 * a, A);
+        ct_axes(s.q + 4 * b, Bx);
+        const double nx = r.normal[3 * m], ny = r.normal[3 * m + 1], nz = r.normal[3 * m + 2];
+        n.local_normal[3 * i] = A[0] * nx + A[1] * ny + A[2] * nz;
+        n.local_normal[3 * i + 1] = A[3] * nx + A[4] * ny + A[5] * nz;
+        n.local_normal[3 * i + 2] = A[6] * nx + A[7] * ny + A[8] * nz;
+        for (int k = 0; k < count; k++) {
+          double* l = n.local + 6 * (P * i + k);
+          const double half = 0.5 * r.separation[m * P + k];
+          const double px = r.point[3 * (m * P + k)], py = r.point[3 * (m * P + k) + 1], pz = r.point[3 * (m * P + k) + 2];
+          const double ax = px - nx * half - s.p[3 * a], ay = py - ny * half - s.p[3 * a + 1], az = pz - nz * half - s.p[3 * a + 2];
+          const double bx = px + nx * half - s.p[3 * b], by = py + ny * half - s.p[3 * b + 1], bz = pz + nz * half - s.p[3 * b + 2];
+          l[0] = A[0] * ax + A[1] * ay + A[2] * az;
+          l[1] = A[3] * ax + A[4] * ay + A[5] * az;
+          l[2] = A[6] * ax + A[7] * ay + A[8] * az;
+          l[3] = Bx[0] * bx + Bx[1] * by + Bx[2] * bz;
+          l[4] = Bx[3] * bx + Bx[4] * by + Bx[5] * bz;
+          l[5] = Bx[6] * bx + Bx[7] * by + Bx[8] * bz;
+          ct_cored(s, a, l);
+          ct_cored(s, b, l + 3);
+          n.cache_id[P * i + k] = r.pid[m * P + k];
+        }
+      }
+    }
+    // carry(), from the pair's record
     const int remembered = j < 0 ? 0 : e.old.points[j];
     if (remembered == 0) continue;
     const int m3 = 3 * m, j3 = 3 * j;
@@ -350,6 +554,7 @@ struct KeepParams {
   Memory old, next;
   uint8_t* touching;             // per pair
   int32_t* points_solved;        // sum of the solved rows' points
+  int32_t reuse;
 };
 
 // For each pair of the list: its record for the next call (keep(), src/contact.js:1091-1115, for a
@@ -362,6 +567,8 @@ __global__ void ct_keep(KeepParams k) {
     const int count = k.points[i];
     if (count == 0) {
       k.next.points[i] = 0;
+      k.next.touching[i] = 0;
+      k.next.cached[i] = 0;   // forget() uncaches: src/pairs.js:236
       k.touching[i] = 0;
       continue;
     }
@@ -370,6 +577,8 @@ __global__ void ct_keep(KeepParams k) {
     bool meets = R.gap[d] <= R.tolerance[d];
     for (int q = 0; q < count && !meets; q++) meets = R.maxni[q * cap + d] > 0;
     k.touching[i] = meets ? 1 : 0;
+    k.next.touching[i] = meets ? 1 : 0;
+    if (!k.reuse) k.next.cached[i] = 0;
     if (d >= k.solved) {
       const int j = k.memory[i];
       const int have = j < 0 ? 0 : k.old.points[j];

@@ -124,6 +124,13 @@ struct Pairs {
   // with the contact step on another device (bw_set_contact_step): where the pair's memory is, its
   // index in the last list handed over, or -1 (nothing remembered)
   std::vector<int32_t> record;
+  // The kept manifold (src/pairs.js:55-80, contact.js reused/remember), by pair rather than in rows
+  // of its own (which rows hold which pair changes no result): whether one is kept, its point count,
+  // the pose it was found at (7), how far it fell short of exact, its normal in a's frame (3), each
+  // point's end on a in a's frame and on b in b's frame (6 a point) and feature ids.
+  std::vector<uint8_t> cached, cachePoints;
+  std::vector<double> cachePose, cacheLoss, cacheNormal, cacheLocal;
+  std::vector<uint32_t> cacheId;
   std::unordered_map<uint64_t, int32_t> index;
 
   static uint64_t key(int x, int y) { return (static_cast<uint64_t>(x) << 32) | static_cast<uint32_t>(y); }
@@ -133,6 +140,8 @@ struct Pairs {
     size_t cap = a.size() > 16 ? a.size() : 16;
     while (cap < c) cap *= 2;
     a.resize(cap); b.resize(cap); points.resize(cap); touching.resize(cap); record.resize(cap, -1);
+    cached.resize(cap); cachePoints.resize(cap); cachePose.resize(7 * cap); cacheLoss.resize(cap);
+    cacheNormal.resize(3 * cap); cacheLocal.resize(6 * P * cap); cacheId.resize(P * cap);
     pid.resize(P * cap); normalImpulse.resize(P * cap);
     friction.resize(3 * cap); slip.resize(3 * cap); twist.resize(3 * cap);
   }
@@ -143,7 +152,7 @@ struct Pairs {
     if (index.count(key(lo, hi))) return;
     const int p = count;
     reserve(p + 1);
-    a[p] = lo; b[p] = hi; points[p] = 0; touching[p] = 0; record[p] = -1;
+    a[p] = lo; b[p] = hi; points[p] = 0; touching[p] = 0; record[p] = -1; cached[p] = 0;
     index[key(lo, hi)] = p;
     count++;
     active = count;
@@ -151,6 +160,13 @@ struct Pairs {
   void moveTo(int from, int to) {
     a[to] = a[from]; b[to] = b[from]; points[to] = points[from]; touching[to] = touching[from];
     record[to] = record[from];
+    cached[to] = cached[from];
+    cachePoints[to] = cachePoints[from];
+    cacheLoss[to] = cacheLoss[from];
+    for (int k = 0; k < 7; k++) cachePose[7 * to + k] = cachePose[7 * from + k];
+    for (int k = 0; k < 3; k++) cacheNormal[3 * to + k] = cacheNormal[3 * from + k];
+    for (int k = 0; k < 6 * P; k++) cacheLocal[6 * P * to + k] = cacheLocal[6 * P * from + k];
+    for (int k = 0; k < P; k++) cacheId[P * to + k] = cacheId[P * from + k];
     for (int k = 0; k < P; k++) { pid[P * to + k] = pid[P * from + k]; normalImpulse[P * to + k] = normalImpulse[P * from + k]; }
     for (int k = 0; k < 3; k++) {
       friction[3 * to + k] = friction[3 * from + k];
@@ -171,6 +187,7 @@ struct Pairs {
     points[p] = 0;
     touching[p] = 0;
     record[p] = -1;
+    cached[p] = 0;   // uncache: src/pairs.js:236
   }
 };
 
@@ -469,6 +486,142 @@ struct bw_world {
     for (int k = 0; k < 9; k++) s.axes[k] = axes[9 * slot + k];
   }
 
+  // ---- the kept manifold: src/contact.js:388-595 (REUSE) ----
+
+  // relative(): src/contact.js:596-610.  The smaller body's centre in the larger's frame and the
+  // larger's rotation undone from the smaller's, into pose; returns the smaller body.
+  int relative(int a, int b, double* pose) const {
+    const int h = reach[a] >= reach[b] ? a : b, g = h == a ? b : a;
+    const double* A = axes.data();
+    const int h3 = 3 * h, g3 = 3 * g, h9 = 9 * h, h4 = 4 * h, g4 = 4 * g;
+    const double dx = position[g3] - position[h3], dy = position[g3 + 1] - position[h3 + 1],
+                 dz = position[g3 + 2] - position[h3 + 2];
+    pose[0] = A[h9] * dx + A[h9 + 1] * dy + A[h9 + 2] * dz;
+    pose[1] = A[h9 + 3] * dx + A[h9 + 4] * dy + A[h9 + 5] * dz;
+    pose[2] = A[h9 + 6] * dx + A[h9 + 7] * dy + A[h9 + 8] * dz;
+    const double ax = -rotation[h4], ay = -rotation[h4 + 1], az = -rotation[h4 + 2], aw = rotation[h4 + 3];
+    const double bx = rotation[g4], by = rotation[g4 + 1], bz = rotation[g4 + 2], bw = rotation[g4 + 3];
+    pose[3] = aw * bx + ax * bw + ay * bz - az * by;
+    pose[4] = aw * by + ay * bw + az * bx - ax * bz;
+    pose[5] = aw * bz + az * bw + ax * by - ay * bx;
+    pose[6] = aw * bw - ax * bx - ay * by - az * bz;
+    return g;
+  }
+
+  // moving(): src/contact.js:695-703.
+  double moving(int a, int b) const {
+    const double dt = stepDt;
+    const int a3 = 3 * a, b3 = 3 * b;
+    const double ga = type[a] == BG_DYNAMIC ? gravityScale[a] : 0, gb = type[b] == BG_DYNAMIC ? gravityScale[b] : 0;
+    const double dx = velocity[b3] - velocity[a3], dy = velocity[b3 + 1] - velocity[a3 + 1],
+                 dz = velocity[b3 + 2] - velocity[a3 + 2];
+    const double gs = gb - ga, gl = std::sqrt(gravity[0] * gravity[0] + gravity[1] * gravity[1] + gravity[2] * gravity[2]) * std::fabs(gs);
+    const double* w = angular.data();
+    const double turning = std::sqrt(w[a3] * w[a3] + w[a3 + 1] * w[a3 + 1] + w[a3 + 2] * w[a3 + 2]) * reach[a]
+      + std::sqrt(w[b3] * w[b3] + w[b3 + 1] * w[b3 + 1] + w[b3 + 2] * w[b3 + 2]) * reach[b];
+    return (std::sqrt(dx * dx + dy * dy + dz * dz) + 0.5 * gl * dt + turning) * dt;
+  }
+
+  // keeps(): src/contact.js:516-537.
+  bool keeps(int p, int a, int b, double tolerance) const {
+    const double* pose = &pairs.cachePose[7 * p];
+    double now[7];
+    const int g = relative(a, b, now);
+    const double ex = now[0] - pose[0], ey = now[1] - pose[1], ez = now[2] - pose[2];
+    const double cx = -pose[3], cy = -pose[4], cz = -pose[5], cw = pose[6];
+    const double rx = now[3], ry = now[4], rz = now[5], rw = now[6];
+    const double ux = cw * rx + cx * rw + cy * rz - cz * ry;
+    const double uy = cw * ry + cy * rw + cz * rx - cx * rz;
+    const double uz = cw * rz + cz * rw + cx * ry - cy * rx;
+    const double drift = std::sqrt(ex * ex + ey * ey + ez * ez) + 2 * std::sqrt(ux * ux + uy * uy + uz * uz) * reach[g];
+    if (pairs.cacheLoss[p] + 2 * drift > tolerance) return false;
+    if (jointHead[a] != 0 || jointHead[b] != 0) return false;
+    return pairs.touching[p] == 1 || drift + moving(a, b) <= tolerance;
+  }
+
+  // rounded(): src/contact.js:571-575.
+  double rounded(int s) const { return shape[s] == BG_SPHERE || shape[s] == BG_CAPSULE ? dims[3 * s] : 0; }
+
+  // cored(): src/contact.js:578-585.
+  void cored(int s, double* local) const {
+    if (shape[s] == BG_SPHERE) { local[0] = 0; local[1] = 0; local[2] = 0; return; }
+    if (shape[s] != BG_CAPSULE) return;
+    const double half = (dims[3 * s + 1] - 2 * dims[3 * s]) * 0.5, y = local[1];
+    local[0] = 0; local[1] = y < -half ? -half : y > half ? half : y; local[2] = 0;
+  }
+
+  // reused(): src/contact.js:468-510 (never shifted: no time of impact here).
+  bool reused(int p, int a, int b, double tolerance, double margin, Manifold& mf) const {
+    if (pairs.cached[p] == 0 || !keeps(p, a, b, tolerance)) return false;
+    const int count = pairs.cachePoints[p];
+    const double* A = axes.data();
+    const int a3 = 3 * a, b3 = 3 * b, a9 = 9 * a, b9 = 9 * b;
+    const double* ln = &pairs.cacheNormal[3 * p];
+    const double lx = ln[0], ly = ln[1], lz = ln[2];
+    const double nx = A[a9] * lx + A[a9 + 3] * ly + A[a9 + 6] * lz;
+    const double ny = A[a9 + 1] * lx + A[a9 + 4] * ly + A[a9 + 7] * lz;
+    const double nz = A[a9 + 2] * lx + A[a9 + 5] * ly + A[a9 + 8] * lz;
+    mf.normal[0] = nx; mf.normal[1] = ny; mf.normal[2] = nz;
+    const double ra = rounded(a), rb = -rounded(b);
+    mf.count = count;
+    double least = INF;
+    for (int k = 0; k < count; k++) {
+      const double* l = &pairs.cacheLocal[6 * (P * p + k)];
+      const double ax = l[0], ay = l[1], az = l[2], bx = l[3], by = l[4], bz = l[5];
+      const double pax = position[a3] + A[a9] * ax + A[a9 + 3] * ay + A[a9 + 6] * az + nx * ra;
+      const double pay = position[a3 + 1] + A[a9 + 1] * ax + A[a9 + 4] * ay + A[a9 + 7] * az + ny * ra;
+      const double paz = position[a3 + 2] + A[a9 + 2] * ax + A[a9 + 5] * ay + A[a9 + 8] * az + nz * ra;
+      const double pbx = position[b3] + A[b9] * bx + A[b9 + 3] * by + A[b9 + 6] * bz + nx * rb;
+      const double pby = position[b3 + 1] + A[b9 + 1] * bx + A[b9 + 4] * by + A[b9 + 7] * bz + ny * rb;
+      const double pbz = position[b3 + 2] + A[b9 + 2] * bx + A[b9 + 5] * by + A[b9 + 8] * bz + nz * rb;
+      const double sep = (pbx - pax) * nx + (pby - pay) * ny + (pbz - paz) * nz, half = 0.5 * sep;
+      mf.separations[k] = sep;
+      double* q = &mf.points[3 * k];
+      if (rb != 0) {
+        q[0] = pbx - nx * half; q[1] = pby - ny * half; q[2] = pbz - nz * half;
+      } else if (ra != 0) {
+        q[0] = pax + nx * half; q[1] = pay + ny * half; q[2] = paz + nz * half;
+      } else {
+        q[0] = (pax + pbx) * 0.5; q[1] = (pay + pby) * 0.5; q[2] = (paz + pbz) * 0.5;
+      }
+      mf.ids[k] = pairs.cacheId[P * p + k];
+      if (sep < least) least = sep;
+    }
+    return !(least > margin);   // least(): src/contact.js:684-688
+  }
+
+  // remember(): src/contact.js:540-569, with the manifold collide() just found.
+  void remember(int p, int a, int b, const Manifold& mf) {
+    const int count = mf.count;
+    pairs.cached[p] = 1;
+    pairs.cachePoints[p] = static_cast<uint8_t>(count);
+    relative(a, b, &pairs.cachePose[7 * p]);
+    pairs.cacheLoss[p] = mf.loss;
+    const double* A = axes.data();
+    const int a3 = 3 * a, b3 = 3 * b, a9 = 9 * a, b9 = 9 * b;
+    const double nx = mf.normal[0], ny = mf.normal[1], nz = mf.normal[2];
+    double* ln = &pairs.cacheNormal[3 * p];
+    ln[0] = A[a9] * nx + A[a9 + 1] * ny + A[a9 + 2] * nz;
+    ln[1] = A[a9 + 3] * nx + A[a9 + 4] * ny + A[a9 + 5] * nz;
+    ln[2] = A[a9 + 6] * nx + A[a9 + 7] * ny + A[a9 + 8] * nz;
+    for (int k = 0; k < count; k++) {
+      double* l = &pairs.cacheLocal[6 * (P * p + k)];
+      const double half = 0.5 * mf.separations[k];
+      const double px = mf.points[3 * k], py = mf.points[3 * k + 1], pz = mf.points[3 * k + 2];
+      const double ax = px - nx * half - position[a3], ay = py - ny * half - position[a3 + 1], az = pz - nz * half - position[a3 + 2];
+      const double bx = px + nx * half - position[b3], by = py + ny * half - position[b3 + 1], bz = pz + nz * half - position[b3 + 2];
+      l[0] = A[a9] * ax + A[a9 + 1] * ay + A[a9 + 2] * az;
+      l[1] = A[a9 + 3] * ax + A[a9 + 4] * ay + A[a9 + 5] * az;
+      l[2] = A[a9 + 6] * ax + A[a9 + 7] * ay + A[a9 + 8] * az;
+      l[3] = A[b9] * bx + A[b9 + 1] * by + A[b9 + 2] * bz;
+      l[4] = A[b9 + 3] * bx + A[b9 + 4] * by + A[b9 + 5] * bz;
+      l[5] = A[b9 + 6] * bx + A[b9 + 7] * by + A[b9 + 8] * bz;
+      cored(a, l);
+      cored(b, l + 3);
+      pairs.cacheId[P * p + k] = mf.ids[k];
+    }
+  }
+
   // basis(): src/contact.js:1283-1292.
   void basis(int m) {
     const double nx = c.normal[3 * m], ny = c.normal[3 * m + 1], nz = c.normal[3 * m + 2];
@@ -545,6 +698,12 @@ struct bw_world {
   // The pairs narrow() handed to collide() this step, with the margin and tolerance it passed.
   std::vector<int32_t> narrowA, narrowB;
   std::vector<double> narrowMargin, narrowTol;
+  // The pairs whose boxes meet (listPairs), and for the two-pass walk which of them kept their
+  // manifold (nmKept) and where the others are in the list handed to the narrowphase.
+  std::vector<int32_t> listA, listB, nmSent;
+  std::vector<double> listMargin, listTol;
+  std::vector<Manifold> nmKept;
+  bool reuse = false;   // the kept-manifold cache (REUSE) on
 
   // narrow() with the narrowphase itself on another device (bw_set_narrowphase): the same walk
   // over the pairs (src/contact.js:312-327), in two passes.  The first drops the pairs whose fat
@@ -556,7 +715,7 @@ struct bw_world {
   // The first pass: the list of pairs whose boxes meet, each with its slot, margin, tolerance and
   // contact record (nmRecord, for bw_set_contact_step).
   void listPairs() {
-    narrowA.clear(); narrowB.clear(); narrowMargin.clear(); narrowTol.clear(); nmPair.clear(); nmRecord.clear();
+    listA.clear(); listB.clear(); listMargin.clear(); listTol.clear(); nmPair.clear(); nmRecord.clear();
     for (int p = 0; p < pairs.active;) {
       const int a = pairs.a[p], b = pairs.b[p];
       if (!fatOverlap(a, b)) {
@@ -569,8 +728,8 @@ struct bw_world {
           || box[b6 + 1] > box[a6 + 4] || box[a6 + 2] > box[b6 + 5] || box[b6 + 2] > box[a6 + 5]) {
         pairs.forget(p);
       } else {
-        narrowA.push_back(a); narrowB.push_back(b); narrowMargin.push_back(motion[a] + motion[b] + tol);
-        narrowTol.push_back(tol); nmPair.push_back(p); nmRecord.push_back(pairs.record[p]);
+        listA.push_back(a); listB.push_back(b); listMargin.push_back(motion[a] + motion[b] + tol);
+        listTol.push_back(tol); nmPair.push_back(p); nmRecord.push_back(pairs.record[p]);
       }
       p++;
     }
@@ -578,6 +737,18 @@ struct bw_world {
 
   int narrowOnDevice() {
     listPairs();
+    // The pairs that keep their manifold (reused(), src/contact.js:356) need no narrowphase; the
+    // rest go to the device, in list order.
+    const size_t listed = listA.size();
+    narrowA.clear(); narrowB.clear(); narrowMargin.clear(); narrowTol.clear();
+    nmSent.assign(listed, -1);
+    nmKept.resize(listed);
+    for (size_t i = 0; i < listed; i++) {
+      if (reuse && reused(nmPair[i], listA[i], listB[i], listTol[i], listMargin[i], nmKept[i])) continue;
+      nmSent[i] = static_cast<int32_t>(narrowA.size());
+      narrowA.push_back(listA[i]); narrowB.push_back(listB[i]);
+      narrowMargin.push_back(listMargin[i]); narrowTol.push_back(listTol[i]);
+    }
     const size_t n = narrowA.size();
     nmPoints.resize(std::max<size_t>(n, 1)); nmPid.resize(P * std::max<size_t>(n, 1));
     nmNormal.resize(3 * std::max<size_t>(n, 1)); nmPoint.resize(3 * P * std::max<size_t>(n, 1));
@@ -592,27 +763,36 @@ struct bw_world {
       if (rc != BG_OK) return rc;
     }
     Manifold mf;
-    for (size_t i = 0; i < n; i++) {
+    for (size_t i = 0; i < listed; i++) {
       const int p = nmPair[i];
-      const int count = nmPoints[i];
+      const int j = nmSent[i];
+      if (j < 0) {
+        const int m = emit(p, listA[i], listB[i], nmKept[i], listTol[i]);
+        carry(p, m);
+        continue;
+      }
+      const int count = nmPoints[j];
       if (count == 0) {
         pairs.forget(p);
         continue;
       }
       mf.count = count;
-      for (int k = 0; k < 3; k++) mf.normal[k] = nmNormal[3 * i + k];
+      mf.loss = 0;   // collide() of boxes, spheres and capsules falls short of nothing
+      for (int k = 0; k < 3; k++) mf.normal[k] = nmNormal[3 * j + k];
       for (int k = 0; k < count; k++) {
-        for (int q = 0; q < 3; q++) mf.points[3 * k + q] = nmPoint[3 * (P * i + k) + q];
-        mf.separations[k] = nmSeparation[P * i + k];
-        mf.ids[k] = nmPid[P * i + k];
+        for (int q = 0; q < 3; q++) mf.points[3 * k + q] = nmPoint[3 * (P * j + k) + q];
+        mf.separations[k] = nmSeparation[P * j + k];
+        mf.ids[k] = nmPid[P * j + k];
       }
-      const int m = emit(p, narrowA[i], narrowB[i], mf, narrowTol[i]);
+      if (reuse) remember(p, listA[i], listB[i], mf);
+      const int m = emit(p, listA[i], listB[i], mf, listTol[i]);
       carry(p, m);
     }
     return BG_OK;
   }
 
-  // narrow(): src/contact.js:296-327 with find() 334-368 (no reuse cache, no time of impact).
+  // narrow(): src/contact.js:296-327 with find() 334-368 (the reuse cache when `reuse` is on; no
+  // time of impact).  narrowA.. list the pairs handed to collide().
   void narrow() {
     Shape sa, sb;
     Manifold mf;
@@ -632,12 +812,16 @@ struct bw_world {
         met = false;
       } else {
         const double margin = motion[a] + motion[b] + tol;
-        narrowA.push_back(a); narrowB.push_back(b); narrowMargin.push_back(margin); narrowTol.push_back(tol);
-        load(a, sa);
-        load(b, sb);
-        if (bearing::collide(sa, sb, margin, tol, mf) == 0) {
-          pairs.forget(p);
-          met = false;
+        if (!(reuse && reused(p, a, b, tol, margin, mf))) {
+          narrowA.push_back(a); narrowB.push_back(b); narrowMargin.push_back(margin); narrowTol.push_back(tol);
+          load(a, sa);
+          load(b, sb);
+          if (bearing::collide(sa, sb, margin, tol, mf) == 0) {
+            pairs.forget(p);
+            met = false;
+          } else if (reuse) {
+            remember(p, a, b, mf);
+          }
         }
       }
       if (met) {
@@ -774,15 +958,16 @@ struct bw_world {
     c.solved = 0;
     std::fill(c.starts, c.starts + COLOURS + 3, 0);
     listPairs();
+    narrowA = listA; narrowB = listB; narrowMargin = listMargin; narrowTol = listTol;
     const size_t np = narrowA.size();
     nmPoints.assign(std::max<size_t>(np, 1), 0);
     nmTouching.assign(std::max<size_t>(np, 1), 0);
     bg_bodies B;
     fillBodies(&B);
-    const bg_materials M = {friction.data(), restitution.data(), size.data()};
+    const bg_materials M = {friction.data(), restitution.data(), size.data(), reach.data()};
     const bg_contact_pairs CP = {{static_cast<int32_t>(np), narrowA.data(), narrowB.data(), narrowMargin.data(),
                                   narrowTol.data()},
-                                 nmRecord.data()};
+                                 nmRecord.data(), reuse ? 1 : 0};
     bg_step S;
     S.dt = dt;
     S.substeps = substeps;
@@ -847,6 +1032,7 @@ bw_world* bw_create(const bw_options* options) {
   if (options != nullptr) {
     for (int k = 0; k < 3; k++) w->gravity[k] = options->gravity[k];
     w->substeps = options->substeps > 0 ? options->substeps : 8;
+    w->reuse = options->reuse != 0;
   }
   w->c.alloc(0);
   return w;

@@ -28,7 +28,7 @@ DEFAULTS = dict(
     angularVelocity=(0.0, 0.0, 0.0),
 )
 BODY_OPTIONS = set(DEFAULTS)
-WORLD_OPTIONS = {"gravity", "substeps", "sleeping", "workers"}
+WORLD_OPTIONS = {"gravity", "substeps", "sleeping", "workers", "reuse"}
 
 
 class BearingError(RuntimeError):
@@ -90,7 +90,9 @@ class World:
             raise BearingError("World: sleeping islands are not on this path; pass sleeping: false")
         self._workers = o.get("workers", "auto")
         self._lib = _ffi.host()
-        opts = _ffi.Options((C.c_double * 3)(*g), substeps)
+        # reuse: the kept-manifold cache of src/contact.js:388-595 (the reference always keeps one;
+        # off by default here, where every pair whose boxes meet is collided afresh each step)
+        opts = _ffi.Options((C.c_double * 3)(*g), substeps, 1 if o.get("reuse", False) else 0)
         self._w = self._lib.bw_create(C.byref(opts))
         self._count = 0
         self._solver = None

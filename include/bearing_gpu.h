@@ -430,11 +430,15 @@ typedef struct bg_materials {
   const double* friction;      /* per slot: World._friction */
   const double* restitution;   /* per slot: World._restitution */
   const double* size;          /* per slot: World._size (a row's patch, src/contact.js:906) */
+  const double* reach;         /* per slot: World._reach (read only with reuse on) */
 } bg_materials;
 
 typedef struct bg_contact_pairs {
   bg_pairs list;               /* the pairs whose boxes meet, in pair order (src/contact.js:312-327) */
   const int32_t* memory;       /* per pair: its record in the previous call's list, or -1 */
+  int32_t reuse;               /* nonzero: a pair whose record keeps a manifold reuses it while
+                                  the bodies barely move (src/contact.js:388-595 reused/keeps) and
+                                  a fresh manifold is kept (remember); records hold the manifolds */
 } bg_contact_pairs;
 
 typedef struct bg_contact_result {

@@ -30,6 +30,8 @@ typedef struct bw_world bw_world;
 typedef struct bw_options {
   double gravity[3];
   int32_t substeps;
+  int32_t reuse;               /* nonzero: keep touching pairs' manifolds and reuse them while the
+                                  bodies barely move against each other (src/contact.js:388-595) */
 } bw_options;
 
 /* addBody's spec for a box, sphere or capsule (src/world.js:190-221 defaults). */

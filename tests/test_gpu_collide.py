@@ -105,12 +105,14 @@ def test_refusals_write_nothing():
     w.destroy()
 
 
+@pytest.mark.parametrize("reuse", [False, True], ids=["fresh", "reuse"])
 @pytest.mark.parametrize("build,steps", [(pile3000, 60), (rain, 80)], ids=["pile3000", "rain300"])
-def test_a_world_stepping_with_the_device_narrowphase_is_the_same_world(build, steps):
+def test_a_world_stepping_with_the_device_narrowphase_is_the_same_world(build, steps, reuse):
     # bw_set_narrowphase: each step's pairs go to bg_collide, and the step emits and carries its
-    # manifolds; the state after every step equals the host narrowphase's, bit for bit.
-    a = World({}, solver=oracle_io.solver(0))
-    b = World({}, solver=oracle_io.solver(0))
+    # manifolds; the state after every step equals the host narrowphase's, bit for bit, with the
+    # kept-manifold cache on as well (the pairs that keep theirs stay on the host).
+    a = World({"reuse": reuse}, solver=oracle_io.solver(0))
+    b = World({"reuse": reuse}, solver=oracle_io.solver(0))
     build(a)
     build(b)
     device = GpuSolver()

@@ -36,19 +36,19 @@ def _same(x, y):
     return x.tobytes() == y.tobytes()
 
 
-def oracle_world(workers=0):
-    return World({}, solver=oracle_io.solver(workers))
+def oracle_world(workers=0, options=None):
+    return World(options or {}, solver=oracle_io.solver(workers))
 
 
-def device_world():
-    w = World({})
+def device_world(options=None):
+    w = World(options or {})
     w.set_contact_step(w._solver)
     return w
 
 
-def step_pair(build, steps, every=1, workers=0):
+def step_pair(build, steps, every=1, workers=0, options=None):
     """Steps both worlds `steps` times, comparing them at every `every`-th step and the last."""
-    wa, wb = oracle_world(workers), device_world()
+    wa, wb = oracle_world(workers, options), device_world(options)
     build(wa)
     build(wb)
     most = 0
@@ -140,6 +140,51 @@ def test_the_50k_pile_120_steps():
     # host threads on the other side.
     most, ms = step_pair(lambda w: scenes.pile(w, count=50_000, seed=50_000), 120, every=20, workers=16)
     assert most > 60_000 and ms is not None
+
+
+# ---- with the kept-manifold cache (src/contact.js:388-595), kept in the device's records ----
+
+REUSE = {"reuse": True}
+
+
+def test_pyramid_reusing_kept_manifolds():
+    most, _ = step_pair(scenes.pyramid, 200, options=REUSE)
+    assert most > 200
+
+
+def test_tumbling_and_kinematic_reusing_kept_manifolds():
+    def build(w):
+        scenes.ground(w, friction=0.6)
+        w.addBody({"type": "kinematic", "size": (6.0, 0.4, 6.0), "position": (0.0, 1.0, 0.0),
+                   "velocity": (0.3, 0.0, 0.0), "angularVelocity": (0.0, 0.4, 0.0)})
+        rng = np.random.default_rng(5)
+        for i in range(30):
+            q = rng.standard_normal(4)
+            q = tuple(float(x) for x in q / np.linalg.norm(q))
+            pos = (float(rng.uniform(-2.5, 2.5)), float(1.8 + 0.6 * i), float(rng.uniform(-2.5, 2.5)))
+            if i % 3 == 0:
+                w.addBody({"shape": "capsule", "radius": 0.2, "height": 0.9, "rotation": q, "position": pos})
+            elif i % 3 == 1:
+                w.addBody({"shape": "sphere", "radius": 0.3, "position": pos, "restitution": 0.3})
+            else:
+                w.addBody({"size": (0.6, 0.4, 0.5), "rotation": q, "position": pos})
+    step_pair(build, 150, options=REUSE)
+
+
+def test_rain_reusing_kept_manifolds():
+    most, _ = step_pair(lambda w: scenes.rain(w, count=2000, seed=2000), 300, every=10, options=REUSE)
+    assert most > 1000
+
+
+def test_mixed_pile_3000_reusing_kept_manifolds():
+    most, _ = step_pair(lambda w: scenes.pile(w, count=3000, seed=5, extent=30.0), 100, every=5, options=REUSE)
+    assert most > 2000
+
+
+def test_the_50k_pile_reusing_kept_manifolds():
+    most, _ = step_pair(lambda w: scenes.pile(w, count=50_000, seed=50_000), 120, every=20, workers=16,
+                        options=REUSE)
+    assert most > 60_000
 
 
 # ---- the C ABI directly ----

@@ -79,10 +79,12 @@ NARROWPHASE = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(_ffi.Bodies), C.POINT
                           C.POINTER(_ffi.Pairs), C.POINTER(_ffi.Manifolds))
 
 
+@pytest.mark.parametrize("reuse", [False, True], ids=["fresh", "reuse"])
 @pytest.mark.parametrize("build,steps", [(boxes_and_balls, 60), (raining, 100)], ids=["pile600", "rain150"])
-def test_a_world_with_its_narrowphase_handed_out_is_the_same_world(build, steps):
+def test_a_world_with_its_narrowphase_handed_out_is_the_same_world(build, steps, reuse):
     # bw_set_narrowphase with the host's own narrowphase behind it (what bg_collide computes on
-    # the device, bit for bit): the two-pass walk over the pairs gives the same world, step by step.
+    # the device, bit for bit): the two-pass walk over the pairs gives the same world, step by step,
+    # with the kept-manifold cache on as well (the pairs that keep theirs are not handed out).
     host = _ffi.host()
     calls = []
 
@@ -91,8 +93,8 @@ def test_a_world_with_its_narrowphase_handed_out_is_the_same_world(build, steps)
         return host.bw_collide_pairs(bodies, gravity, pairs, out, 2)
 
     hook = NARROWPHASE(collide)
-    a = World({}, solver=oracle_io.solver(0))
-    b = World({}, solver=oracle_io.solver(0))
+    a = World({"reuse": reuse}, solver=oracle_io.solver(0))
+    b = World({"reuse": reuse}, solver=oracle_io.solver(0))
     build(a)
     build(b)
     assert host.bw_set_narrowphase(b._w, C.cast(hook, C.c_void_p), None) == 0
