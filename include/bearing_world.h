@@ -11,7 +11,8 @@
  * with the signature of bg_solve_step (bearing_gpu.h): the GPU library, or any other.
  *
  * Not covered (a world using them is refused): hulls, compounds, meshes, heightfields, joints,
- * characters, sensors, sleeping islands, the time-of-impact sweep and the contact-reuse cache.
+ * characters, sensors, sleeping islands and the time-of-impact sweep.  The contact-reuse cache
+ * (src/contact.js:388-595) is an option (bw_options.reuse), off by default.
  */
 #ifndef BEARING_WORLD_H
 #define BEARING_WORLD_H
