@@ -341,11 +341,11 @@ int64_t bg_backward_bytes(const bg_ctx* ctx);
  * BG_STATIC_MAX_BODIES slots and BG_STATIC_MAX_ROWS rows, and larger ones are refused with
  * BG_EINVAL (use bg_solve_step for those).  The first call on a device looks up that array's
  * device address with the device current, in the device's primary context (the CUDA runtime's
- * own), and keeps it for later calls on that device; make that first call before any stream
- * capture, and do not call this again on a device after cudaDeviceReset.  All calls share the one
- * array: calls that overlap on the GPU (other streams, other host threads) race, so run them one
- * after another.  Each call waits for `stream` to finish its work before it returns.  It calls no
- * cudaMalloc or cudaFree.
+ * own), and keeps it for later calls on that device; do not call this again on a device after
+ * cudaDeviceReset.  All calls share the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race, so run them one after another.  Each call synchronises `stream`
+ * before it returns (it reads the kernel's status back), so no call can be captured into a CUDA
+ * graph.  It calls no cudaMalloc or cudaFree.
  * The counts and colour starts are checked on the host as bg_solve_step checks them; the index
  * columns (device memory) are checked by the kernel before it writes anything.  Either refusal
  * returns BG_EINVAL and leaves the caller's arrays untouched.  Otherwise it returns BG_OK,
