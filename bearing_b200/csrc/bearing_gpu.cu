@@ -2660,9 +2660,27 @@ __global__ void collide_starts(CollideParams c) {
   }
 }
 
+// Each block places a chunk of pairs at a time: a place in the block's share of each class from a
+// shared-memory count, and one global add per class a block for the share itself (the order
+// within a class changes no manifold: each pair's is its own).
 __global__ void collide_scatter(CollideParams c) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x)
-    if (c.skip == nullptr || c.skip[i] == 0) c.order[atomicAdd(&c.counts[kPairClasses + pair_class(c, i)], 1)] = i;
+  __shared__ int local[kPairClasses], base[kPairClasses];
+  for (int i0 = blockIdx.x * blockDim.x; i0 < c.n; i0 += gridDim.x * blockDim.x) {
+    if (threadIdx.x < kPairClasses) local[threadIdx.x] = 0;
+    __syncthreads();
+    const int i = i0 + threadIdx.x;
+    int cls = -1, at = 0;
+    if (i < c.n && (c.skip == nullptr || c.skip[i] == 0)) {
+      cls = pair_class(c, i);
+      at = atomicAdd(&local[cls], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < kPairClasses)
+      base[threadIdx.x] = local[threadIdx.x] > 0 ? atomicAdd(&c.counts[kPairClasses + threadIdx.x], local[threadIdx.x]) : 0;
+    __syncthreads();
+    if (cls >= 0) c.order[base[cls] + at] = i;
+    __syncthreads();
+  }
 }
 
 // load(): src/contact.js:1244-1276, for boxes, spheres and capsules, with the axes of
@@ -2898,6 +2916,15 @@ bool colour_block(bg_ctx* c, size_t nb, size_t n) {
   return true;
 }
 
+// Exclusive scan of in[0..n) into out[0..n] (out[n] the total) on the stream, across blocks (n > 0;
+// `tiles` holds n / kTile + 2 entries).  in and out may be the same array.
+void scan_into(cudaStream_t st, const int32_t* in, int32_t* out, int n, int32_t* tiles) {
+  const int ntiles = (n + bgcol::kTile - 1) / bgcol::kTile;
+  bgcol::col_tile_sums<<<ntiles, bgcol::kScanThreads, 0, st>>>(in, n, tiles);
+  bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(tiles, tiles, ntiles);
+  bgcol::col_tile_scan<<<ntiles, bgcol::kScanThreads, 0, st>>>(in, out, n, tiles);
+}
+
 // colour() and arrange()'s order for p.n manifolds over p.nb slots, queued on the context's
 // stream (p's arrays zeroed as colour_layout() says; `tiles` holds kRuns * nb / kTile + 2).
 bool colour_kernels(bg_ctx* c, bgcol::ColourParams& p, int32_t* tiles) {
@@ -2907,7 +2934,7 @@ bool colour_kernels(bg_ctx* c, bgcol::ColourParams& p, int32_t* tiles) {
   const int body_grid = std::max(1, std::min(static_cast<int>((nb + 255) / 256), 8 * c->sms));
   const int bin_grid = std::max(1, std::min(static_cast<int>((bgcol::kRuns * nb + 255) / 256), 8 * c->sms));
   bgcol::col_degrees<<<rows_grid, 256, 0, st>>>(p);
-  bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(p.deg, p.off, static_cast<int>(nb));
+  scan_into(st, p.deg, p.off, static_cast<int>(nb), tiles);
   bgcol::col_fill<<<rows_grid, 256, 0, st>>>(p);
   bgcol::col_ranks<<<body_grid, 256, 0, st>>>(p);
   {
@@ -2927,7 +2954,7 @@ bool colour_kernels(bg_ctx* c, bgcol::ColourParams& p, int32_t* tiles) {
   bgcol::col_scatter<<<rows_grid, 256, 0, st>>>(p);
   bgcol::col_settle<<<bin_grid, 256, 0, st>>>(p);
   bgcol::col_starts<<<1, 64, 0, st>>>(p);
-  c->last_launches += 12;
+  c->last_launches += 14;
   return cuda_ok(c, cudaGetLastError(), "colour launch");
 }
 
@@ -3082,7 +3109,7 @@ ContactLayout contact_layout(unsigned char* base, size_t nb, size_t np) {
   L.counts = k.take<int32_t>(2 * kPairClasses); L.corder = k.take<int32_t>(np);
   L.points = k.take<uint8_t>(np); L.normal = k.take<double>(3 * np); L.point = k.take<double>(3 * bg::P * np);
   L.separation = k.take<double>(bg::P * np); L.pid = k.take<uint32_t>(bg::P * np);
-  L.rowof = k.take<int32_t>(np + 1); L.scan_tiles = k.take<int32_t>(np / bgcol::kTile + 2);
+  L.rowof = k.take<int32_t>(np + 1); L.scan_tiles = k.take<int32_t>(std::max(np, nb) / bgcol::kTile + 2);
   bgct::FoundRows& r = L.r;
   r.row = k.take<int32_t>(np); r.a = k.take<int32_t>(np); r.b = k.take<int32_t>(np); r.pair = k.take<int32_t>(np);
   r.points = k.take<uint8_t>(np); r.pid = k.take<uint32_t>(bg::P * np);
@@ -3190,14 +3217,6 @@ bool contact_blocks(bg_ctx* c, size_t nb, size_t np) {
   if (d.ev[0] == nullptr)
     for (cudaEvent_t& e : d.ev) cudaEventCreate(&e);
   return true;
-}
-
-// Exclusive scan of in[0..n) into out[0..n] (out[n] the total) on the stream, across blocks.
-void scan_into(cudaStream_t st, const int32_t* in, int32_t* out, int n, int32_t* tiles) {
-  const int ntiles = (n + bgcol::kTile - 1) / bgcol::kTile;
-  bgcol::col_tile_sums<<<ntiles, bgcol::kScanThreads, 0, st>>>(in, n, tiles);
-  bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(tiles, tiles, ntiles);
-  bgcol::col_tile_scan<<<ntiles, bgcol::kScanThreads, 0, st>>>(in, out, n, tiles);
 }
 
 // What the host checks before anything is copied: every index a kernel addresses memory with.
@@ -3379,11 +3398,11 @@ int32_t bg_contact_step(bg_ctx* c, const bg_bodies* B, const bg_materials* M, co
     op.perm = c->perm_dev; op.iperm = c->iperm_dev; op.groups = L.groups; op.chunks = c->chunks_dev;
     op.chunk_base = L.chunk_base;
     bgct::ct_order_count<<<op.tiles, bgct::kOrderThreads, 0, st>>>(op);
-    bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(L.ocounts, L.ocounts, bgct::kKeys * op.tiles);
+    scan_into(st, L.ocounts, L.ocounts, bgct::kKeys * op.tiles, L.scan_tiles);
     bgct::ct_order_place<<<op.tiles, bgct::kOrderThreads, 0, st>>>(op);
-    bgct::ct_order_runs<<<1, 32, 0, st>>>(op);
+    bgct::ct_order_runs<<<1, bgct::kRunThreads, 0, st>>>(op);
     bgct::ct_order_chunks<<<rgrid, 256, 0, st>>>(op);
-    c->last_launches += 7;
+    c->last_launches += 9;
     if (!cuda_ok(c, cudaGetLastError(), "bg_contact_step launch")) return BG_ECUDA;
     // the host waits for what the stage's launch needs
     if (!fetch(sum, CL.starts, sizeof(int32_t) * bg::NSTARTS, "bg_contact_step") ||
@@ -3423,10 +3442,10 @@ int32_t bg_contact_step(bg_ctx* c, const bg_bodies* B, const bg_materials* M, co
     const int rgrid = std::max(1, std::min((nrows + 255) / 256, 8 * c->sms));
     const int bgrid = std::max(1, std::min((nb + 255) / 256, 8 * c->sms));
     bgct::ct_flow_degrees<<<rgrid, 256, 0, st>>>(f);
-    bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(c->deg_dev, L.off, nb);
+    scan_into(st, c->deg_dev, L.off, nb, L.scan_tiles);
     bgct::ct_flow_fill<<<rgrid, 256, 0, st>>>(f);
     bgct::ct_flow_ranks<<<bgrid, 256, 0, st>>>(f);
-    c->last_launches += 4;
+    c->last_launches += 6;
   }
   c->nchunks = nchunks;
   c->chunks.clear();

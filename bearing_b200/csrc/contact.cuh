@@ -447,16 +447,23 @@ __global__ void __launch_bounds__(kOrderThreads) ct_order_place(OrderParams p) {
 
 // Each key's first device row, and the runs the grid's dataflow takes: each colour's rows of one
 // point count in runs of 32 (the last shorter), then the overflow's rows one a run, in order (as
-// the host's order_rows() makes them).  One thread.
-__global__ void ct_order_runs(OrderParams p) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// the host's order_rows() makes them).  One block: a thread a key, then one thread adds them up.
+constexpr int kRunThreads = 160;
+__global__ void __launch_bounds__(kRunThreads) ct_order_runs(OrderParams p) {
+  __shared__ int32_t runs_of[kKeys];
+  const int k = threadIdx.x;
+  if (k < kKeys) {
+    const int first = p.counts[k * p.tiles];
+    const int size = (k + 1 < kKeys ? p.counts[(k + 1) * p.tiles] : p.n) - first;
+    p.groups[k] = first;
+    runs_of[k] = k < 128 ? (size + 31) / 32 : k == 128 ? size : 0;
+  }
+  __syncthreads();
+  if (k != 0) return;
   int runs = 0;
-  for (int k = 0; k < kKeys; k++) {
-    p.groups[k] = p.counts[k * p.tiles];
-    p.chunk_base[k] = runs;
-    const int size = (k + 1 < kKeys ? p.counts[(k + 1) * p.tiles] : p.n) - p.groups[k];
-    if (k < 128) runs += (size + 31) / 32;
-    else if (k == 128) runs += size;
+  for (int j = 0; j < kKeys; j++) {
+    p.chunk_base[j] = runs;
+    runs += runs_of[j];
   }
   p.groups[kKeys] = p.n;
   p.chunk_base[kKeys] = runs;
