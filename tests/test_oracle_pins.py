@@ -354,3 +354,56 @@ def test_spun_about_its_middle_axis_a_box_flips(k, flips):
         w.step(DT)
         lowest = min(lowest, rotation_matrix(col(w, "rotation", body, 4))[k, k])
     assert (lowest < -0.99) if flips else (lowest > 0.99), f"axis {k}: lowest {lowest}"
+
+
+# ---- the World's own (test/world.test.js) ----
+
+def test_mass_is_density_times_volume_for_every_shape():
+    w = world()
+    r, h = 0.3, 1.8
+    box = w.addBody({"size": (2.0, 3.0, 4.0), "density": 10.0})
+    sphere = w.addBody({"shape": "sphere", "radius": r})
+    capsule = w.addBody({"shape": "capsule", "radius": r, "height": h})
+    given = w.addBody({"shape": "capsule", "mass": 80.0})
+    assert body_mass(w, box) == 240
+    near(body_mass(w, sphere), 1000 * (4 / 3) * math.pi * r ** 3, 1e-9, "sphere")
+    near(body_mass(w, capsule), 1000 * (math.pi * r * r * (h - 2 * r) + (4 / 3) * math.pi * r ** 3), 1e-9, "capsule")
+    assert body_mass(w, given) == 80
+
+
+def test_static_stays_put_and_kinematic_moves_at_its_velocity_ignoring_gravity():
+    w = world()
+    ground_slot = w.addBody({"type": "static", "position": (0.0, -1.0, 0.0)})
+    lift = w.addBody({"type": "kinematic", "velocity": (0.0, 2.0, 0.0)})
+    for _ in range(30):
+        w.step(DT)
+    assert list(col(w, "position", ground_slot, 3)) == [0.0, -1.0, 0.0]
+    assert np.max(np.abs(col(w, "position", lift, 3) - np.array([0.0, 1.0, 0.0]))) <= 1e-14
+    assert list(col(w, "velocity", lift, 3)) == [0.0, 2.0, 0.0]
+
+
+def test_angular_velocity_turns_a_body_about_the_world_axis_it_names():
+    w = world({"gravity": (0.0, 0.0, 0.0)})
+    body = w.addBody({"angularVelocity": (0.0, math.pi, 0.0)})
+    for _ in range(600):
+        w.step(1 / 600)   # half a turn
+    x, y, z, s = col(w, "rotation", body, 4)
+    assert np.max(np.abs(np.array([x, abs(y), z, s]) - np.array([0.0, 1.0, 0.0, 0.0]))) <= 2e-3
+    assert abs(math.sqrt(x * x + y * y + z * z + s * s) - 1) <= 1e-15
+
+
+def test_a_step_does_what_it_did_before_bit_for_bit():
+    def run():
+        w = world()
+        for i in range(50):
+            axis = np.array([1.0, i, -i / 2])
+            axis /= np.linalg.norm(axis)
+            half = i * 0.7 / 2
+            q = (axis[0] * math.sin(half), axis[1] * math.sin(half), axis[2] * math.sin(half), math.cos(half))
+            w.addBody({"shape": ("box", "sphere", "capsule")[i % 3], "position": (i * 0.37, i * 1.1, -i * 0.13),
+                       "velocity": (math.sqrt(i), 1 / (i + 1), -i / 7), "angularVelocity": (i / 3, -i / 5, i / 11),
+                       "rotation": q})
+        for _ in range(240):
+            w.step(DT)
+        return w.transforms.tobytes()
+    assert run() == run()
