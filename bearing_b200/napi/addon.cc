@@ -67,7 +67,7 @@ napi_value Create(napi_env env, napi_callback_info info) {
 // World's and Contacts' own typed arrays as bg_bodies / bg_rows; false (with an exception
 // pending) if one is missing or of the wrong type.  sliding, anchorA and anchorB stay NULL: after
 // the stage only slipped() reads them, and the device runs it (src/contact.js:1122-1182).
-bool views(napi_env env, napi_value w, napi_value c, bg_bodies& B, bg_rows& R) {
+void bodies(napi_env env, napi_value w, bg_bodies& B) {
   std::memset(&B, 0, sizeof B);
   B.capacity = number(env, w, "_capacity");
   B.awake_count = number(env, w, "_awakeCount");
@@ -95,6 +95,10 @@ bool views(napi_env env, napi_value w, napi_value c, bg_bodies& B, bg_rows& R) {
   B.framed = static_cast<const uint8_t*>(column(env, w, "_framed", napi_uint8_array));
   B.lock = static_cast<const uint8_t*>(column(env, w, "_lock", napi_uint8_array));
   B.joint_head = static_cast<const int32_t*>(column(env, w, "_jointHead", napi_int32_array));
+}
+
+bool views(napi_env env, napi_value w, napi_value c, bg_bodies& B, bg_rows& R) {
+  bodies(env, w, B);
   std::memset(&R, 0, sizeof R);
   R.count = number(env, c, "count");
   R.solved = number(env, c, "solved");
@@ -176,6 +180,75 @@ napi_value RegisterHost(napi_env env, napi_callback_info info) {
   return out;
 }
 
+void set_int(napi_env env, napi_value obj, const char* name, int32_t v) {
+  napi_value x;
+  napi_create_int32(env, v, &x);
+  napi_set_named_property(env, obj, name, x);
+}
+
+// contactStep(ctx, world, list, dt, substeps, out) -> 0 or a BG_E* code: the step's whole contact
+// side on the device (bg_contact_step).  list: {count, a, b, margin, tolerance, memory, reuse},
+// the pairs narrow() reaches meet() with and each one's record; out: {points, touching} typed
+// arrays of list.count, and on return rows, solved, pointsSolved and starts.
+napi_value ContactStep(napi_env env, napi_callback_info info) {
+  size_t argc = 6;
+  napi_value argv[6];
+  napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr);
+  if (argc < 6) return fail(env, "contactStep(ctx, world, list, dt, substeps, out)");
+  bg_ctx* ctx = nullptr;
+  napi_get_value_external(env, argv[0], reinterpret_cast<void**>(&ctx));
+  napi_value w = argv[1], l = argv[2], o = argv[5];
+  bg_bodies B;
+  bodies(env, w, B);
+  bg_materials M;
+  M.friction = static_cast<const double*>(column(env, w, "_friction", napi_float64_array));
+  M.restitution = static_cast<const double*>(column(env, w, "_restitution", napi_float64_array));
+  M.size = static_cast<const double*>(column(env, w, "_size", napi_float64_array));
+  M.reach = static_cast<const double*>(column(env, w, "_reach", napi_float64_array));
+  bg_contact_pairs P;
+  P.list.count = number(env, l, "count");
+  P.list.a = static_cast<const int32_t*>(column(env, l, "a", napi_int32_array));
+  P.list.b = static_cast<const int32_t*>(column(env, l, "b", napi_int32_array));
+  P.list.margin = static_cast<const double*>(column(env, l, "margin", napi_float64_array));
+  P.list.tolerance = static_cast<const double*>(column(env, l, "tolerance", napi_float64_array));
+  P.memory = static_cast<const int32_t*>(column(env, l, "memory", napi_int32_array));
+  P.reuse = number(env, l, "reuse");
+  bg_contact_result R;
+  std::memset(&R, 0, sizeof R);
+  R.points = static_cast<uint8_t*>(column(env, o, "points", napi_uint8_array));
+  R.touching = static_cast<uint8_t*>(column(env, o, "touching", napi_uint8_array));
+  bool pending = false;
+  napi_is_exception_pending(env, &pending);
+  if (pending) return nullptr;
+  bg_step S;
+  napi_get_value_double(env, argv[3], &S.dt);
+  napi_get_value_int32(env, argv[4], &S.substeps);
+  napi_value g;
+  napi_get_named_property(env, w, "_gravity", &g);
+  for (uint32_t k = 0; k < 3; k++) {
+    napi_value x;
+    napi_get_element(env, g, k, &x);
+    napi_get_value_double(env, x, &S.gravity[k]);
+  }
+  const int32_t rc = bg_contact_step(ctx, &B, &M, &P, &S, &R);
+  if (rc == BG_OK) {
+    set_int(env, o, "rows", R.rows);
+    set_int(env, o, "solved", R.solved);
+    set_int(env, o, "pointsSolved", R.points_solved);
+    napi_value starts;
+    napi_create_array_with_length(env, BG_STARTS, &starts);
+    for (uint32_t k = 0; k < BG_STARTS; k++) {
+      napi_value x;
+      napi_create_int32(env, R.starts[k], &x);
+      napi_set_element(env, starts, k, x);
+    }
+    napi_set_named_property(env, o, "starts", starts);
+  }
+  napi_value out;
+  napi_create_int32(env, rc, &out);
+  return out;
+}
+
 napi_value LastError(napi_env env, napi_callback_info info) {
   size_t argc = 1;
   napi_value argv[1];
@@ -192,6 +265,7 @@ napi_value Init(napi_env env, napi_value exports) {
       {"create", nullptr, Create, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"solveStep", nullptr, SolveStep, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"registerHost", nullptr, RegisterHost, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"contactStep", nullptr, ContactStep, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"lastError", nullptr, LastError, nullptr, nullptr, nullptr, napi_default, nullptr},
   };
   napi_define_properties(env, exports, sizeof props / sizeof props[0], props);
