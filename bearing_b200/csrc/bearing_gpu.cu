@@ -3252,8 +3252,25 @@ int contact_problem(bg_ctx* c, const bg_bodies* B, const bg_materials* M, const 
     set_error(c, "bg_contact_step: bodies.awake_list must be given");
     return BG_EINVAL;
   }
+  // The pairs are checked in chunks on the host pool; the first bad pair in list order is reported.
   const int32_t records = c->ct.count;
-  for (int64_t i = 0; i < np; i++) {
+  constexpr int64_t kChunk = 16384;
+  const int chunks = static_cast<int>((np + kChunk - 1) / kChunk);
+  std::vector<int64_t> first_bad(static_cast<size_t>(chunks), -1);
+  pool_of(c)->run(chunks, [&](int k) {
+    for (int64_t i = k * kChunk; i < std::min(np, (k + 1) * kChunk); i++) {
+      const int32_t a = CP->list.a[i], b = CP->list.b[i], j = CP->memory[i];
+      bool bad = a < 0 || a >= nb || b < 0 || b >= nb || a == b || j < -1 || j >= records;
+      if (!bad)
+        for (const int32_t s : {a, b}) bad = bad || (B->shape[s] != BG_BOX && B->shape[s] != BG_SPHERE && B->shape[s] != BG_CAPSULE);
+      if (bad) {
+        first_bad[static_cast<size_t>(k)] = i;
+        return;
+      }
+    }
+  });
+  for (const int64_t i : first_bad) {
+    if (i < 0) continue;
     const int32_t a = CP->list.a[i], b = CP->list.b[i], j = CP->memory[i];
     if (a < 0 || a >= nb || b < 0 || b >= nb || a == b) {
       set_error(c, "bg_contact_step: pair %lld has slots %d, %d of %lld", static_cast<long long>(i), a, b,
@@ -3265,10 +3282,8 @@ int contact_problem(bg_ctx* c, const bg_bodies* B, const bg_materials* M, const 
         set_error(c, "bg_contact_step: slot %d is not a box, sphere or capsule", s);
         return BG_EUNSUPPORTED;
       }
-    if (j < -1 || j >= records) {
-      set_error(c, "bg_contact_step: pair %lld names contact record %d of %d", static_cast<long long>(i), j, records);
-      return BG_EINVAL;
-    }
+    set_error(c, "bg_contact_step: pair %lld names contact record %d of %d", static_cast<long long>(i), j, records);
+    return BG_EINVAL;
   }
   for (int64_t i = 0; i < na; i++)
     if (static_cast<uint32_t>(B->awake_list[i]) >= static_cast<uint32_t>(nb)) {

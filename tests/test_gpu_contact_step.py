@@ -23,6 +23,7 @@ from bearing_b200.world import GpuSolver, World
 pytestmark = pytest.mark.gpu
 
 DT = 1 / 60
+REUSE = {"reuse": True}
 _PI = C.POINTER(C.c_int32)
 _PD = C.POINTER(C.c_double)
 
@@ -142,10 +143,30 @@ def test_the_50k_pile_120_steps():
     assert most > 60_000 and ms is not None
 
 
+def test_bodies_added_between_steps():
+    # The World's columns grow under the contact step (new slots, new pairs, the pair list's slots
+    # moving), and its records still follow their pairs.
+    wa, wb = oracle_world(options=REUSE), device_world(REUSE)
+    for w in (wa, wb):
+        scenes.pyramid(w, rows=8)
+    rng = np.random.default_rng(3)
+    drops = [(float(rng.uniform(-2, 2)), float(6 + i), float(rng.uniform(-2, 2))) for i in range(12)]
+    for i in range(150):
+        if i in (30, 60, 90):
+            for w in (wa, wb):
+                for p in drops[(i // 30 - 1) * 4:(i // 30) * 4]:
+                    w.addBody({"shape": "sphere" if p[1] % 2 else "box", "radius": 0.3, "position": p})
+        wa.step(DT)
+        wb.step(DT)
+        sa, sb = wa.state(), wb.state()
+        for k in sa:
+            assert _same(sa[k], sb[k]), f"step {i + 1}: {k} differs"
+        assert wa.stats() == wb.stats(), f"step {i + 1}"
+    wa.destroy()
+    wb.destroy()
+
+
 # ---- with the kept-manifold cache (src/contact.js:388-595), kept in the device's records ----
-
-REUSE = {"reuse": True}
-
 
 def test_pyramid_reusing_kept_manifolds():
     most, _ = step_pair(scenes.pyramid, 200, options=REUSE)
