@@ -2874,7 +2874,8 @@ double bg_last_collide_ms(bg_ctx* c) {
 namespace {
 
 struct ColourLayout {
-  int32_t *a, *b, *deg, *off, *cursor, *list, *rank, *colour, *bins, *bincur, *order, *starts, *status, *tiles;
+  int32_t *a, *b, *deg, *off, *cursor, *list, *rank, *colour, *order, *starts, *status, *tiles;
+  int32_t *keys[2], *vals[2], *rcounts, *colour_counts;
   uint8_t *type, *frozen;
   uint32_t* used;
   unsigned int* done;
@@ -2884,15 +2885,17 @@ struct ColourLayout {
 ColourLayout colour_layout(unsigned char* base, size_t nb, size_t n) {
   Carve k{base};
   ColourLayout L;
+  const size_t tiles = (n + bgcol::kRadixThreads - 1) / bgcol::kRadixThreads;
   L.a = k.take<int32_t>(n); L.b = k.take<int32_t>(n);
   L.type = k.take<uint8_t>(nb); L.frozen = k.take<uint8_t>(nb);
-  // zeroed together before each call: deg, cursor, used, done, bins, bincur, status
+  // zeroed together before each call: deg, cursor, used, done, colour_counts, status
   L.deg = k.take<int32_t>(nb); L.cursor = k.take<int32_t>(nb); L.used = k.take<uint32_t>(nb);
-  L.done = k.take<unsigned int>(nb); L.bins = k.take<int32_t>(bgcol::kRuns * nb + 1);
-  L.bincur = k.take<int32_t>(bgcol::kRuns * nb); L.status = k.take<int32_t>(1);
+  L.done = k.take<unsigned int>(nb); L.colour_counts = k.take<int32_t>(bgcol::kRuns); L.status = k.take<int32_t>(1);
   L.off = k.take<int32_t>(nb + 1); L.list = k.take<int32_t>(2 * n); L.rank = k.take<int32_t>(2 * n);
   L.colour = k.take<int32_t>(n); L.order = k.take<int32_t>(n); L.starts = k.take<int32_t>(bgcol::kStarts);
-  L.tiles = k.take<int32_t>(bgcol::kRuns * nb / bgcol::kTile + 2);
+  for (int j = 0; j < 2; j++) { L.keys[j] = k.take<int32_t>(n); L.vals[j] = k.take<int32_t>(n); }
+  L.rcounts = k.take<int32_t>(bgcol::kBuckets * tiles + 1);
+  L.tiles = k.take<int32_t>(std::max(nb, bgcol::kBuckets * tiles) / bgcol::kTile + 2);
   L.bytes = k.end;
   return L;
 }
@@ -2926,13 +2929,12 @@ void scan_into(cudaStream_t st, const int32_t* in, int32_t* out, int n, int32_t*
 }
 
 // colour() and arrange()'s order for p.n manifolds over p.nb slots, queued on the context's
-// stream (p's arrays zeroed as colour_layout() says; `tiles` holds kRuns * nb / kTile + 2).
+// stream (p's arrays zeroed as colour_layout() says; `tiles` holds max(nb, kBuckets * p.tiles) / kTile + 2).
 bool colour_kernels(bg_ctx* c, bgcol::ColourParams& p, int32_t* tiles) {
   cudaStream_t st = c->stream;
   const int64_t n = p.n, nb = p.nb;
   const int rows_grid = std::max(1, std::min(static_cast<int>((n + 255) / 256), 8 * c->sms));
   const int body_grid = std::max(1, std::min(static_cast<int>((nb + 255) / 256), 8 * c->sms));
-  const int bin_grid = std::max(1, std::min(static_cast<int>((bgcol::kRuns * nb + 255) / 256), 8 * c->sms));
   bgcol::col_degrees<<<rows_grid, 256, 0, st>>>(p);
   scan_into(st, p.deg, p.off, static_cast<int>(nb), tiles);
   bgcol::col_fill<<<rows_grid, 256, 0, st>>>(p);
@@ -2943,18 +2945,18 @@ bool colour_kernels(bg_ctx* c, bgcol::ColourParams& p, int32_t* tiles) {
                                                 args, 0, st), "col_colour launch"))
       return false;
   }
-  bgcol::col_bins<<<rows_grid, 256, 0, st>>>(p);
-  {
-    const int nbins = bgcol::kRuns * static_cast<int>(nb);
-    const int ntiles = (nbins + bgcol::kTile - 1) / bgcol::kTile;
-    bgcol::col_tile_sums<<<ntiles, bgcol::kScanThreads, 0, st>>>(p.bins, nbins, tiles);
-    bgcol::col_scan<<<1, bgcol::kScanThreads, 0, st>>>(tiles, tiles, ntiles);
-    bgcol::col_tile_scan<<<ntiles, bgcol::kScanThreads, 0, st>>>(p.bins, p.bins, nbins, tiles);
+  // arrange()'s order: the stable radix sort by (colour, b), 8 bits a pass
+  bgcol::col_keys<<<rows_grid, 256, 0, st>>>(p);
+  int bits = 1;
+  while ((static_cast<int64_t>(1) << bits) <= static_cast<int64_t>(bgcol::kRuns) * nb) bits++;
+  const int passes = (bits + 7) / 8;
+  for (int pass = 0; pass < passes; pass++) {
+    bgcol::col_radix_count<<<p.tiles, bgcol::kRadixThreads, 0, st>>>(p, pass & 1, 8 * pass);
+    scan_into(st, p.rcounts, p.rcounts, bgcol::kBuckets * p.tiles, tiles);
+    bgcol::col_radix_place<<<p.tiles, bgcol::kRadixThreads, 0, st>>>(p, pass & 1, 8 * pass, pass + 1 == passes);
   }
-  bgcol::col_scatter<<<rows_grid, 256, 0, st>>>(p);
-  bgcol::col_settle<<<bin_grid, 256, 0, st>>>(p);
-  bgcol::col_starts<<<1, 64, 0, st>>>(p);
-  c->last_launches += 14;
+  bgcol::col_starts<<<1, 32, 0, st>>>(p);
+  c->last_launches += 9 + 5 * passes;
   return cuda_ok(c, cudaGetLastError(), "colour launch");
 }
 
@@ -3013,8 +3015,11 @@ int32_t bg_colour(bg_ctx* c, const bg_bodies* B, int32_t count, const int32_t* a
   bgcol::ColourParams p;
   p.n = static_cast<int32_t>(n); p.nb = static_cast<int32_t>(nb); p.a = L.a; p.b = L.b; p.type = L.type;
   p.frozen = L.frozen; p.any_frozen = any_frozen; p.deg = L.deg; p.off = L.off; p.cursor = L.cursor; p.list = L.list;
-  p.rank = L.rank; p.used = L.used; p.done = L.done; p.colour = L.colour; p.bins = L.bins; p.bincur = L.bincur;
-  p.order = L.order; p.starts = L.starts; p.status = L.status; p.budget = c->budget;
+  p.rank = L.rank; p.used = L.used; p.done = L.done; p.colour = L.colour; p.order = L.order; p.starts = L.starts;
+  p.status = L.status; p.budget = c->budget;
+  for (int j = 0; j < 2; j++) { p.keys[j] = L.keys[j]; p.vals[j] = L.vals[j]; }
+  p.rcounts = L.rcounts; p.colour_counts = L.colour_counts;
+  p.tiles = static_cast<int32_t>((n + bgcol::kRadixThreads - 1) / bgcol::kRadixThreads);
   cudaEventRecord(d.begin, st);
   if (!colour_kernels(c, p, L.tiles)) return BG_ECUDA;
   cudaEventRecord(d.end, st);
@@ -3402,8 +3407,11 @@ int32_t bg_contact_step(bg_ctx* c, const bg_bodies* B, const bg_materials* M, co
     bgcol::ColourParams p;
     p.n = nrows; p.nb = nb; p.a = L.r.a; p.b = L.r.b; p.type = c->bin.type; p.frozen = c->bin.frozen;
     p.any_frozen = any_frozen; p.deg = CL.deg; p.off = CL.off; p.cursor = CL.cursor; p.list = CL.list;
-    p.rank = CL.rank; p.used = CL.used; p.done = CL.done; p.colour = CL.colour; p.bins = CL.bins;
-    p.bincur = CL.bincur; p.order = CL.order; p.starts = CL.starts; p.status = CL.status; p.budget = c->budget;
+    p.rank = CL.rank; p.used = CL.used; p.done = CL.done; p.colour = CL.colour; p.order = CL.order;
+    p.starts = CL.starts; p.status = CL.status; p.budget = c->budget;
+    for (int j = 0; j < 2; j++) { p.keys[j] = CL.keys[j]; p.vals[j] = CL.vals[j]; }
+    p.rcounts = CL.rcounts; p.colour_counts = CL.colour_counts;
+    p.tiles = (nrows + bgcol::kRadixThreads - 1) / bgcol::kRadixThreads;
     if (!colour_kernels(c, p, CL.tiles)) return BG_ECUDA;
     bgct::ct_rest<<<rgrid, 256, 0, st>>>(L.r, CL.colour, nrows);
     // the solve order and its runs

@@ -14,10 +14,12 @@
 // which independent thread scheduling lets them do.)  Every wait is bounded, as the stage's are.
 //
 // The row order is then a sort by (colour, b's slot, found order): arrange()'s stable counting
-// sorts by b's low and high digits and then by colour give exactly that order.  The device
-// counts each (colour, b) bin, scans the counts, drops each manifold into its bin and puts the
-// few bins that hold more than one manifold (the overflow, the resting run, a kinematic b) in
-// found order.
+// sorts by b's low and high digits and then by colour give exactly that order.  The device sorts
+// the manifolds, taken in found order, by the key colour * slots + b with a stable radix sort of
+// 8-bit digits (col_radix_*): each pass counts its digit per tile of 1,024, scans the (digit,
+// tile) counts and places each manifold after those of its digit in earlier tiles, warps and
+// lanes, so ties keep found order whatever the bins' sizes (a static b under thousands of
+// manifolds of one colour costs no more than any other).
 #pragma once
 
 #include <stdint.h>
@@ -43,8 +45,11 @@ struct ColourParams {
   uint32_t* used;         // nb: the colours a body's coloured manifolds took
   unsigned int* done;     // nb: the body's manifolds coloured so far
   int32_t* colour;        // n: each manifold's colour (found order)
-  int32_t* bins;          // kRuns * nb + 1: manifolds per (colour, b), then the scan
-  int32_t* bincur;        // kRuns * nb
+  int32_t* keys[2];       // n each: the sort's keys, two buffers it passes between
+  int32_t* vals[2];       // n each: the found indices that go with them
+  int32_t* rcounts;       // kBuckets * tiles + 1: a pass's (digit, tile) counts, then their scan
+  int32_t* colour_counts; // kRuns: manifolds of each colour
+  int32_t tiles;          // ceil(n / kRadixThreads)
   int32_t* order;         // n: the manifold found order[o]-th goes to row o
   int32_t* starts;        // kStarts
   int32_t* status;        // 1: a wait ran past its budget
@@ -239,50 +244,78 @@ __global__ void col_colour(ColourParams p) {
   }
 }
 
-// The row order: manifolds per (colour, b) bin, the bins scanned (col_scan), each manifold into
-// its bin, then each bin of more than one in found order.  (A manifold left uncoloured by a wait
-// that ran out has colour -1: it is left out, and the call fails.)
-__global__ void col_bins(ColourParams p) {
+// ---- the row order: a stable radix sort by (colour, b), ties in found order ----
+
+constexpr int kRadixThreads = 1024;   // one block a tile, one manifold a thread
+constexpr int kBuckets = 256;         // 8-bit digits
+
+// The first pass's input: each manifold's key in found order (a manifold left uncoloured by a wait
+// that ran out sorts last; the call then fails), and each colour's count.
+__global__ void col_keys(ColourParams p) {
+  __shared__ int32_t local[kRuns];
+  for (int k = threadIdx.x; k < kRuns; k += blockDim.x) local[k] = 0;
+  __syncthreads();
+  const int last = kRuns * p.nb;
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < p.n; f += gridDim.x * blockDim.x) {
     const int k = p.colour[f];
-    if (k < 0 || k > kResting) continue;
-    atomicAdd(&p.bins[k * p.nb + p.b[f]], 1);
+    const bool ok = k >= 0 && k <= kResting;
+    p.keys[0][f] = ok ? k * p.nb + p.b[f] : last;
+    p.vals[0][f] = f;
+    if (ok) atomicAdd(&local[k], 1);
   }
+  __syncthreads();
+  for (int k = threadIdx.x; k < kRuns; k += blockDim.x)
+    if (local[k] > 0) atomicAdd(&p.colour_counts[k], local[k]);
 }
 
-__global__ void col_scatter(ColourParams p) {
-  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < p.n; f += gridDim.x * blockDim.x) {
-    const int k = p.colour[f];
-    if (k < 0 || k > kResting) continue;
-    const int bin = k * p.nb + p.b[f];
-    p.order[p.bins[bin] + atomicAdd(&p.bincur[bin], 1)] = f;
-  }
+__global__ void __launch_bounds__(kRadixThreads) col_radix_count(ColourParams p, int from, int shift) {
+  __shared__ int32_t hist[kBuckets];
+  for (int d = threadIdx.x; d < kBuckets; d += blockDim.x) hist[d] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * kRadixThreads + threadIdx.x;
+  if (i < p.n) atomicAdd(&hist[(p.keys[from][i] >> shift) & (kBuckets - 1)], 1);
+  __syncthreads();
+  for (int d = threadIdx.x; d < kBuckets; d += blockDim.x) p.rcounts[d * p.tiles + blockIdx.x] = hist[d];
 }
 
-__global__ void col_settle(ColourParams p) {
-  const int nbins = kRuns * p.nb;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nbins; k += gridDim.x * blockDim.x) {
-    const int lo = p.bins[k], d = p.bins[k + 1] - lo;
-    if (d < 2) continue;
-    int32_t* l = p.order + lo;
-    for (int i = 1; i < d; i++) {
-      const int32_t v = l[i];
-      int j = i - 1;
-      while (j >= 0 && l[j] > v) {
-        l[j + 1] = l[j];
-        j--;
-      }
-      l[j + 1] = v;
-    }
+// Each manifold after its digit's manifolds in earlier tiles (the scanned counts), earlier warps
+// of its tile and earlier lanes of its warp: stable.  The last pass writes the found indices
+// straight into `order`.
+__global__ void __launch_bounds__(kRadixThreads) col_radix_place(ColourParams p, int from, int shift, int last) {
+  constexpr int kWarps = kRadixThreads / 32;
+  __shared__ int32_t warp_counts[kWarps][kBuckets];
+  for (int i = threadIdx.x; i < kWarps * kBuckets; i += blockDim.x) (&warp_counts[0][0])[i] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * kRadixThreads + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int key = i < p.n ? p.keys[from][i] : 0;
+  const int digit = i < p.n ? (key >> shift) & (kBuckets - 1) : -1;
+  const unsigned peers = __match_any_sync(0xffffffffu, digit);
+  const int before = __popc(peers & ((1u << lane) - 1u));
+  if (digit >= 0 && before == 0) warp_counts[warp][digit] = __popc(peers);
+  __syncthreads();
+  if (digit < 0) return;
+  int at = p.rcounts[digit * p.tiles + blockIdx.x] + before;
+  for (int w = 0; w < warp; w++) at += warp_counts[w][digit];
+  const int to = 1 - from;
+  if (last) {
+    p.order[at] = p.vals[from][i];
+  } else {
+    p.keys[to][at] = key;
+    p.vals[to][at] = p.vals[from][i];
   }
 }
 
 // starts[k]: where colour k's rows begin (k <= RESTING), starts[RESTING + 1] = n
 // (src/graph.js:152-166).
 __global__ void col_starts(ColourParams p) {
-  const int k = threadIdx.x;
-  if (k < kRuns) p.starts[k] = p.bins[k * p.nb];
-  if (k == kRuns) p.starts[k] = p.n;
+  if (threadIdx.x != 0) return;
+  int at = 0;
+  for (int k = 0; k < kRuns; k++) {
+    p.starts[k] = at;
+    at += p.colour_counts[k];
+  }
+  p.starts[kRuns] = p.n;
 }
 
 }  // namespace bgcol

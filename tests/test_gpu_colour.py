@@ -129,3 +129,18 @@ def test_the_50k_pile_colours_as_the_host_does():
     check_against_the_world(StageCopy(w))
     assert _ffi.gpu().bg_last_colour_ms(ctx()) > 0
     w.destroy()
+
+
+def test_a_static_body_under_ten_thousand_manifolds_of_one_colour():
+    # The ground added last, so it is b (the higher slot) of every pair it is in: 10,000 boxes
+    # resting on it put 10,000 manifolds of one colour on one (colour, b) key.  The order keeps
+    # found order within it, and the sort costs what any other does.
+    def build(w):
+        for i in range(100):
+            for j in range(100):
+                w.addBody({"size": (0.8, 0.8, 0.8), "position": (i - 49.5, 0.4, j - 49.5)})
+        w.addBody({"type": "static", "size": (120.0, 1.0, 120.0), "position": (0.0, -0.5, 0.0)})
+    copy = world_input(build, 3)
+    assert copy.count >= 10_000
+    check_against_the_world(copy)
+    assert 0 < _ffi.gpu().bg_last_colour_ms(ctx()) < 5.0
