@@ -340,6 +340,9 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
         if i >= args.warmup:
             resident.append(e0.elapsed_time(e1))
     cta_threads = lib.bg_block_threads(ctx)   # chosen by the library's tuner on the first solve
+    split = None
+    if world_size == 1:
+        split = measure_batch_split(args, lib, torch, device, base, statistics.mean(resident), log)
     # batched, host arrays: pageable (as the loop below has them), then page-locked.  A large
     # batch moves in groups of worlds on contexts of the library's own, so the events only bracket
     # the synchronous call (the context's own stream is idle meanwhile).
@@ -417,7 +420,78 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
                                         "how": "sum over the worlds of bg_solve with that world's input resident"},
             "speedup_e2e": ms_loop / ms_bat, "speedup_resident": ms_loop_res / ms_res,
             "bit_identical": same, "cta_threads": cta_threads,
-            "roofline": batch_roofline(algo, ms_res, cta_threads)}
+            "roofline": batch_roofline(algo, ms_res, cta_threads), "size_class_split": split}
+
+
+def measure_batch_split(args, lib, torch, device, base, ms_whole, log):
+    """The batch split by size class: its small worlds (at most `cut` solved rows) one CTA a world
+    at a fixed CTA size, its large ones on the persistent grid, each half resident and timed on
+    its own (the grid kernel holds every SM, so the halves run one after the other and the split
+    costs their sum), against the whole batch as the tuner ran it; the best split's results are
+    checked against the whole batch's, world by world."""
+    import numpy as np
+    from stage_io import first_difference
+    solved = np.array([int(base.starts[k * 35 + 33]) for k in range(base.worlds)])
+
+    def resident(sub, threads):
+        ctx = lib.bg_create(device, 0)
+        assert lib.bg_set_block_threads(ctx, threads) == 0
+        stream = torch.cuda.ExternalStream(lib.bg_stream(ctx))
+        B, R, W, S = sub.views()
+        assert lib.bg_batch_upload(ctx, C.byref(B), C.byref(R), C.byref(W)) == 0, lib.bg_last_error(ctx)
+        times = []
+        for i in range(args.warmup + args.steps):
+            assert lib.bg_restore(ctx) == 0
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            assert lib.bg_batch_solve(ctx, C.byref(S)) == 0, lib.bg_last_error(ctx)
+            e1.record(stream)
+            e1.synchronize()
+            if i >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+        out = sub.copy()
+        Bo, Ro, _, _ = out.views()
+        assert lib.bg_batch_download(ctx, C.byref(Bo), C.byref(Ro)) == 0
+        lib.bg_destroy(ctx)
+        return statistics.mean(times), out
+
+    tried = []
+    best = None
+    for cut in (16, 64, 256):
+        small = np.flatnonzero(solved <= cut)
+        large = np.flatnonzero(solved > cut)
+        if small.size == 0 or large.size == 0:
+            continue
+        sub_s, sub_l = base.subset(small), base.subset(large)
+        ms_l, out_l = resident(sub_l, _ffi_grid())
+        for threads in (64, 128):
+            ms_s, out_s = resident(sub_s, threads)
+            tried.append({"cut_rows": cut, "small_worlds": int(small.size), "cta_threads": threads,
+                          "small_ms": ms_s, "large_ms": ms_l, "ms_per_step": ms_s + ms_l})
+            if best is None or ms_s + ms_l < best[0]:
+                best = (ms_s + ms_l, small, large, out_s, out_l)
+    if best is None:
+        return None
+    # the whole batch's own results, solved once more as it ran
+    whole = base.copy()
+    ctx = lib.bg_create(device, 0)
+    B, R, W, S = whole.views()
+    assert lib.bg_batch_solve_step(ctx, C.byref(B), C.byref(R), C.byref(W), C.byref(S)) == 0
+    lib.bg_destroy(ctx)
+    _, small, large, out_s, out_l = best
+    same = all(first_difference(whole.world(int(w)), out_s.world(j)) is None for j, w in enumerate(small)) and \
+        all(first_difference(whole.world(int(w)), out_l.world(j)) is None for j, w in enumerate(large))
+    result = {"what": "small worlds one CTA a world, large ones on the grid, run one after the other",
+              "whole_batch_ms": ms_whole, "best_split_ms": best[0], "tried": tried, "bit_identical": same}
+    if log:
+        log(f"batch split by size class: best {best[0]:.2f} ms against {ms_whole:.2f} ms for the whole batch "
+            f"as the tuner ran it; bit-identical {same}")
+    return result
+
+
+def _ffi_grid():
+    from bearing_b200 import _ffi
+    return _ffi.BG_BATCH_ON_GRID
 
 
 def measure_adjoint(args, device, log):

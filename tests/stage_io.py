@@ -247,6 +247,25 @@ class BatchCopy:
             rows={f: st.rows[f][per * r0: per * r1].copy() for f, _, per in ROW_COLUMNS},
             dt=st.dt, substeps=st.substeps, gravity=st.gravity))
 
+    def subset(self, indices):
+        """A batch of only the worlds `indices`, in that order (their parts laid end to end)."""
+        parts = [self.world(int(i)) for i in indices]
+        c = BatchCopy.__new__(BatchCopy)
+        c.worlds = len(parts)
+        st = self.stage
+        c.body_offset = np.cumsum([0] + [p.capacity for p in parts]).astype(np.int32)
+        c.awake_offset = np.cumsum([0] + [p.awake_count for p in parts]).astype(np.int32)
+        c.row_offset = np.cumsum([0] + [p.count for p in parts]).astype(np.int32)
+        c.starts = np.concatenate([p.starts for p in parts]).astype(np.int32)
+        c.stage = StageCopy(arrays=dict(
+            capacity=int(c.body_offset[-1]), awake_count=int(c.awake_offset[-1]),
+            awake_list=np.concatenate([p.awake_list for p in parts]).astype(np.int32),
+            body={f: np.concatenate([p.body[f] for p in parts]) for f, _, _ in BODY_COLUMNS},
+            count=int(c.row_offset[-1]), solved=0, starts=np.zeros(_ffi.BG_STARTS, np.int32),
+            rows={f: np.concatenate([p.rows[f] for p in parts]) for f, _, _ in ROW_COLUMNS},
+            dt=st.dt, substeps=st.substeps, gravity=st.gravity))
+        return c
+
     def part(self, i, out):
         """Writes StageCopy `out` (world i's part, solved alone) back over this batch's arrays."""
         b0, b1 = int(self.body_offset[i]), int(self.body_offset[i + 1])
