@@ -286,3 +286,38 @@ def test_an_empty_list_still_steps_the_bodies():
     assert w.stats()["rows"] == 0
     w.destroy()
     wa.destroy()
+
+
+def test_a_lost_contact_step_keeps_the_records_and_the_retry_matches():
+    # A wait budget of one iteration makes the colouring's waits run out: the call returns
+    # BG_ETIMEOUT (the reference's Jobs.lost), holds no new records, and the same call with the
+    # default budget then gives exactly what a context that never lost the step gives.
+    w = oracle_world()
+    scenes.pile(w, count=2000, seed=9, extent=14.0)
+    for _ in range(60):
+        w.step(DT)
+    w.begin_step(DT)
+    copy = StageCopy(w)
+    pairs = narrow_io.world_pairs(w)
+    fr, rs = np.empty(copy.capacity), np.empty(copy.capacity)
+    assert w._lib.bw_materials(w._w, fr.ctypes.data_as(_PD), rs.ctypes.data_as(_PD)) == 0
+    w.destroy()
+    none = -np.ones(pairs.count, np.int32)
+    good, lost = GpuSolver(), GpuSolver()
+    want = copy.copy()
+    rc, _, _, out = _call(good.lib, good.ctx, want, pairs, fr, rs, none)
+    assert rc == 0 and out.rows > 1000
+    got = copy.copy()
+    assert lost.lib.bg_set_wait_budget(lost.ctx, 1) == 0
+    rc, _, _, _ = _call(lost.lib, lost.ctx, got, pairs, fr, rs, none)
+    assert rc == _ffi.BG_ETIMEOUT, lost.error()
+    assert lost.lib.bg_contact_records(lost.ctx) == 0
+    assert lost.lib.bg_set_wait_budget(lost.ctx, 1 << 24) == 0
+    got = copy.copy()
+    rc, _, _, _ = _call(lost.lib, lost.ctx, got, pairs, fr, rs, none)
+    assert rc == 0, lost.error()
+    for f in got.body:
+        assert _same(got.body[f], want.body[f]), f
+    assert lost.lib.bg_contact_records(lost.ctx) == pairs.count
+    good.close()
+    lost.close()
