@@ -9,6 +9,11 @@
 // host thread works out the solve order; unpack them into the device layout; run the solve stage
 // (a persistent cooperative grid for a single world, one CTA per world for a batch); pack the written
 // columns and copy them out the same way.
+//
+// Around the solve stage the same context also runs the narrowphase (bg_collide, sources in
+// host/collide_impl.hpp), the colouring and row order (bg_colour, colour.cuh), the adjoint
+// (bg_backward, adjoint.cuh) and a step's whole contact side from the pair list (bg_contact_step,
+// contact.cuh), each with device memory of its own next to the solve stage's.
 #include <cuda_runtime.h>
 
 #include <algorithm>

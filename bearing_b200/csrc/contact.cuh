@@ -11,6 +11,9 @@
 // The contact memory (src/pairs.js:50-58: a pair's remembered point count, point ids and normal
 // impulses, and its friction, twist and slip as world vectors) is kept as one record per pair of
 // the last call's list, in two banks: the call reads the last call's bank and writes the other.
+// With reuse on, a record also keeps the pair's manifold and touching flag (src/pairs.js:55-80),
+// and a pair whose kept manifold still holds by REUSE's rules (src/contact.js:388-537) takes it
+// rebuilt from the bodies' poses instead of a fresh one from the narrowphase (ct_reuse).
 #pragma once
 
 #include <stdint.h>
