@@ -15,7 +15,7 @@ import os
 
 import numpy as np
 
-from . import _ffi
+from . import _ffi, check
 
 SHAPES = {"box": _ffi.BG_BOX, "sphere": _ffi.BG_SPHERE, "capsule": _ffi.BG_CAPSULE}
 TYPES = {"dynamic": _ffi.BG_DYNAMIC, "static": _ffi.BG_STATIC, "kinematic": _ffi.BG_KINEMATIC}
@@ -27,8 +27,22 @@ DEFAULTS = dict(
     position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0, 1.0), velocity=(0.0, 0.0, 0.0),
     angularVelocity=(0.0, 0.0, 0.0),
 )
+# The reference's option lists (src/world.js:57-82, 190-196), for its messages; this path covers
+# boxes, spheres and capsules that are dynamic, static or kinematic.
+REFERENCE_BODY_OPTIONS = [
+    "type", "shape", "size", "radius", "height", "vertices", "indices", "heights", "columns", "spacing", "parts",
+    "density", "mass", "inertia", "centerOfMass",
+    "friction", "restitution", "damping", "angularDamping", "gravityScale", "layers", "mask", "sensor",
+    "lockRotation", "maxSlope", "stepHeight",
+    "position", "rotation", "velocity", "angularVelocity",
+]
+REFERENCE_SHAPES = ["box", "sphere", "capsule", "hull", "compound", "mesh", "heightfield"]
+REFERENCE_TYPES = ["dynamic", "static", "kinematic", "character"]
+SHAPE_SIZES = {"box": ["size"], "sphere": ["radius"], "capsule": ["radius", "height"], "hull": ["vertices"],
+               "compound": ["parts"], "mesh": ["vertices", "indices"], "heightfield": ["heights", "columns", "spacing"]}
+SIZES = ["size", "radius", "height", "vertices", "indices", "heights", "columns", "spacing", "parts"]
 BODY_OPTIONS = set(DEFAULTS)
-WORLD_OPTIONS = {"gravity", "substeps", "sleeping", "workers", "reuse"}
+WORLD_OPTIONS = ["gravity", "substeps", "sleeping", "workers", "reuse"]
 
 
 class BearingError(RuntimeError):
@@ -67,6 +81,92 @@ class GpuSolver:
             self.ctx = None
 
 
+def _workers(name, value):
+    """'auto' or a whole number from 0 (src/world.js _setWorkers): `name` is "World" for the
+    option, "world.workers" for the property."""
+    if value != "auto" and (isinstance(value, bool) or not isinstance(value, int) or value < 0):
+        text = f"must be 'auto' or a whole number, 0 or more, got {check.show(value)}"
+        check.fail("", f"World: workers {text}" if name == "World" else f"world.workers {text}")
+    return value
+
+
+def _not_here(caller, what):
+    check.fail(caller, f"{what} is not on this path (boxes, spheres and capsules, dynamic, static or kinematic)")
+
+
+def _resolve(caller, given_):
+    """addBody's options checked in the reference's order (src/world.js:2328-2462, from DEFAULTS),
+    the ones this path does not cover refused where the reference would first meet them."""
+    given = check.options(caller, given_)
+    check.known(caller, given, REFERENCE_BODY_OPTIONS)
+
+    def has(k):
+        return k in given
+
+    shape = check.one_of(caller, "shape", given["shape"], REFERENCE_SHAPES) if has("shape") else "box"
+    level = shape in ("mesh", "heightfield")
+    ttype = check.one_of(caller, "type", given["type"], REFERENCE_TYPES) if has("type") else \
+        ("static" if level else "dynamic")
+    for k in SIZES:
+        if has(k) and k not in SHAPE_SIZES[shape]:
+            check.fail(caller, f"a {shape} has no {k}")
+    if level and ttype in ("dynamic", "character"):
+        check.fail(caller, f"type must be 'static' or 'kinematic' for a {shape}, got '{ttype}'")
+    if shape in ("hull", "compound") and ttype == "character":
+        check.fail(caller, f"type must be 'dynamic', 'static' or 'kinematic' for a {shape}, got 'character'")
+    if shape not in SHAPES:
+        _not_here(caller, f"a {shape}")
+    if ttype not in TYPES:
+        _not_here(caller, f"a {ttype} body")
+    size = check.positive3(caller, "size", given["size"]) if has("size") else DEFAULTS["size"]
+    radius = check.positive(caller, "radius", given["radius"]) if has("radius") else DEFAULTS["radius"]
+    height = check.positive(caller, "height", given["height"]) if has("height") else DEFAULTS["height"]
+    if shape == "capsule" and height < 2 * radius:
+        check.fail(caller, f"height must be at least twice radius ({check.js_number(2 * radius)}), "
+                           f"got {check.js_number(height)}")
+    if has("mass") and has("density"):
+        check.fail(caller, "give mass or density, not both")
+    mass = check.positive(caller, "mass", given["mass"]) if has("mass") else 0.0
+    density = check.positive(caller, "density", given["density"]) if has("density") else DEFAULTS["density"]
+    for k in ("inertia", "centerOfMass"):
+        if has(k):
+            _not_here(caller, f"{k} given")
+    friction = check.at_least_zero(caller, "friction", given["friction"]) if has("friction") else DEFAULTS["friction"]
+    restitution = DEFAULTS["restitution"]
+    if has("restitution"):
+        r = given["restitution"]
+        if isinstance(r, bool) or not isinstance(r, (int, float)) or not (0 <= r <= 1):
+            check.fail(caller, f"restitution must be from 0 to 1, got {check.show(r)}")
+        restitution = float(r)
+    damping = check.at_least_zero(caller, "damping", given["damping"]) if has("damping") else DEFAULTS["damping"]
+    angular_damping = check.at_least_zero(caller, "angularDamping", given["angularDamping"]) \
+        if has("angularDamping") else DEFAULTS["angularDamping"]
+    gravity_scale = check.finite(caller, "gravityScale", given["gravityScale"]) if has("gravityScale") \
+        else DEFAULTS["gravityScale"]
+    for k in ("layers", "mask", "sensor", "lockRotation"):
+        if has(k):
+            _not_here(caller, f"{k}")
+    if ttype != "character":
+        for k in ("maxSlope", "stepHeight"):
+            if has(k):
+                check.fail(caller, f"a {ttype} body has no {k}")
+    position = check.vec3(caller, "position", given["position"]) if has("position") else DEFAULTS["position"]
+    rotation = check.quat(caller, "rotation", given["rotation"]) if has("rotation") else DEFAULTS["rotation"]
+    if ttype == "static":
+        for k in ("velocity", "angularVelocity"):
+            if has(k):
+                check.fail(caller, f"a static body has no {k}")
+        velocity = angular = (0.0, 0.0, 0.0)
+    else:
+        velocity = check.vec3(caller, "velocity", given["velocity"]) if has("velocity") else DEFAULTS["velocity"]
+        angular = check.vec3(caller, "angularVelocity", given["angularVelocity"]) if has("angularVelocity") \
+            else DEFAULTS["angularVelocity"]
+    return dict(type=ttype, shape=shape, size=size, radius=radius, height=height, density=density, mass=mass,
+                friction=friction, restitution=restitution, damping=damping, angularDamping=angular_damping,
+                gravityScale=gravity_scale, position=position, rotation=rotation, velocity=velocity,
+                angularVelocity=angular)
+
+
 def _vec(v, n, name):
     v = tuple(float(x) for x in v)
     if len(v) != n or not all(math.isfinite(x) for x in v):
@@ -78,17 +178,21 @@ class World:
     """A world of bodies, stepped with the solve stage on the GPU (or another bw_solver)."""
 
     def __init__(self, options: dict | None = None, solver=None):
-        o = dict(options or {})
-        unknown = set(o) - WORLD_OPTIONS
-        if unknown:
-            raise BearingError(f"World: unknown option {sorted(unknown)[0]!r}")
-        g = _vec(o.get("gravity", (0.0, -9.81, 0.0)), 3, "gravity")
-        substeps = int(o.get("substeps", 8))
-        if substeps < 1:
-            raise BearingError("World: substeps must be a whole number from 1")
+        try:
+            o = dict(check.options("World", options))
+            # the reference's options (src/world.js:82, 314-395), and this path's own `reuse`
+            check.known("World", {k: v for k, v in o.items() if k != "reuse"}, WORLD_OPTIONS[:4])
+            g = check.vec3("World", "gravity", o["gravity"]) if "gravity" in o else (0.0, -9.81, 0.0)
+            substeps = o.get("substeps", 8)
+            if isinstance(substeps, bool) or not isinstance(substeps, int) or substeps < 1:
+                check.fail("World", f"substeps must be a whole number, 1 or more, got {check.show(substeps)}")
+            if "sleeping" in o and not isinstance(o["sleeping"], bool):
+                check.fail("World", f"sleeping must be true or false, got {check.show(o['sleeping'])}")
+            self._workers = _workers("World", o.get("workers", "auto"))
+        except check.CheckError as e:
+            raise BearingError(str(e)) from None
         if o.get("sleeping", False):
             raise BearingError("World: sleeping islands are not on this path; pass sleeping: false")
-        self._workers = o.get("workers", "auto")
         self._lib = _ffi.host()
         # reuse: the kept-manifold cache of src/contact.js:388-595 (the reference always keeps one;
         # off by default here, where every pair whose boxes meet is collided afresh each step)
@@ -142,17 +246,15 @@ class World:
 
     # -- bodies ------------------------------------------------------------------------------
     def addBody(self, spec: dict | None = None) -> int:
-        """Adds a box, sphere or capsule (src/world.js:563-578); returns its slot."""
-        s = dict(DEFAULTS)
-        spec = dict(spec or {})
-        unknown = set(spec) - BODY_OPTIONS
-        if unknown:
-            raise BearingError(f"addBody: unknown option {sorted(unknown)[0]!r}")
-        s.update(spec)
-        if s["shape"] not in SHAPES:
-            raise BearingError(f"addBody: shape must be 'box', 'sphere' or 'capsule', got {s['shape']!r}")
-        if s["type"] not in TYPES:
-            raise BearingError(f"addBody: type must be 'dynamic', 'static' or 'kinematic', got {s['type']!r}")
+        """Adds a box, sphere or capsule (src/world.js:563-578); returns its slot.  Every option is
+        checked before anything is written, in the reference's order and words (src/world.js
+        resolve(), 2328-2462); a call that throws adds nothing."""
+        if not self._w:
+            raise BearingError("addBody: this world was destroyed")
+        try:
+            s = _resolve("addBody", spec)
+        except check.CheckError as e:
+            raise BearingError(str(e)) from None
         b = _ffi.BodySpec()
         b.type = TYPES[s["type"]]
         b.shape = SHAPES[s["shape"]]
@@ -179,8 +281,10 @@ class World:
     # -- stepping ----------------------------------------------------------------------------
     def step(self, dt: float):
         """One step of dt seconds (src/world.js:880-1072)."""
-        if not isinstance(dt, (int, float)) or not (dt > 0) or dt == math.inf:
-            raise BearingError(f"step: dt must be a positive number of seconds, got {dt!r}")
+        if not self._w:
+            raise BearingError("step: this world was destroyed")
+        if isinstance(dt, bool) or not isinstance(dt, (int, float)) or not (dt > 0) or dt == math.inf:
+            raise BearingError(f"step: dt must be a positive number of seconds, got {check.show(dt)}")
         rc = self._lib.bw_step(self._w, float(dt))
         if rc != 0:
             extra = ""
@@ -220,13 +324,16 @@ class World:
     def workers(self):
         """World.workers (src/world.js:501-524).  The solve stage runs on the GPU whatever it
         is; as in the reference, results do not depend on it."""
+        if not self._w:
+            raise BearingError("workers: this world was destroyed")
         return self._workers
 
     @workers.setter
     def workers(self, value):
-        if value != "auto" and (not isinstance(value, int) or value < 0):
-            raise BearingError(f"workers must be 'auto' or a whole number from 0, got {value!r}")
-        self._workers = value
+        try:
+            self._workers = _workers("world.workers", value)
+        except check.CheckError as e:
+            raise BearingError(str(e)) from None
 
     def stats(self) -> dict:
         st = _ffi.Stats()

@@ -155,7 +155,8 @@ def test_bodies_added_between_steps():
         if i in (30, 60, 90):
             for w in (wa, wb):
                 for p in drops[(i // 30 - 1) * 4:(i // 30) * 4]:
-                    w.addBody({"shape": "sphere" if p[1] % 2 else "box", "radius": 0.3, "position": p})
+                    shape = {"shape": "sphere", "radius": 0.3} if p[1] % 2 else {"size": (0.6, 0.6, 0.6)}
+                    w.addBody(dict(shape, position=p))
         wa.step(DT)
         wb.step(DT)
         sa, sb = wa.state(), wb.state()
