@@ -407,3 +407,26 @@ def test_a_step_does_what_it_did_before_bit_for_bit():
             w.step(DT)
         return w.transforms.tobytes()
     assert run() == run()
+
+
+def test_add_body_with_no_options_makes_a_1_m_box_of_water_at_rest_at_the_origin():
+    # test/world.test.js:16-30, for what this World's API reads back (its state and columns).
+    w = world()
+    s = w.addBody({})
+    assert body_mass(w, s) == 1000
+    st = w.state()
+    assert list(st["position"]) == [0.0, 0.0, 0.0] and list(st["rotation"]) == [0.0, 0.0, 0.0, 1.0]
+    assert list(st["velocity"]) == [0.0, 0.0, 0.0] and list(st["angular"]) == [0.0, 0.0, 0.0]
+    B, _, _ = w.views()
+    assert list(np.ctypeslib.as_array(B.dims, shape=(3,))) == [1.0, 1.0, 1.0]
+    assert w.addBody() == 1 and list(w.state()["position"][3:6]) == [0.0, 0.0, 0.0]
+
+
+def test_rotations_are_normalized_as_they_come_in():
+    # test/world.test.js:94-104: [0, 0, 0, 2] is the identity, and a huge quaternion is scaled
+    # before it is squared (src/core/check.js:100-117).
+    w = world()
+    a = w.addBody({"rotation": (0.0, 0.0, 0.0, 2.0)})
+    b = w.addBody({"rotation": (0.0, 1e200, 0.0, 1e200), "position": (3.0, 0.0, 0.0)})
+    assert list(col(w, "rotation", a, 4)) == [0.0, 0.0, 0.0, 1.0]
+    assert np.max(np.abs(col(w, "rotation", b, 4) - np.array([0.0, math.sqrt(0.5), 0.0, math.sqrt(0.5)]))) <= 1e-15
