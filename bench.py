@@ -57,6 +57,10 @@ def parse():
     p.add_argument("--adjoint-steps", type=int, default=120)
     p.add_argument("--no-adjoint", action="store_true", help="skip the backward-pass measurement")
     p.add_argument("--no-contact", action="store_true", help="skip the device contact-step measurement")
+    p.add_argument("--save-batch", default=None, help="write the batch's timed input (files PATH.npz, PATH.stage.npz)")
+    p.add_argument("--load-batch", default=None,
+                   help="solve a batch written by --save-batch once on the persistent grid and exit (a profiler "
+                        "then sees one launch of the batched kernel)")
     p.add_argument("--save-input", default=None, help="write the timed solve stage's input to this .npz")
     p.add_argument("--load-input", default=None,
                    help="time the solve stage of an input written by --save-input instead of building the pile "
@@ -321,6 +325,8 @@ def measure_batch(args, lib, torch, device, log, rank=0, world_size=1, dist=None
         batch.step(DT)
     batch.begin_step(DT)
     base = BatchCopy(*batch.views())
+    if args.save_batch:
+        base.save(args.save_batch)
     if log:
         log(f"batch of {args.batch_worlds} worlds built and stepped to {args.batch_at} in {time.time() - t0:.0f} s: "
             f"{base.stage.capacity} slots, {base.stage.count} rows")
@@ -492,6 +498,23 @@ def measure_batch_split(args, lib, torch, device, base, ms_whole, log):
 def _ffi_grid():
     from bearing_b200 import _ffi
     return _ffi.BG_BATCH_ON_GRID
+
+
+def solve_saved_batch(args, log):
+    """One batched solve of a saved batch on the persistent grid (no tuning), for a profiler."""
+    from bearing_b200 import _ffi
+    from stage_io import BatchCopy
+    lib = _ffi.gpu()
+    base = BatchCopy.load(args.load_batch)
+    ctx = lib.bg_create(0, 0)
+    assert lib.bg_set_block_threads(ctx, _ffi.BG_BATCH_ON_GRID) == 0
+    B, R, W, S = base.views()
+    assert lib.bg_batch_upload(ctx, C.byref(B), C.byref(R), C.byref(W)) == 0, lib.bg_last_error(ctx)
+    assert lib.bg_batch_solve(ctx, C.byref(S)) == 0, lib.bg_last_error(ctx)
+    ms = lib.bg_last_stage_ms(ctx)
+    lib.bg_destroy(ctx)
+    if log:
+        log(f"saved batch: {base.worlds} worlds, {base.stage.count} rows, stage {ms:.3f} ms")
 
 
 def measure_adjoint(args, device, log):
@@ -831,6 +854,9 @@ def main():
         print(json.dumps(line), flush=True)
         return
 
+    if args.load_batch:
+        solve_saved_batch(args, log)
+        return
     import torch
     torch.cuda.set_device(local)
     dist = None

@@ -247,6 +247,24 @@ class BatchCopy:
             rows={f: st.rows[f][per * r0: per * r1].copy() for f, _, per in ROW_COLUMNS},
             dt=st.dt, substeps=st.substeps, gravity=st.gravity))
 
+    def save(self, path):
+        """The batch's arrays and its table of worlds into one .npz file (BatchCopy.load reads it)."""
+        base = str(path)
+        self.stage.save(base + ".stage.npz")
+        np.savez(base, body_offset=self.body_offset, awake_offset=self.awake_offset, row_offset=self.row_offset,
+                 starts=self.starts)
+
+    @staticmethod
+    def load(path):
+        base = str(path)
+        z = np.load(base if base.endswith(".npz") else base + ".npz")
+        c = BatchCopy.__new__(BatchCopy)
+        c.stage = StageCopy.load(base + ".stage.npz")
+        for k in ("body_offset", "awake_offset", "row_offset", "starts"):
+            setattr(c, k, z[k].copy())
+        c.worlds = len(c.body_offset) - 1
+        return c
+
     def subset(self, indices):
         """A batch of only the worlds `indices`, in that order (their parts laid end to end)."""
         parts = [self.world(int(i)) for i in indices]

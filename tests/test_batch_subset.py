@@ -62,3 +62,14 @@ def test_every_world_in_order_gives_the_batch_back():
     for f, _, _ in ROW_COLUMNS:
         assert whole.stage.rows[f].tobytes() == base.stage.rows[f].tobytes(), f
     assert np.array_equal(whole.stage.awake_list, base.stage.awake_list)
+
+
+def test_save_and_load_give_the_batch_back(tmp_path):
+    base = a_batch(count=4)
+    base.save(tmp_path / "b")
+    back = BatchCopy.load(tmp_path / "b")
+    assert back.worlds == base.worlds
+    for k in ("body_offset", "awake_offset", "row_offset", "starts"):
+        assert np.array_equal(getattr(back, k), getattr(base, k)), k
+    for i in range(base.worlds):
+        same_world(back.world(i), base.world(i))
