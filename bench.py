@@ -781,15 +781,15 @@ def batch_roofline(algo, ms, cta_threads):
     committed capture of 1,024 of the same worlds by algorithmic bytes."""
     hbm, peak_source = hbm_peak()
     achieved = algo / (ms / 1000) / 1e9
-    traffic = None
-    got = profiled("stage_grid_batch_1024worlds")
+    traffic, source = None, None
+    got = profiled("stage_grid_batch_4096worlds_step301")
     if got is not None and cta_threads == 1:   # the capture is of the grid's kernel
         traffic = int(round(got["traffic_bytes_per_launch"] * algo / got["algorithmic_bytes_per_launch"]))
+        source = ("ncu capture of this launch (profiles/counters.json)" if algo == got["algorithmic_bytes_per_launch"]
+                  else "ncu capture of the 4,096 worlds at step 301, scaled by algorithmic bytes")
     kernel = "stage_grid_batch" if cta_threads == 1 else f"stage_block ({cta_threads} threads a world)"
     return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "algorithmic_bytes": algo, "traffic": traffic,
-            "traffic_source": "ncu capture of 1,024 of the worlds at step 61 (profiles/counters.json), scaled by "
-                              "algorithmic bytes",
+            "frac": achieved / hbm, "algorithmic_bytes": algo, "traffic": traffic, "traffic_source": source,
             "peak_source": peak_source}
 
 
