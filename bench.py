@@ -777,8 +777,8 @@ def measure_contact_step(args, lib, solver, world, device, steps, warmup, log):
 
 def batch_roofline(algo, ms, cta_threads):
     """The batched kernel's roofline line: this rank's algorithmic bytes over the resident solve's
-    time (the max over ranks), against the measured HBM copy rate; DRAM traffic scaled from the
-    committed capture of 1,024 of the same worlds by algorithmic bytes."""
+    time (the max over ranks), against the measured HBM copy rate; DRAM traffic from the committed
+    capture of the same 4,096 worlds at step 301, scaled by algorithmic bytes where the batch differs."""
     hbm, peak_source = hbm_peak()
     achieved = algo / (ms / 1000) / 1e9
     traffic, source = None, None
