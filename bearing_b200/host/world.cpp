@@ -714,25 +714,79 @@ struct bw_world {
   // pairs' memory are the one-pass walk's.
   // The first pass: the list of pairs whose boxes meet, each with its slot, margin, tolerance and
   // contact record (nmRecord, for bw_set_contact_step).
-  void listPairs() {
-    listA.clear(); listB.clear(); listMargin.clear(); listTol.clear(); nmPair.clear(); nmRecord.clear();
-    for (int p = 0; p < pairs.active;) {
-      const int a = pairs.a[p], b = pairs.b[p];
-      if (!fatOverlap(a, b)) {
-        pairs.remove(p);
+  // Each pair's fate depends only on its two bodies' boxes, so the boxes are compared first, on
+  // several threads when the list is long (kGone: the fat boxes part, kApart: the boxes miss,
+  // kMeet).  The removals then run in the walk's order over those marks alone: the walk removes
+  // the pair at its position by moving the last pair (and its mark) there and looking again, and
+  // never moves a pair it has passed, so every pair it keeps ends where the walk handles it.  Last,
+  // the kept pairs are forgotten or listed by position, on the same threads: the walk's list, in
+  // its order, with each pair's final position.
+  enum : uint8_t { kGone = 0, kApart = 1, kMeet = 2 };
+  std::vector<uint8_t> fate;
+  std::vector<int32_t> meetBefore;
+  void handle(int lo, int hi, int at) {
+    for (int p = lo; p < hi; p++) {
+      if (fate[p] == kApart) {
+        pairs.forget(p);
         continue;
       }
+      const int a = pairs.a[p], b = pairs.b[p];
       const double tol = jmin(size[a], size[b]) * PIXEL;
-      const int a6 = a * 6, b6 = b * 6;
-      if (box[a6] > box[b6 + 3] || box[b6] > box[a6 + 3] || box[a6 + 1] > box[b6 + 4]
-          || box[b6 + 1] > box[a6 + 4] || box[a6 + 2] > box[b6 + 5] || box[b6 + 2] > box[a6 + 5]) {
-        pairs.forget(p);
-      } else {
-        listA.push_back(a); listB.push_back(b); listMargin.push_back(motion[a] + motion[b] + tol);
-        listTol.push_back(tol); nmPair.push_back(p); nmRecord.push_back(pairs.record[p]);
-      }
-      p++;
+      listA[at] = a; listB[at] = b; listMargin[at] = motion[a] + motion[b] + tol; listTol[at] = tol;
+      nmPair[at] = p; nmRecord[at] = pairs.record[p];
+      at++;
     }
+  }
+  uint8_t fateOf(int p) const {
+    const int a = pairs.a[p], b = pairs.b[p];
+    if (!fatOverlap(a, b)) return kGone;
+    const int a6 = a * 6, b6 = b * 6;
+    return box[a6] > box[b6 + 3] || box[b6] > box[a6 + 3] || box[a6 + 1] > box[b6 + 4] || box[b6 + 1] > box[a6 + 4]
+               || box[a6 + 2] > box[b6 + 5] || box[b6 + 2] > box[a6 + 5]
+           ? kApart
+           : kMeet;
+  }
+  // Runs f(t, lo, hi) over `threads` consecutive ranges of [0, n), on threads when more than one.
+  template <class F>
+  static void ranges(int n, int threads, F f) {
+    if (threads <= 1) {
+      f(0, 0, n);
+      return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++)
+      pool.emplace_back([&f, t, threads, n] {
+        f(t, static_cast<int>(static_cast<int64_t>(n) * t / threads),
+          static_cast<int>(static_cast<int64_t>(n) * (t + 1) / threads));
+      });
+    for (auto& th : pool) th.join();
+  }
+  void listPairs() {
+    constexpr int kPerThread = 1 << 16;
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int before = pairs.active;
+    fate.resize(static_cast<size_t>(std::max(before, 1)));
+    ranges(before, std::min({16, hw, before / kPerThread}), [this](int, int lo, int hi) {
+      for (int p = lo; p < hi; p++) fate[p] = fateOf(p);
+    });
+    for (int p = 0; p < pairs.active; p++)
+      while (p < pairs.active && fate[p] == kGone) {
+        fate[p] = fate[pairs.active - 1];   // the last pair moves into p
+        pairs.remove(p);
+      }
+    const int active = pairs.active;
+    const int chunks = std::max(1, std::min({16, hw, active / kPerThread}));
+    meetBefore.assign(static_cast<size_t>(chunks) + 1, 0);
+    ranges(active, chunks, [this](int t, int lo, int hi) {
+      int m = 0;
+      for (int p = lo; p < hi; p++) m += fate[p] == kMeet;
+      meetBefore[t + 1] = m;
+    });
+    for (int t = 0; t < chunks; t++) meetBefore[t + 1] += meetBefore[t];
+    const size_t listed = static_cast<size_t>(meetBefore[chunks]);
+    listA.resize(listed); listB.resize(listed); listMargin.resize(listed); listTol.resize(listed);
+    nmPair.resize(listed); nmRecord.resize(listed);
+    ranges(active, chunks, [this](int t, int lo, int hi) { handle(lo, hi, meetBefore[t]); });
   }
 
   int narrowOnDevice() {

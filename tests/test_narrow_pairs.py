@@ -111,6 +111,35 @@ def test_a_world_with_its_narrowphase_handed_out_is_the_same_world(build, steps,
     b.destroy()
 
 
+def test_a_long_pair_list_is_marked_on_several_threads_with_the_same_result():
+    # Past 131,072 pairs the walk's box comparisons run on several threads before the walk takes
+    # the pairs in order: a 20,000-body pile falling reaches 200,000 pairs by step 50.
+    host = _ffi.host()
+
+    def collide(user, bodies, gravity, pairs, out):
+        return host.bw_collide_pairs(bodies, gravity, pairs, out, 4)
+
+    hook = NARROWPHASE(collide)
+    a = World({}, solver=oracle_io.solver(0))
+    b = World({}, solver=oracle_io.solver(0))
+    for w in (a, b):
+        scenes.pile(w, count=20_000, extent=60.0)
+    assert host.bw_set_narrowphase(b._w, C.cast(hook, C.c_void_p), None) == 0
+    most = 0
+    for i in range(55):
+        a.step(DT)
+        b.step(DT)
+        sa, sb = a.state(), b.state()
+        for k in ("position", "rotation", "velocity", "angular"):
+            assert sa[k].tobytes() == sb[k].tobytes(), f"step {i + 1}: {k}"
+        assert a.stats()["pairs"] == b.stats()["pairs"]
+        most = max(most, b.stats()["pairs"])
+    assert most >= 2 * 65536
+    assert host.bw_set_narrowphase(b._w, None, None) == 0
+    a.destroy()
+    b.destroy()
+
+
 def test_a_failing_narrowphase_fails_the_step():
     host = _ffi.host()
     hook = NARROWPHASE(lambda *args: _ffi.BG_ECUDA)
