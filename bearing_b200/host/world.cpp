@@ -114,6 +114,71 @@ struct Contacts {
   }
 };
 
+// Where each pair is in the list, by its key (the reference's Map from pair key to pair,
+// src/pairs.js): open addressing with linear probing in two flat arrays, at most half full, keys
+// spread by MurmurHash3's 64-bit finaliser.  A removal shifts the entries after it back into the
+// hole where their probe path allows, so no deleted marks build up over a long run.
+struct PairIndex {
+  static constexpr uint64_t kEmpty = ~0ull;   // no pair key is all ones (slots are below 2^31)
+  std::vector<uint64_t> keys;
+  std::vector<int32_t> vals;
+  size_t used = 0;
+
+  static size_t spread(uint64_t k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return static_cast<size_t>(k);
+  }
+  size_t mask() const { return keys.size() - 1; }
+  // The key's entry, or the empty entry where it would go.
+  size_t find(uint64_t k) const {
+    size_t i = spread(k) & mask();
+    while (keys[i] != kEmpty && keys[i] != k) i = (i + 1) & mask();
+    return i;
+  }
+  bool contains(uint64_t k) const { return !keys.empty() && keys[find(k)] == k; }
+  void set(uint64_t k, int32_t v) {
+    if (2 * (used + 1) > keys.size()) rehash(keys.empty() ? 64 : 2 * keys.size());
+    const size_t i = find(k);
+    if (keys[i] == kEmpty) {
+      keys[i] = k;
+      used++;
+    }
+    vals[i] = v;
+  }
+  void erase(uint64_t k) {
+    if (keys.empty()) return;
+    size_t hole = find(k);
+    if (keys[hole] != k) return;
+    for (size_t j = (hole + 1) & mask(); keys[j] != kEmpty; j = (j + 1) & mask()) {
+      // The entry at j may fill the hole if the hole lies on its probe path, from its home to j.
+      const size_t home = spread(keys[j]) & mask();
+      if (((j - home) & mask()) >= ((j - hole) & mask())) {
+        keys[hole] = keys[j];
+        vals[hole] = vals[j];
+        hole = j;
+      }
+    }
+    keys[hole] = kEmpty;
+    used--;
+  }
+  void rehash(size_t capacity) {
+    std::vector<uint64_t> oldKeys(capacity, kEmpty);
+    std::vector<int32_t> oldVals(capacity, 0);
+    oldKeys.swap(keys);
+    oldVals.swap(vals);
+    for (size_t i = 0; i < oldKeys.size(); i++) {
+      if (oldKeys[i] == kEmpty) continue;
+      const size_t at = find(oldKeys[i]);
+      keys[at] = oldKeys[i];
+      vals[at] = oldVals[i];
+    }
+  }
+};
+
 // The pair list: src/pairs.js (awake pairs only: every pair here has an awake body).
 struct Pairs {
   int count = 0, active = 0;
@@ -131,7 +196,7 @@ struct Pairs {
   std::vector<uint8_t> cached, cachePoints;
   std::vector<double> cachePose, cacheLoss, cacheNormal, cacheLocal;
   std::vector<uint32_t> cacheId;
-  std::unordered_map<uint64_t, int32_t> index;
+  PairIndex index;
 
   static uint64_t key(int x, int y) { return (static_cast<uint64_t>(x) << 32) | static_cast<uint32_t>(y); }
   void reserve(int n) {
@@ -149,11 +214,11 @@ struct Pairs {
   void found(int x, int y, const uint8_t* type) {
     if (type[x] != BG_DYNAMIC && type[y] != BG_DYNAMIC) return;
     const int lo = x < y ? x : y, hi = x < y ? y : x;
-    if (index.count(key(lo, hi))) return;
+    if (index.contains(key(lo, hi))) return;
     const int p = count;
     reserve(p + 1);
     a[p] = lo; b[p] = hi; points[p] = 0; touching[p] = 0; record[p] = -1; cached[p] = 0;
-    index[key(lo, hi)] = p;
+    index.set(key(lo, hi), p);
     count++;
     active = count;
   }
@@ -173,7 +238,7 @@ struct Pairs {
       slip[3 * to + k] = slip[3 * from + k];
       twist[3 * to + k] = twist[3 * from + k];
     }
-    index[key(a[to], b[to])] = to;
+    index.set(key(a[to], b[to]), to);
   }
   // remove: src/pairs.js:217-232 (one run).
   void remove(int p) {
