@@ -276,6 +276,7 @@ def host() -> C.CDLL:
         lib.bw_copy.argtypes = [C.c_void_p, C.c_void_p]
         lib.bw_narrow_pairs.argtypes = [C.c_void_p, C.POINTER(Pairs)]
         lib.bw_set_narrowphase.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.bw_set_workers.argtypes = [C.c_void_p, C.c_int32]
         lib.bw_set_contact_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         lib.bw_colour_rows.argtypes = [C.POINTER(Bodies), C.c_int32, _i32, _i32, _i32, _i32, _i32, _i32]
         lib.bw_collide_pairs.argtypes = [C.POINTER(Bodies), _d, C.POINTER(Pairs), C.POINTER(Manifolds), C.c_int32]
@@ -283,7 +284,7 @@ def host() -> C.CDLL:
                   "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_stats_get", "bw_batch_begin_step",
                   "bw_batch_views", "bw_batch_end_step", "bw_row_memory_get", "bw_batch_row_memory", "bw_copy",
                   "bw_keep_backward", "bw_narrow_backward", "bw_materials", "bw_narrow_pairs", "bw_collide_pairs",
-                  "bw_set_narrowphase", "bw_colour_rows", "bw_set_contact_step"):
+                  "bw_set_narrowphase", "bw_set_workers", "bw_colour_rows", "bw_set_contact_step"):
             getattr(lib, f).restype = C.c_int32
         _host = lib
     return _host
@@ -383,6 +384,6 @@ HOST_SYMBOLS = [
     "bw_end_step", "bw_bodies_view", "bw_rows_view", "bw_step_params", "bw_transforms", "bw_stats_get",
     "bw_batch_create", "bw_batch_destroy", "bw_batch_begin_step", "bw_batch_views", "bw_batch_end_step",
     "bw_row_memory_get", "bw_batch_row_memory", "bw_clone", "bw_copy", "bw_keep_backward", "bw_narrow_backward",
-    "bw_materials", "bw_narrow_pairs", "bw_collide_pairs", "bw_set_narrowphase", "bw_colour_rows",
+    "bw_materials", "bw_narrow_pairs", "bw_collide_pairs", "bw_set_narrowphase", "bw_set_workers", "bw_colour_rows",
     "bw_set_contact_step",
 ]

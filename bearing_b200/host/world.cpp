@@ -338,8 +338,6 @@ struct bw_world {
   double cell = 0;
   std::unordered_map<uint64_t, std::vector<int32_t>> grid;
   std::vector<int32_t> largeList;
-  std::vector<int32_t> seen;
-  int32_t seenMark = 0;
   Pairs pairs;
   Contacts c;
   bw_solver solver = nullptr;
@@ -368,7 +366,7 @@ struct bw_world {
     grow(axes, 9 * s); grow(box, 6 * s); grow(motion, s); grow(invI, 6 * s); grow(start, 3 * s); grow(startQ, 4 * s);
     grow(type, s); grow(shape, s); grow(framed, s); grow(lock, s); grow(frozen, s); grow(awake, s);
     grow(jointHead, s); grow(awakeList, s); grow(transforms, 7 * s);
-    grow(fat, 6 * s); grow(filed, s); grow(isMoved, s); grow(large, s); grow(seen, s);
+    grow(fat, 6 * s); grow(filed, s); grow(isMoved, s); grow(large, s);
   }
 
   // _boundsOf: src/world.js:1581-1630 (boxes, spheres, capsules).
@@ -494,38 +492,58 @@ struct bw_world {
       fileIn(s);
       mark(s);
     }
-    std::vector<int32_t> found;
-    for (size_t i = 0; i < moved.size(); i++) {
-      const int a = moved[i];
-      isMoved[a] = 0;
-      const bool aStatic = type[a] == BG_STATIC;
-      found.clear();
-      seenMark++;
-      auto consider = [&](int b) {
-        if (b == a || seen[b] == seenMark) return;
-        seen[b] = seenMark;
-        if (aStatic && type[b] == BG_STATIC) return;
-        if (fatOverlap(a, b)) found.push_back(b);
-      };
-      if (large[a]) {
-        for (auto& kv : grid)
-          for (int b : kv.second) consider(b);
-      } else {
-        int64_t lo[3], hi[3];
-        cellRange(a, lo, hi);
-        for (int64_t x = lo[0]; x <= hi[0]; x++)
-          for (int64_t y = lo[1]; y <= hi[1]; y++)
-            for (int64_t z = lo[2]; z <= hi[2]; z++) {
-              auto it = grid.find(cellKey(x, y, z));
-              if (it == grid.end()) continue;
-              for (int b : it->second) consider(b);
-            }
+    // Each moved body's overlaps depend only on the grid and the fat boxes, which stay as they are
+    // until the next step, so they are found on several threads when many bodies moved; the pairs
+    // are then made in the moved bodies' order, each body's in slot order, as one thread would.
+    const int m = static_cast<int>(moved.size());
+    const int threads = std::max(1, std::min(hostThreads(), m / 2048));
+    std::vector<std::vector<int32_t>> found(static_cast<size_t>(threads));
+    std::vector<int32_t> counts(static_cast<size_t>(std::max(m, 1)));
+    ranges(m, threads, [&](int t, int lo, int hi) {
+      std::vector<int32_t> one;
+      for (int i = lo; i < hi; i++) {
+        overlaps(moved[i], one);
+        counts[i] = static_cast<int32_t>(one.size());
+        found[t].insert(found[t].end(), one.begin(), one.end());
       }
-      for (int b : largeList) consider(b);
-      std::sort(found.begin(), found.end());
-      for (int b : found) pairs.found(a, b, type.data());
+    });
+    for (int t = 0; t < threads; t++) {
+      const int lo = static_cast<int>(static_cast<int64_t>(m) * t / threads);
+      const int hi = static_cast<int>(static_cast<int64_t>(m) * (t + 1) / threads);
+      size_t at = 0;
+      for (int i = lo; i < hi; i++) {
+        const int a = moved[i];
+        isMoved[a] = 0;
+        for (int k = 0; k < counts[i]; k++) pairs.found(a, found[t][at++], type.data());
+      }
     }
     moved.clear();
+  }
+  // The bodies whose fat boxes overlap a's, in slot order: those filed in the cells a's fat box
+  // covers (every filed body, for a large box) and the large ones, but not a, nor a static body
+  // for a static a (src/broadphase.js:146-165).
+  void overlaps(int a, std::vector<int32_t>& out) const {
+    out.clear();
+    if (large[a]) {
+      for (const auto& kv : grid) out.insert(out.end(), kv.second.begin(), kv.second.end());
+    } else {
+      int64_t lo[3], hi[3];
+      cellRange(a, lo, hi);
+      for (int64_t x = lo[0]; x <= hi[0]; x++)
+        for (int64_t y = lo[1]; y <= hi[1]; y++)
+          for (int64_t z = lo[2]; z <= hi[2]; z++) {
+            auto it = grid.find(cellKey(x, y, z));
+            if (it != grid.end()) out.insert(out.end(), it->second.begin(), it->second.end());
+          }
+    }
+    out.insert(out.end(), largeList.begin(), largeList.end());
+    std::sort(out.begin(), out.end());
+    out.erase(std::unique(out.begin(), out.end()), out.end());
+    const bool aStatic = type[a] == BG_STATIC;
+    size_t k = 0;
+    for (const int b : out)
+      if (b != a && !(aStatic && type[b] == BG_STATIC) && fatOverlap(a, b)) out[k++] = b;
+    out.resize(k);
   }
 
   int awakeCount = 0;
@@ -787,6 +805,13 @@ struct bw_world {
   // the kept pairs are forgotten or listed by position, on the same threads: the walk's list, in
   // its order, with each pair's final position.
   enum : uint8_t { kGone = 0, kApart = 1, kMeet = 2 };
+  // World.workers (src/world.js:501-524): how many threads besides the caller's a step may use
+  // (bw_set_workers); -1, 'auto', is the machine's cores up to 16.  Results do not depend on it.
+  int workers = -1;
+  int hostThreads() const {
+    if (workers >= 0) return std::min(workers + 1, 64);
+    return std::min(16, static_cast<int>(std::max(1u, std::thread::hardware_concurrency())));
+  }
   std::vector<uint8_t> fate;
   std::vector<int32_t> meetBefore;
   void handle(int lo, int hi, int at) {
@@ -828,10 +853,10 @@ struct bw_world {
   }
   void listPairs() {
     constexpr int kPerThread = 1 << 16;
-    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int hw = hostThreads();
     const int before = pairs.active;
     fate.resize(static_cast<size_t>(std::max(before, 1)));
-    ranges(before, std::min({16, hw, before / kPerThread}), [this](int, int lo, int hi) {
+    ranges(before, std::min(hw, before / kPerThread), [this](int, int lo, int hi) {
       for (int p = lo; p < hi; p++) fate[p] = fateOf(p);
     });
     for (int p = 0; p < pairs.active; p++)
@@ -840,7 +865,7 @@ struct bw_world {
         pairs.remove(p);
       }
     const int active = pairs.active;
-    const int chunks = std::max(1, std::min({16, hw, active / kPerThread}));
+    const int chunks = std::max(1, std::min(hw, active / kPerThread));
     meetBefore.assign(static_cast<size_t>(chunks) + 1, 0);
     ranges(active, chunks, [this](int t, int lo, int hi) {
       int m = 0;
@@ -1253,6 +1278,12 @@ int32_t bw_add_body(bw_world* w, const bw_body* spec) {
     w->awake[s] = 1;
   }
   return s;
+}
+
+int32_t bw_set_workers(bw_world* w, int32_t workers) {
+  if (w == nullptr || workers < -1) return BG_EINVAL;
+  w->workers = workers;
+  return BG_OK;
 }
 
 int32_t bw_set_narrowphase(bw_world* w, bw_narrowphase fn, void* user) {

@@ -198,6 +198,7 @@ class World:
         # off by default here, where every pair whose boxes meet is collided afresh each step)
         opts = _ffi.Options((C.c_double * 3)(*g), substeps, 1 if o.get("reuse", False) else 0)
         self._w = self._lib.bw_create(C.byref(opts))
+        self._lib.bw_set_workers(self._w, -1 if self._workers == "auto" else min(self._workers, 1 << 20))
         self._count = 0
         self._solver = None
         self._solver_keep = None
@@ -322,18 +323,22 @@ class World:
 
     @property
     def workers(self):
-        """World.workers (src/world.js:501-524).  The solve stage runs on the GPU whatever it
-        is; as in the reference, results do not depend on it."""
+        """World.workers (src/world.js:501-524): the threads besides the caller's that the step's
+        host side uses for its pair upkeep ('auto': the machine's cores, up to 16).  The solve stage
+        runs on the GPU whatever it is; as in the reference, results do not depend on it."""
         if not self._w:
             raise BearingError("workers: this world was destroyed")
         return self._workers
 
     @workers.setter
     def workers(self, value):
+        if not self._w:
+            raise BearingError("workers: this world was destroyed")
         try:
             self._workers = _workers("world.workers", value)
         except check.CheckError as e:
             raise BearingError(str(e)) from None
+        self._lib.bw_set_workers(self._w, -1 if value == "auto" else min(value, 1 << 20))
 
     def stats(self) -> dict:
         st = _ffi.Stats()

@@ -78,6 +78,12 @@ const char* bw_last_error(const bw_world* world);
 /* Adds a body; returns its slot, or a negative BG_E* code. */
 int32_t bw_add_body(bw_world* world, const bw_body* body);
 
+/* World.workers (src/world.js:501-524): how many threads besides the caller's the step's host side
+ * may use for its pair upkeep (the broadphase's overlap search and the walk over the pairs); -1,
+ * the reference's 'auto' and the default, is the machine's cores up to 16.  Results are the same
+ * bits whatever it is.  BG_EINVAL below -1. */
+int32_t bw_set_workers(bw_world* world, int32_t workers);
+
 /* The solve stage to call; NULL restores none (bw_step then fails with BG_EUNSUPPORTED). */
 int32_t bw_set_solver(bw_world* world, bw_solver solver, void* user);
 

@@ -140,6 +140,38 @@ def test_a_long_pair_list_is_marked_on_several_threads_with_the_same_result():
     b.destroy()
 
 
+def test_the_pair_upkeep_is_the_same_on_one_thread_and_on_many():
+    # World.workers sets the threads of the broadphase's overlap search (past 4,096 moved bodies)
+    # and of the walk over the pairs (past 131,072 pairs); with none, both run on the caller's
+    # thread alone, as the reference's World does with workers 0.  The 20,000-body pile moves every
+    # body at its first steps and passes 200,000 pairs by step 50, with pairs dropped as it falls.
+    host = _ffi.host()
+
+    def collide(user, bodies, gravity, pairs, out):
+        return host.bw_collide_pairs(bodies, gravity, pairs, out, 4)
+
+    hook = NARROWPHASE(collide)
+    one = World({"workers": 0}, solver=oracle_io.solver(0))
+    many = World({"workers": 7}, solver=oracle_io.solver(0))
+    for w in (one, many):
+        scenes.pile(w, count=20_000, extent=60.0)
+        assert host.bw_set_narrowphase(w._w, C.cast(hook, C.c_void_p), None) == 0
+    for i in range(55):
+        one.step(DT)
+        many.step(DT)
+        sa, sb = one.state(), many.state()
+        for k in ("position", "rotation", "velocity", "angular"):
+            assert sa[k].tobytes() == sb[k].tobytes(), f"step {i + 1}: {k}"
+        assert one.stats() == many.stats()
+        ca, cb = one.contacts(), many.contacts()
+        assert all(ca[k].tobytes() == cb[k].tobytes() for k in ca), f"step {i + 1}: contacts"
+    assert many.stats()["pairs"] >= 2 * 65536
+    for w in (one, many):
+        assert host.bw_set_narrowphase(w._w, None, None) == 0
+        w.destroy()
+    assert host.bw_set_workers(None, 0) == _ffi.BG_EINVAL
+
+
 def test_a_failing_narrowphase_fails_the_step():
     host = _ffi.host()
     hook = NARROWPHASE(lambda *args: _ffi.BG_ECUDA)
