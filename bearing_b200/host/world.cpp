@@ -338,6 +338,8 @@ struct bw_world {
   double cell = 0;
   std::unordered_map<uint64_t, std::vector<int32_t>> grid;
   std::vector<int32_t> largeList;
+  std::vector<int32_t> seen;
+  int32_t seenMark = 0;
   Pairs pairs;
   Contacts c;
   bw_solver solver = nullptr;
@@ -366,7 +368,7 @@ struct bw_world {
     grow(axes, 9 * s); grow(box, 6 * s); grow(motion, s); grow(invI, 6 * s); grow(start, 3 * s); grow(startQ, 4 * s);
     grow(type, s); grow(shape, s); grow(framed, s); grow(lock, s); grow(frozen, s); grow(awake, s);
     grow(jointHead, s); grow(awakeList, s); grow(transforms, 7 * s);
-    grow(fat, 6 * s); grow(filed, s); grow(isMoved, s); grow(large, s);
+    grow(fat, 6 * s); grow(filed, s); grow(isMoved, s); grow(large, s); grow(seen, s);
   }
 
   // _boundsOf: src/world.js:1581-1630 (boxes, spheres, capsules).
@@ -492,58 +494,38 @@ struct bw_world {
       fileIn(s);
       mark(s);
     }
-    // Each moved body's overlaps depend only on the grid and the fat boxes, which stay as they are
-    // until the next step, so they are found on several threads when many bodies moved; the pairs
-    // are then made in the moved bodies' order, each body's in slot order, as one thread would.
-    const int m = static_cast<int>(moved.size());
-    const int threads = std::max(1, std::min(hostThreads(), m / 2048));
-    std::vector<std::vector<int32_t>> found(static_cast<size_t>(threads));
-    std::vector<int32_t> counts(static_cast<size_t>(std::max(m, 1)));
-    ranges(m, threads, [&](int t, int lo, int hi) {
-      std::vector<int32_t> one;
-      for (int i = lo; i < hi; i++) {
-        overlaps(moved[i], one);
-        counts[i] = static_cast<int32_t>(one.size());
-        found[t].insert(found[t].end(), one.begin(), one.end());
+    std::vector<int32_t> found;
+    for (size_t i = 0; i < moved.size(); i++) {
+      const int a = moved[i];
+      isMoved[a] = 0;
+      const bool aStatic = type[a] == BG_STATIC;
+      found.clear();
+      seenMark++;
+      auto consider = [&](int b) {
+        if (b == a || seen[b] == seenMark) return;
+        seen[b] = seenMark;
+        if (aStatic && type[b] == BG_STATIC) return;
+        if (fatOverlap(a, b)) found.push_back(b);
+      };
+      if (large[a]) {
+        for (auto& kv : grid)
+          for (int b : kv.second) consider(b);
+      } else {
+        int64_t lo[3], hi[3];
+        cellRange(a, lo, hi);
+        for (int64_t x = lo[0]; x <= hi[0]; x++)
+          for (int64_t y = lo[1]; y <= hi[1]; y++)
+            for (int64_t z = lo[2]; z <= hi[2]; z++) {
+              auto it = grid.find(cellKey(x, y, z));
+              if (it == grid.end()) continue;
+              for (int b : it->second) consider(b);
+            }
       }
-    });
-    for (int t = 0; t < threads; t++) {
-      const int lo = static_cast<int>(static_cast<int64_t>(m) * t / threads);
-      const int hi = static_cast<int>(static_cast<int64_t>(m) * (t + 1) / threads);
-      size_t at = 0;
-      for (int i = lo; i < hi; i++) {
-        const int a = moved[i];
-        isMoved[a] = 0;
-        for (int k = 0; k < counts[i]; k++) pairs.found(a, found[t][at++], type.data());
-      }
+      for (int b : largeList) consider(b);
+      std::sort(found.begin(), found.end());
+      for (int b : found) pairs.found(a, b, type.data());
     }
     moved.clear();
-  }
-  // The bodies whose fat boxes overlap a's, in slot order: those filed in the cells a's fat box
-  // covers (every filed body, for a large box) and the large ones, but not a, nor a static body
-  // for a static a (src/broadphase.js:146-165).
-  void overlaps(int a, std::vector<int32_t>& out) const {
-    out.clear();
-    if (large[a]) {
-      for (const auto& kv : grid) out.insert(out.end(), kv.second.begin(), kv.second.end());
-    } else {
-      int64_t lo[3], hi[3];
-      cellRange(a, lo, hi);
-      for (int64_t x = lo[0]; x <= hi[0]; x++)
-        for (int64_t y = lo[1]; y <= hi[1]; y++)
-          for (int64_t z = lo[2]; z <= hi[2]; z++) {
-            auto it = grid.find(cellKey(x, y, z));
-            if (it != grid.end()) out.insert(out.end(), it->second.begin(), it->second.end());
-          }
-    }
-    out.insert(out.end(), largeList.begin(), largeList.end());
-    std::sort(out.begin(), out.end());
-    out.erase(std::unique(out.begin(), out.end()), out.end());
-    const bool aStatic = type[a] == BG_STATIC;
-    size_t k = 0;
-    for (const int b : out)
-      if (b != a && !(aStatic && type[b] == BG_STATIC) && fatOverlap(a, b)) out[k++] = b;
-    out.resize(k);
   }
 
   int awakeCount = 0;

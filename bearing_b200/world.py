@@ -324,7 +324,7 @@ class World:
     @property
     def workers(self):
         """World.workers (src/world.js:501-524): the threads besides the caller's that the step's
-        host side uses for its pair upkeep ('auto': the machine's cores, up to 16).  The solve stage
+        host side uses for its walk over the pairs ('auto': the machine's cores, up to 16).  The solve stage
         runs on the GPU whatever it is; as in the reference, results do not depend on it."""
         if not self._w:
             raise BearingError("workers: this world was destroyed")

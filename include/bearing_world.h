@@ -79,7 +79,7 @@ const char* bw_last_error(const bw_world* world);
 int32_t bw_add_body(bw_world* world, const bw_body* body);
 
 /* World.workers (src/world.js:501-524): how many threads besides the caller's the step's host side
- * may use for its pair upkeep (the broadphase's overlap search and the walk over the pairs); -1,
+ * may use for its walk over the pairs when their boxes meet on another device; -1,
  * the reference's 'auto' and the default, is the machine's cores up to 16.  Results are the same
  * bits whatever it is.  BG_EINVAL below -1. */
 int32_t bw_set_workers(bw_world* world, int32_t workers);

@@ -141,10 +141,9 @@ def test_a_long_pair_list_is_marked_on_several_threads_with_the_same_result():
 
 
 def test_the_pair_upkeep_is_the_same_on_one_thread_and_on_many():
-    # World.workers sets the threads of the broadphase's overlap search (past 4,096 moved bodies)
-    # and of the walk over the pairs (past 131,072 pairs); with none, both run on the caller's
-    # thread alone, as the reference's World does with workers 0.  The 20,000-body pile moves every
-    # body at its first steps and passes 200,000 pairs by step 50, with pairs dropped as it falls.
+    # World.workers sets the threads of the walk over the pairs (past 131,072 pairs); with none it
+    # runs on the caller's thread alone, as the reference's World does with workers 0.  The
+    # 20,000-body pile passes 200,000 pairs by step 50, with pairs dropped as it falls.
     host = _ffi.host()
 
     def collide(user, bodies, gravity, pairs, out):
